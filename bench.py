@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Phases 1-4 of cf1-rs on B200: distinct k-mers classified per second.
+
+Default workload: the 3.1 Gbp k=31 synthetic genome (workload 5: 25
+chromosomes, ~50% repeats, poly-N every 10 Mb, 256 bins), generated seeded
+in host memory (the reference's GRCh38 input is not available).  A step is
+one pass of phases 1-4 over the whole genome: pack, minimizer histogram,
+partition, super k-mer routing, per-bin sort + unique, MPHF construction and
+classification into the 5-bit state vector.
+
+  value : distinct k-mers / device time of a step, input resident in HBM
+          (library CUDA events on its stream; the input is 3.1 GB, larger
+          than the 126 MB L2, so steps do not reuse cached data)
+  e2e   : the same metric through the C ABI from host buffers: records
+          copied into pinned staging, host->device copy, phases 1-4, and the
+          state vector copied back, timed on the host around synchronous calls
+
+Both MPHF forms run: plain per-bin GPU BBHash, and the learned index +
+batched (persistent queue kernels) form; the headline is the faster one,
+the other is reported beside it.  --impl reference times the CPU oracle port
+(all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    1: dict(k=31, bins=128, name="1 record, 5 Mbp uniform ACGT, k=31"),
+    2: dict(k=31, bins=128, name="transcriptome: 20k genes, 100k transcripts, k=31", short=True),
+    3: dict(k=31, bins=128, name="repetitive genome 200 Mbp, 24 chromosomes, k=31"),
+    4: dict(k=63, bins=128, name="repetitive genome 1 Gbp, 30 chromosomes, k=63"),
+    5: dict(k=31, bins=256, name="human-scale synthetic genome 3.1 Gbp, 25 chromosomes, ~50% repeats, k=31"),
+}
+METRIC = "k-mers classified/s, 1 B200: learned-index vs GPU BBHash vs CPU (bit-exact)"
+UNIT = "distinct k-mers/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
+    p.add_argument("--workload", type=int, default=5, choices=sorted(WORKLOADS))
+    p.add_argument("--scale", type=float, default=1.0)
+    p.add_argument("--forms", default="bbhash,learned")
+    p.add_argument("--cpu-sample-mbp", type=float, default=40.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def committed_traffic():
+    """dram bytes per classify launch from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "classify_traffic.json")) as f:
+            return json.load(f)
+    except OSError:
+        return None
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=5)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample(x, sample_bp: int):
+    """First records of the workload up to sample_bp bases (a prefix of the
+    first chromosome for genome workloads)."""
+    off = x.offsets
+    end = 0
+    recs = [0]
+    i = 0
+    while i < len(off) - 1 and end < sample_bp:
+        end = min(int(off[i + 1]), int(off[0]) + sample_bp)
+        recs.append(end - int(off[0]))
+        i += 1
+    seq = np.ascontiguousarray(x.seq[int(off[0]):end])
+    return seq, np.array(recs, dtype=np.uint64)
+
+
+def run_cpu_baseline(x, k: int, sample_bp: int, threads: int):
+    from oracle import oracle as o
+
+    seq, off = cpu_sample(x, sample_bp)
+    t0 = time.perf_counter()
+    r = o.run(k, seq, off, nthreads=threads, method=0)
+    dt = time.perf_counter() - t0
+    return len(r.states) / dt, dt, len(seq), len(r.states)
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import cf1_rs_b200 as cg
+
+    wl = WORKLOADS[args.workload]
+    x = cg.SynthInput(args.workload, scale=args.scale)
+    threads = os.cpu_count() or 1
+    sample_bp = int(args.cpu_sample_mbp * 1e6)
+    for _ in range(args.warmup):
+        run_cpu_baseline(x, wl["k"], sample_bp, threads)
+    rates, secs = [], []
+    for _ in range(args.steps):
+        rate, dt, nb, nd = run_cpu_baseline(x, wl["k"], sample_bp, threads)
+        rates.append(rate)
+        secs.append(dt)
+    value = len(rates) / sum(1.0 / r for r in rates)
+    sample = f"first {nb / 1e6:.1f} Mbp of the workload ({nd} distinct k-mers) per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(secs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64" if wl["k"] <= 32 else "u128",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": wl["name"], "k": wl["k"], "num_bins": wl["bins"], "scale": args.scale,
+                   "parallelism": "cpu threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "CPU oracle port of phases 1-4 (phase-3 sort+dedup, classify.rs restatement); "
+                "the Rust reference cannot be built here (no cargo)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import cf1_rs_b200 as cg
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+
+    def maxall(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sumall(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    wl = WORKLOADS[args.workload]
+    k, bins = wl["k"], wl["bins"]
+    # weak scaling: every rank classifies its own genome of the same size
+    x = cg.SynthInput(args.workload, scale=args.scale, seed=0 if rank == 0 else 1000 + rank)
+    forms = {}
+    clocks = Clocks(local)
+    clock_info = None
+    for form in args.forms.split(","):
+        batched = form == "learned"
+        g = cg.Cf1Gpu(k=k, num_bins=bins, device=local, mode=form, batched=batched,
+                      track_short_seqs=bool(wl.get("short")))
+        g.add_records(x.seq, x.offsets)
+        g.upload()
+        for _ in range(args.warmup):
+            g.run_resident()
+        barrier()
+        if clock_info is None:
+            clocks.start()
+        ms, ms_cls, launches, phase = [], [], 0, {}
+        for _ in range(args.steps):
+            g.run_resident()
+            s = g.stats()
+            ms.append(s["ms_total"])
+            ms_cls.append(s["ms_classify_kernel"])
+            launches += s["n_kernel_launches"]
+            for key in ("ms_phase1", "ms_phase2", "ms_phase3_sort", "ms_phase3_mphf", "ms_phase4"):
+                phase[key] = phase.get(key, 0.0) + s[key] / args.steps
+        barrier()
+        if clock_info is None:
+            clock_info = clocks.stop()
+        total_ms = maxall(sum(ms))
+        distinct = sumall(s["n_distinct"])
+        forms[form] = dict(
+            value=distinct * args.steps / (total_ms / 1e3), ms_per_step=total_ms / args.steps,
+            ms_classify_kernel=maxall(statistics.mean(ms_cls)), launches=launches, stats=s,
+            phases_ms={k2: round(v, 3) for k2, v in phase.items()},
+            learned=g.learned_stats() if form == "learned" else None, ctx=g)
+        if form != args.forms.split(",")[-1]:
+            g.close()
+            forms[form]["ctx"] = None
+    head_name = max(forms, key=lambda f: forms[f]["value"])
+    head = forms[head_name]
+    s = head["stats"]
+    # ---- end to end through the C ABI from host buffers
+    e2e = None
+    if not args.no_e2e:
+        g = head["ctx"]
+        if g is None:
+            g = cg.Cf1Gpu(k=k, num_bins=bins, device=local, mode=head_name, batched=head_name == "learned",
+                          track_short_seqs=bool(wl.get("short")))
+        words = np.empty((s["n_distinct"] + 11) // 12, np.uint64)
+        times = []
+        for i in range(args.warmup + args.steps):
+            barrier()
+            t0 = time.perf_counter()
+            g.reset_input()
+            g.add_records(x.seq, x.offsets)
+            g.run()
+            g.states(out=words)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dt)
+        e2e_s = maxall(sum(times))
+        e2e = {"value": sumall(s["n_distinct"]) * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(s["n_bases"] + s["n_records"]),
+               "d2h_bytes_per_step": int(words.nbytes), "ms_per_step": 1e3 * e2e_s / args.steps}
+        g.close()
+    for f in forms.values():
+        if f["ctx"] is not None:
+            f["ctx"].close()
+        f["ctx"] = None
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    peaks, peak_kind = measured_peaks()
+    L = s["n_bases"] + s["n_records"]
+    n_occ, n_dist = s["n_kmer_occurrences"], s["n_distinct"]
+    w = 8 if k <= 32 else 16
+    # classification kernel: 2-bit sequence read once + one 32-B sector read
+    # and one written per occurrence (state word RMW); MPHF probes excluded
+    b4 = 0.25 * L + 64.0 * n_occ
+    ach = b4 / (head["ms_classify_kernel"] / 1e3) / 1e9
+    traffic = committed_traffic()
+    roofline = {"kernel": "classify_kernel", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "peak_kind": peak_kind,
+                "traffic": traffic.get("dram_bytes_per_launch_scaled") if traffic else None,
+                "algorithmic_bytes": b4}
+    # whole phases 1-4 (algorithmic bytes of SURVEY-style accounting)
+    s_bins = 8.0 * s["n_superkmers"]
+    b14 = 0.25 * L + 2 * s_bins + 2 * w * n_occ + 2 * w * n_dist + b4
+    pipe = {"achieved": b14 / (head["ms_per_step"] / 1e3) / 1e9, "unit": "GB/s", "algorithmic_bytes": b14,
+            "frac": b14 / (head["ms_per_step"] / 1e3) / 1e9 / peaks["hbm_gbs"]}
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, dt, nb, nd = run_cpu_baseline(x, k, int(args.cpu_sample_mbp * 1e6), os.cpu_count() or 1)
+        cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"first {nb / 1e6:.1f} Mbp of the workload ({nd} distinct k-mers), {dt:.1f} s"}
+    line = {
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64" if k <= 32 else "u128", "data": "synthetic (seeded generator)",
+        "config": {"workload": wl["name"], "k": k, "num_bins": bins, "scale": args.scale, "form": head_name,
+                   "bases": int(s["n_bases"]), "records": int(s["n_records"]), "distinct_kmers": int(n_dist),
+                   "kmer_occurrences": int(n_occ), "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "input 3.1 GB > 126 MB L2 (no flush needed)"},
+        "bp_per_s": (s["n_bases"] * world) / (head["ms_per_step"] / 1e3),
+        "roofline": roofline,
+        "roofline_phases_1_4": pipe,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clock_info,
+        "gpu_launches": int(head["launches"]),
+        "forms": {f: {"value": v["value"], "ms_per_step": v["ms_per_step"],
+                      "ms_classify_kernel": v["ms_classify_kernel"], "phases_ms": v["phases_ms"],
+                      "bbhash_levels": int(v["stats"]["bbhash_levels"]), "mphf_bytes": int(v["stats"]["mphf_bytes"]),
+                      "learned_bins": int(v["stats"]["learned_bins"]), "fallback_bins": int(v["stats"]["fallback_bins"]),
+                      "learned": v["learned"]} for f, v in forms.items()},
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,34 @@
+// Host-side owner of a per-bin BBHash (built by cf1_bbhash.cu).
+#pragma once
+#include "cf1_internal.cuh"
+
+namespace cf1 {
+
+template <class KeyT>
+struct BBHashBuild {
+  std::vector<DevBuf *> A, R;  // per level: bit array, rank prefix (words + 1)
+  uint32_t levels = 0, nbins = 0;
+  uint64_t bytes = 0;
+
+  BBHashBuild() = default;
+  BBHashBuild(const BBHashBuild &) = delete;
+  BBHashBuild &operator=(const BBHashBuild &) = delete;
+  ~BBHashBuild();
+
+  // Builds over the bins with sel[b] != 0 (sel == nullptr: every bin); the
+  // other bins get no levels.  Synchronises the stream between levels.
+  // ws0/ws1 (optional, ws_cap keys each, not aliasing keys) hold the keys
+  // still unplaced between levels; without them the builder allocates.
+  void build(const KeyT *keys, const uint64_t *seg_off, uint32_t nbins, const uint32_t *sel, cudaStream_t s,
+             KeyT *ws0 = nullptr, KeyT *ws1 = nullptr, uint64_t ws_cap = 0);
+  BBView view() const;
+  void clear();
+  uint64_t level_words(uint32_t l) const;
+  const BBMeta *meta_device() const { return meta_.as<const BBMeta>(); }
+
+ private:
+  DevBuf meta_, aptr_, rptr_, base_, rem_[2], rem_off_[2], tile_off_, tile_cnt_, tile_out_, C_, wcnt_, woff_, pc_,
+      scan_tmp_;
+};
+
+}  // namespace cf1

@@ -1,0 +1,82 @@
+// The library context behind the C ABI (cf1gpu_ctx).
+#pragma once
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/cf1gpu.h"
+#include "cf1_bbhash.cuh"
+#include "cf1_internal.cuh"
+#include "cf1_learned.cuh"
+
+namespace cf1 {
+
+// Pinned host staging for the concatenated input.
+struct PinnedBuf {
+  uint8_t *p = nullptr;
+  size_t cap = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf &) = delete;
+  PinnedBuf &operator=(const PinnedBuf &) = delete;
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  // Grows to at least `bytes`, keeping the first `keep` bytes.
+  void reserve(size_t bytes, size_t keep);
+};
+
+template <class KeyT>
+struct Backend {
+  SortScratch<KeyT> sort;
+  BBHashBuild<KeyT> bb;
+  LearnedBuild<KeyT> li;
+};
+
+struct Tuning {
+  uint32_t sk_tile = 2048;      // k-mer positions per minimizer tile (1024/2048/4096)
+  int persistent_ctas = 0;      // 0: derived from the SM count in batched mode
+  uint32_t leaf_size = 32;      // learned index keys per leaf
+};
+
+}  // namespace cf1
+
+struct cf1gpu_ctx {
+  cf1gpu_opts opts;
+  int k = 31, m = 15, w = 17;
+  bool wide = false;  // k > 32: 128-bit keys
+  std::string last_error;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[12] = {};
+  int num_sms = 148;
+  cf1::Tuning tune;
+  cf1::LearnedOpts learned;
+
+  // host input: records concatenated, one placeholder after each
+  cf1::PinnedBuf host;
+  uint64_t L = 0;
+  uint64_t n_records = 0;
+  uint64_t n_bases = 0;
+  std::vector<std::pair<std::string, uint64_t>> short_seqs;
+  bool uploaded = false;
+  bool ran = false;
+
+  // device buffers
+  cf1::DevBuf d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
+      d_keys, d_dist, d_dist_off, d_states, d_scan, d_seen, d_qin, d_qout, d_queue;
+  cf1::Backend<uint64_t> b64;
+  cf1::Backend<cf1::Key2> b128;
+
+  // results of the last run
+  uint64_t n_super = 0, n_occ = 0, n_distinct = 0, n_bins_eff = 0, cas_retries = 0;
+  uint32_t nbins = 0;
+  cf1gpu_stats stats{};
+};
+
+namespace cf1 {
+template <class KeyT>
+inline Backend<KeyT> &ctx_backend(cf1gpu_ctx *c);
+template <>
+inline Backend<uint64_t> &ctx_backend<uint64_t>(cf1gpu_ctx *c) { return c->b64; }
+template <>
+inline Backend<Key2> &ctx_backend<Key2>(cf1gpu_ctx *c) { return c->b128; }
+}  // namespace cf1

@@ -1,0 +1,150 @@
+// Flat host image of the device MPHF and Mphf::hash over it on the CPU.
+//
+// Phase 5 (src/output.rs) calls Mphf::hash / bucket_id for every k-mer from
+// many host threads (src/directed_kmer.rs:81-109, src/output.rs:728-731).
+// The image holds everything a query needs: the bucket -> bin table, the
+// per-bin slot offsets, the BBHash levels and, in learned mode, the roots,
+// leaves and the sorted distinct keys.  The query code is the device code
+// (cf1_mphf.cuh), compiled for the host.
+#include <cstring>
+#include <vector>
+
+#include "cf1_context.cuh"
+#include "cf1_mphf.cuh"
+#include "cf1_pipeline.cuh"
+
+namespace cf1 {
+
+namespace {
+
+constexpr uint64_t IMAGE_MAGIC = 0x3146485048504D43ull;  // "CMPHPHF1"
+
+struct ImageHeader {
+  uint64_t magic;
+  uint32_t version, k, m, nbins, levels, learned, key_words, pad;
+  uint64_t n_distinct, n_leaves;
+  uint64_t lut_off, dist_off_off, meta_off, levels_off, roots_off, leaves_off, keys_off, total;
+};
+struct LevelEntry {
+  uint64_t a_off, r_off, nwords;
+};
+
+inline uint64_t align8(uint64_t x) { return (x + 7) & ~7ull; }
+
+template <class KeyT>
+size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
+  Backend<KeyT> &be = ctx_backend<KeyT>(c);
+  const bool learned = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED;
+  const uint32_t B = c->nbins, NL = be.bb.levels;
+  const uint64_t nleaves = learned ? be.li.stats.leaves : 0;
+  ImageHeader h;
+  std::memset(&h, 0, sizeof(h));
+  h.magic = IMAGE_MAGIC;
+  h.version = 1;
+  h.k = c->k;
+  h.m = c->m;
+  h.nbins = B;
+  h.levels = NL;
+  h.learned = learned;
+  h.key_words = KOps<KeyT>::WORDS;
+  h.n_distinct = c->n_distinct;
+  h.n_leaves = nleaves;
+  uint64_t off = align8(sizeof(ImageHeader));
+  h.lut_off = off;
+  off = align8(off + NUM_BUCKETS * sizeof(uint16_t));
+  h.dist_off_off = off;
+  off = align8(off + (B + 1) * sizeof(uint64_t));
+  h.meta_off = off;
+  off = align8(off + (uint64_t)NL * B * sizeof(BBMeta));
+  h.levels_off = off;
+  off = align8(off + (uint64_t)NL * sizeof(LevelEntry));
+  std::vector<LevelEntry> lev(NL);
+  for (uint32_t l = 0; l < NL; l++) {
+    uint64_t nw = be.bb.A[l]->cap / 8;
+    lev[l].nwords = nw;
+    lev[l].a_off = off;
+    off = align8(off + nw * 8);
+    lev[l].r_off = off;
+    off = align8(off + (nw + 1) * 8);
+  }
+  h.roots_off = off;
+  off = align8(off + (learned ? B * sizeof(LIRoot) : 0));
+  h.leaves_off = off;
+  off = align8(off + nleaves * sizeof(LILeaf));
+  h.keys_off = off;
+  off = align8(off + (learned ? c->n_distinct * sizeof(KeyT) : 0));
+  h.total = off;
+  if (!dst) return off;
+  if (cap < off) throw Error(CF1GPU_ERR_INVALID_ARG, "export buffer too small");
+  if (reinterpret_cast<uintptr_t>(dst) % 8) throw Error(CF1GPU_ERR_INVALID_ARG, "export buffer must be 8-byte aligned");
+  char *d = static_cast<char *>(dst);
+  cudaStream_t s = c->stream;
+  std::memcpy(d, &h, sizeof(h));
+  CF1_CUDA(cudaMemcpyAsync(d + h.lut_off, c->d_lut.p, NUM_BUCKETS * 2, cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaMemcpyAsync(d + h.dist_off_off, c->d_dist_off.p, (B + 1) * 8, cudaMemcpyDeviceToHost, s));
+  if (NL)
+    CF1_CUDA(cudaMemcpyAsync(d + h.meta_off, be.bb.meta_device(), (size_t)NL * B * sizeof(BBMeta), cudaMemcpyDeviceToHost, s));
+  std::memcpy(d + h.levels_off, lev.data(), NL * sizeof(LevelEntry));
+  for (uint32_t l = 0; l < NL; l++) {
+    CF1_CUDA(cudaMemcpyAsync(d + lev[l].a_off, be.bb.A[l]->p, lev[l].nwords * 8, cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaMemcpyAsync(d + lev[l].r_off, be.bb.R[l]->p, (lev[l].nwords + 1) * 8, cudaMemcpyDeviceToHost, s));
+  }
+  if (learned) {
+    CF1_CUDA(cudaMemcpyAsync(d + h.roots_off, be.li.roots_device(), B * sizeof(LIRoot), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaMemcpyAsync(d + h.leaves_off, be.li.leaves_device(), nleaves * sizeof(LILeaf), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaMemcpyAsync(d + h.keys_off, c->d_dist.p, c->n_distinct * sizeof(KeyT), cudaMemcpyDeviceToHost, s));
+  }
+  CF1_CUDA(cudaStreamSynchronize(s));
+  return off;
+}
+
+template <class KeyT>
+void host_query_impl(const ImageHeader &h, const char *img, const uint64_t *keys, size_t n, uint64_t *slots) {
+  std::vector<const uint64_t *> A(h.levels), R(h.levels);
+  const LevelEntry *lev = reinterpret_cast<const LevelEntry *>(img + h.levels_off);
+  for (uint32_t l = 0; l < h.levels; l++) {
+    A[l] = reinterpret_cast<const uint64_t *>(img + lev[l].a_off);
+    R[l] = reinterpret_cast<const uint64_t *>(img + lev[l].r_off);
+  }
+  MphfView<KeyT> v;
+  v.keys = reinterpret_cast<const KeyT *>(img + h.keys_off);
+  v.dist_off = reinterpret_cast<const uint64_t *>(img + h.dist_off_off);
+  v.bb.A = A.data();
+  v.bb.R = R.data();
+  v.bb.meta = reinterpret_cast<const BBMeta *>(img + h.meta_off);
+  v.bb.levels = h.levels;
+  v.bb.nbins = h.nbins;
+  v.li.roots = reinterpret_cast<const LIRoot *>(img + h.roots_off);
+  v.li.leaves = reinterpret_cast<const LILeaf *>(img + h.leaves_off);
+  v.li.k = (int)h.k;
+  v.learned = (int)h.learned;
+  const uint16_t *lut = reinterpret_cast<const uint16_t *>(img + h.lut_off);
+  for (size_t i = 0; i < n; i++) {
+    KeyT key = KOps<KeyT>::make(keys[i * KOps<KeyT>::WORDS], KOps<KeyT>::WORDS == 2 ? keys[i * 2 + 1] : 0);
+    uint64_t mz = kmer_minimizer(key, (int)h.k, (int)h.m);
+    uint32_t bin = lut[mix_bucket((uint32_t)mz)];
+    uint64_t s = mphf_slot(v, bin, key);
+    slots[i] = s == SLOT_NONE ? 0 : s;  // unwrap_or(0), src/mphf.rs:269
+  }
+}
+
+}  // namespace
+
+size_t export_mphf(cf1gpu_ctx *c, void *dst, size_t cap) {
+  if (c->wide) return export_impl<Key2>(c, dst, cap);
+  return export_impl<uint64_t>(c, dst, cap);
+}
+
+void host_query(const void *image, size_t bytes, const uint64_t *keys, size_t n, uint64_t *slots) {
+  if (bytes < sizeof(ImageHeader) || reinterpret_cast<uintptr_t>(image) % 8)
+    throw Error(CF1GPU_ERR_INVALID_ARG, "MPHF image too small or misaligned");
+  ImageHeader h;
+  std::memcpy(&h, image, sizeof(h));
+  if (h.magic != IMAGE_MAGIC || h.version != 1 || h.total > bytes)
+    throw Error(CF1GPU_ERR_INVALID_ARG, "not a cf1 MPHF image");
+  const char *img = static_cast<const char *>(image);
+  if (h.key_words == 2) host_query_impl<Key2>(h, img, keys, n, slots);
+  else host_query_impl<uint64_t>(h, img, keys, n, slots);
+}
+
+}  // namespace cf1

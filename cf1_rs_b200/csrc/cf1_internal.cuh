@@ -1,0 +1,185 @@
+// Host-side plumbing shared by the kernels' launchers and the pipeline.
+#pragma once
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "cf1_common.cuh"
+
+namespace cf1 {
+
+// A failed CUDA call or a broken invariant inside the library; the C ABI turns
+// it into a status code and a message.
+struct Error : std::runtime_error {
+  int status;
+  Error(int st, const std::string &m) : std::runtime_error(m), status(st) {}
+};
+
+#define CF1_CUDA(call)                                                                 \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      throw ::cf1::Error(e_ == cudaErrorMemoryAllocation ? -2 : -3,                    \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+// Kernels launched by this library (every launch is followed by
+// CF1_LAUNCH_CHECK, which counts it).
+extern std::atomic<uint64_t> g_launches;
+#define CF1_LAUNCH_CHECK()                                        \
+  do {                                                            \
+    ::cf1::g_launches.fetch_add(1, std::memory_order_relaxed);    \
+    CF1_CUDA(cudaGetLastError());                                 \
+  } while (0)
+
+// Device allocation that grows on demand and keeps its capacity.
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  void *reserve(size_t bytes) {
+    if (bytes <= cap && p) return p;
+    release();
+    size_t b = bytes ? bytes : 16;
+    CF1_CUDA(cudaMalloc(&p, b));
+    cap = b;
+    return p;
+  }
+  template <class T>
+  T *as() const { return static_cast<T *>(p); }
+  template <class T>
+  T *get(size_t n) { return static_cast<T *>(reserve(n * sizeof(T))); }
+};
+
+inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+// ------------------------------------------------------------ util kernels ----
+// Exclusive prefix sum of n values into out[0..n] (out[n] = total).
+// `scratch` grows as needed.
+void exclusive_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, DevBuf &scratch, cudaStream_t s);
+void exclusive_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, DevBuf &scratch, cudaStream_t s);
+
+// Tiles of TILE elements over segments given by seg_off[0..nseg]; a tile never
+// crosses a segment edge.  tile_off[0..nseg] (u32) gets the first tile of each
+// segment; tile_off[nseg] is the tile count.
+void segment_tiles(const uint64_t *seg_off, uint32_t nseg, uint32_t tile, uint32_t *tile_off, cudaStream_t s);
+
+// ------------------------------------------------------------ phase kernels ----
+void launch_pack(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, cudaStream_t s);
+
+struct SuperkmerArgs {
+  const uint64_t *W;
+  const uint64_t *NM;
+  uint64_t L;
+  int k, m, w;
+  uint32_t tile;          // k-mer positions per tile
+  uint64_t n_tiles;
+  uint32_t *tile_counter; // persistent mode: atomic work queue (zeroed); nullptr = one CTA per tile
+  // histogram mode
+  uint32_t *hist;         // [65536] super k-mers per bucket
+  unsigned long long *n_kmers;  // valid k-mer windows
+  // emit mode
+  const uint16_t *lut;    // bucket -> bin
+  uint32_t num_bins;
+  const uint64_t *rec_off;      // [num_bins+1]
+  uint32_t *bin_cursor;         // [num_bins] zeroed
+  uint64_t *records;
+  uint32_t *err;
+};
+void launch_superkmer_hist(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s);
+void launch_superkmer_emit(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s);
+// Greedy partition of the histogram (src/minimizer.rs:116-172) into the
+// bucket->bin table, plus per-bin record offsets rec_off[0..num_bins].
+void launch_partition(const uint32_t *hist, uint32_t num_bins, uint16_t *lut, uint64_t *rec_off, uint32_t *n_bins_eff,
+                      cudaStream_t s);
+
+// ------------------------------------------------------------ phase 3 ----
+template <class KeyT>
+struct SortScratch {
+  DevBuf alt, hist, hscan, tile_off, tile_cnt, tile_out, scan_tmp;
+};
+
+// Per record k-mer offsets: kpre[i] = sum of n over records < i (kpre[n_rec] = total).
+void record_kmer_prefix(const uint64_t *records, uint64_t n_rec, uint64_t *kpre, DevBuf &lens, DevBuf &scratch,
+                        cudaStream_t s);
+
+// Writes each k-mer's canonical form; keys[kpre[i] + j] is k-mer j of record
+// i.  Writes past n_keys or reads past base L are skipped and flagged in err.
+template <class KeyT>
+void launch_expand(const uint64_t *records, uint64_t n_rec, const uint64_t *kpre, const uint64_t *W, int k, KeyT *keys,
+                   uint64_t n_keys, uint64_t L, uint32_t *queue, uint32_t *err, int persistent_ctas, cudaStream_t s);
+
+// Sorts each segment [seg_off[b], seg_off[b+1]) of keys ascending (LSD radix,
+// segmented).  The result is in `keys` on return.
+template <class KeyT>
+void segmented_sort(KeyT *keys, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int key_bits, SortScratch<KeyT> &sc,
+                    cudaStream_t s);
+
+// Adjacent-unique per segment: writes distinct keys to `out` and their segment
+// offsets to out_off[0..nseg].
+template <class KeyT>
+void segmented_unique(const KeyT *keys, uint64_t n, const uint64_t *seg_off, uint32_t nseg, KeyT *out, uint64_t *out_off,
+                      SortScratch<KeyT> &sc, cudaStream_t s);
+
+// ------------------------------------------------------------ MPHF ----
+struct BBMeta {
+  uint64_t word_off;  // first word of this (level, bin) block in the level array
+  uint64_t m_bits;    // block size in bits (0: bin has no keys at this level)
+  uint64_t rank_adj;  // bin-local slot base minus the level rank at word_off (mod 2^64)
+};
+
+// Device view of a per-bin BBHash (read by query kernels).
+struct BBView {
+  const uint64_t *const *A;  // per level: cleaned bit array
+  const uint64_t *const *R;  // per level: exclusive popcount per word
+  const BBMeta *meta;        // [levels * nbins]
+  uint32_t levels, nbins;
+};
+
+constexpr int LI_HIDDEN = 16;
+struct LIRoot {
+  float w1[LI_HIDDEN], b1[LI_HIDDEN], w2[LI_HIDDEN], b2;
+  uint64_t hmin;     // high64 of the bin's smallest key
+  float inv_range;   // 1 / (high64(max) - high64(min))
+  uint32_t n_leaves; // leaves of this bin
+  uint64_t leaf_off; // first leaf of this bin in the leaf table
+  uint32_t use_learned;  // 0: bin served by BBHash
+  uint32_t max_err;
+};
+struct LILeaf {
+  uint64_t hfirst;   // high64 of the leaf's first key
+  uint32_t first_rank;
+  uint32_t err;      // max |prediction - rank| over the leaf's keys
+  float slope;       // ranks per unit of high64
+  uint32_t n;        // keys routed to the leaf (0: empty)
+};
+struct LIView {
+  const LIRoot *roots;  // [nbins]
+  const LILeaf *leaves;
+  int k;
+};
+
+// Everything a slot query needs: bin -> local slot, then + dist_off[bin].
+template <class KeyT>
+struct MphfView {
+  const KeyT *keys;        // distinct keys, bins in order, each bin sorted
+  const uint64_t *dist_off;  // [nbins+1]
+  BBView bb;
+  LIView li;
+  int learned;             // 0: BBHash for every bin
+};
+
+}  // namespace cf1

@@ -1,0 +1,299 @@
+// Phases 1 and 2 on the device: input packing, canonical-minimizer histogram
+// (src/minimizer.rs:27-110), greedy partition (src/minimizer.rs:116-172) and
+// super k-mer routing into bins (src/superkmer.rs:21-153).
+//
+// The reference routes 2-bit-packed super k-mers to per-bin files
+// (src/superkmer.rs:156-210).  Here the whole input stays resident in HBM as a
+// 2-bit array, so a routed super k-mer is an 8-byte record (first position,
+// k-mer count, bin) grouped by bin; phases 3 and 4 read the bases through it.
+#include "cf1_device_util.cuh"
+#include "cf1_internal.cuh"
+
+namespace cf1 {
+
+namespace {
+
+// ---------------------------------------------------------------- pack ----
+// One thread per 64 input bytes: two words of W and one word of NM.  A byte is
+// a base when (byte & 0xDF) is one of 'A' 'C' 'G' 'T' (upper- or lower-case,
+// src/dna.rs:64-92); bits 1-2 of the upper-case letter give A0 C1 G3 T2, and
+// one xor fixes G/T.
+__global__ void pack_kernel(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, uint64_t n_nm) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_nm) return;
+  uint64_t base = t * 64;
+  uint64_t bytes[8];
+  if (base + 64 <= L) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(ascii + base);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      uint4 v = src[i];
+      bytes[2 * i] = ((uint64_t)v.y << 32) | v.x;
+      bytes[2 * i + 1] = ((uint64_t)v.w << 32) | v.z;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      uint64_t x = 0;
+      for (int j = 0; j < 8; j++) {
+        uint64_t p = base + 8 * i + j;
+        uint64_t c = p < L ? ascii[p] : (uint64_t)'N';
+        x |= c << (8 * j);
+      }
+      bytes[i] = x;
+    }
+  }
+  uint64_t w0 = 0, w1 = 0, nm = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      uint32_t c = (uint32_t)(bytes[i] >> (8 * j)) & 0xFF;
+      uint32_t u = c & 0xDF;
+      bool ok = (u == 'A') | (u == 'C') | (u == 'G') | (u == 'T');
+      uint32_t b = (u >> 1) & 3;
+      b ^= b >> 1;
+      b = ok ? b : 0;
+      int idx = 8 * i + j;
+      if (idx < 32) w0 |= (uint64_t)b << (62 - 2 * idx);
+      else w1 |= (uint64_t)b << (62 - 2 * (idx - 32));
+      nm |= (uint64_t)(!ok) << idx;
+    }
+  }
+  W[2 * t] = w0;
+  W[2 * t + 1] = w1;
+  NM[t] = nm;
+}
+
+// -------------------------------------------------------------- super k-mers ----
+// One CTA per tile of T = BLOCK*ITEMS k-mer start positions (or, in persistent
+// mode, tiles pulled from an atomic counter).  The tile's bases span
+// T + k - 1 positions, so consecutive tiles overlap by k-1 bases.
+//   1. order keys of the T + w - 1 m-mers into shared memory;
+//   2. sliding-window minimum over w by log2(w) doubling passes;
+//   3. a k-mer is valid when its window holds no placeholder; a super k-mer
+//      starts at a valid k-mer whose predecessor in the tile is invalid or has
+//      another minimizer, and runs while the minimizer stays the same.
+template <int BLOCK, int ITEMS, bool EMIT>
+__global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
+  constexpr uint32_t T = BLOCK * ITEMS;
+  extern __shared__ uint64_t dyn[];
+  uint64_t *bufA = dyn;
+  uint64_t *bufB = dyn + T + 64;
+  uint32_t *s_cnt = reinterpret_cast<uint32_t *>(dyn + 2 * (T + 64));
+  uint32_t *s_base = s_cnt + (EMIT ? a.num_bins : 0);
+  __shared__ uint32_t s_tile;
+  const int k = a.k, m = a.m, w = a.w;
+  const unsigned tid = threadIdx.x;
+  const uint64_t NK = a.L - (uint64_t)k + 1;
+  if (EMIT) {
+    for (uint32_t b = tid; b < a.num_bins; b += BLOCK) s_cnt[b] = 0;
+  }
+  __syncthreads();
+  uint64_t tile = blockIdx.x;
+  unsigned long long my_kmers = 0;
+  for (;;) {
+    if (a.tile_counter) {
+      if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+      __syncthreads();
+      tile = s_tile;
+    }
+    if (tile >= a.n_tiles) break;
+    const uint64_t P0 = tile * T;
+    const uint32_t nk = (uint32_t)min((uint64_t)T, NK - P0);
+    const uint32_t nm = nk + w - 1;
+    for (uint32_t q = tid; q < nm; q += BLOCK) {
+      uint32_t fw = (uint32_t)KOps<uint64_t>::extract(a.W, P0 + q, m);
+      bufA[q] = mmer_order(fw, m);
+    }
+    __syncthreads();
+    uint64_t *src = bufA, *dst = bufB;
+    uint32_t len = nm, span = 1;
+    while (span * 2 <= (uint32_t)w) {
+      for (uint32_t q = tid; q + span < len; q += BLOCK) {
+        uint64_t x = src[q], y = src[q + span];
+        dst[q] = x < y ? x : y;
+      }
+      __syncthreads();
+      uint64_t *t2 = src; src = dst; dst = t2;
+      len -= span;
+      span *= 2;
+    }
+    for (uint32_t p = tid; p < nk; p += BLOCK) {
+      uint64_t x = src[p], y = src[p + w - span];
+      uint64_t v = x < y ? x : y;
+      if (!window_clean(a.NM, P0 + p, k)) v = ~0ull;
+      dst[p] = v;
+    }
+    __syncthreads();
+    const uint64_t *z = dst;
+    uint32_t rp[ITEMS], rn[ITEMS], rb[ITEMS], rl[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+      uint32_t p = i * BLOCK + tid;
+      rn[i] = 0;
+      rb[i] = 0;
+      rl[i] = 1;
+      rp[i] = p;
+      if (p < nk) {
+        uint64_t v = z[p];
+        if (v != ~0ull && (p == 0 || z[p - 1] != v)) {
+          uint32_t e = p + 1;
+          while (e < nk && z[e] == v) e++;
+          rn[i] = e - p;
+          uint32_t bucket = mix_bucket((uint32_t)v);
+          if (!EMIT) {
+            atomicAdd(&a.hist[bucket], 1u);
+            my_kmers += rn[i];
+          } else {
+            uint32_t bin = a.lut[bucket];
+            rb[i] = bin;
+            rl[i] = atomicAdd(&s_cnt[bin], 1u);
+          }
+        }
+      }
+    }
+    if (EMIT) {
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++)
+        if (rn[i] && rl[i] == 0) s_base[rb[i]] = atomicAdd(&a.bin_cursor[rb[i]], s_cnt[rb[i]]);
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) {
+        if (rn[i]) {
+          uint64_t idx = a.rec_off[rb[i]] + s_base[rb[i]] + rl[i];
+          if (idx < a.rec_off[rb[i] + 1]) a.records[idx] = rec_pack(P0 + rp[i], rn[i], rb[i]);
+          else atomicOr(a.err, (uint32_t)DEV_OVERFLOW);
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++)
+        if (rn[i] && rl[i] == 0) s_cnt[rb[i]] = 0;
+    }
+    __syncthreads();
+    if (!a.tile_counter) break;
+  }
+  if (!EMIT) {
+    my_kmers = warp_sum(my_kmers);
+    if (lane_id() == 0 && my_kmers) atomicAdd(a.n_kmers, my_kmers);
+  }
+}
+
+constexpr int SK_BLOCK = 256;
+
+template <bool EMIT>
+void launch_sk(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
+  if (a.n_tiles == 0) return;
+  size_t smem = 2 * (a.tile + 64) * sizeof(uint64_t) + (EMIT ? 2 * a.num_bins * sizeof(uint32_t) : 0);
+  unsigned grid = persistent_ctas > 0 ? (unsigned)persistent_ctas : (unsigned)a.n_tiles;
+  switch (a.tile) {
+#define CF1_SK_CASE(IT)                                                                              \
+  case SK_BLOCK * IT: {                                                                            \
+    auto kern = superkmer_kernel<SK_BLOCK, IT, EMIT>;                                              \
+    CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    kern<<<grid, SK_BLOCK, smem, s>>>(a);                                                          \
+    break;                                                                                         \
+  }
+    CF1_SK_CASE(4)
+    CF1_SK_CASE(8)
+    CF1_SK_CASE(16)
+#undef CF1_SK_CASE
+    default:
+      throw Error(-1, "super k-mer tile must be 1024, 2048 or 4096");
+  }
+  CF1_LAUNCH_CHECK();
+}
+
+// -------------------------------------------------------------- partition ----
+// One CTA.  Boundaries follow the reference's greedy walk: add the bucket,
+// place a boundary when the running count reaches total/num_bins, carry the
+// excess.  When no bucket exceeds the target the walk never lags, so the
+// boundaries after bucket i number min(floor(C(i)/target), num_bins-1) with C
+// the inclusive prefix sum; otherwise one thread walks the buckets.
+__global__ void __launch_bounds__(1024) partition_kernel(const uint32_t *hist, uint32_t B, uint16_t *lut,
+                                                         uint64_t *rec_off, uint32_t *n_bins_eff) {
+  constexpr int BLK = 1024;
+  constexpr int PER = NUM_BUCKETS / BLK;  // 64
+  __shared__ uint64_t sm[BLK / 32];
+  __shared__ unsigned long long s_bin[MAX_BINS];
+  __shared__ uint32_t s_max;
+  const unsigned tid = threadIdx.x;
+  const uint32_t b0 = tid * PER;
+  uint64_t lsum = 0;
+  uint32_t lmax = 0;
+  for (int i = 0; i < PER; i++) {
+    uint32_t h = hist[b0 + i];
+    lsum += h;
+    lmax = h > lmax ? h : lmax;
+  }
+  if (tid == 0) s_max = 0;
+  for (uint32_t b = tid; b < B; b += BLK) s_bin[b] = 0;
+  __syncthreads();
+  atomicMax(&s_max, lmax);
+  uint64_t total;
+  uint64_t pre = block_exclusive_scan<BLK>(lsum, sm, total);
+  const uint64_t target = total / B;
+  const uint32_t cap = B - 1;
+  if (target == 0 || (uint64_t)s_max <= target) {
+    uint64_t C = pre;
+    uint64_t j_prev = target == 0 ? min((uint64_t)b0, (uint64_t)cap) : min(C / target, (uint64_t)cap);
+    for (int i = 0; i < PER; i++) {
+      uint32_t bucket = b0 + i;
+      lut[bucket] = (uint16_t)j_prev;
+      C += hist[bucket];
+      j_prev = target == 0 ? min((uint64_t)bucket + 1, (uint64_t)cap) : min(C / target, (uint64_t)cap);
+    }
+  } else if (tid == 0) {
+    uint64_t cur = 0, nb = 0;
+    for (uint32_t bucket = 0; bucket < NUM_BUCKETS; bucket++) {
+      lut[bucket] = (uint16_t)nb;
+      cur += hist[bucket];
+      if (cur >= target && nb < cap) {
+        nb++;
+        cur -= target;
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = 0; i < PER; i++) atomicAdd(&s_bin[lut[b0 + i]], (unsigned long long)hist[b0 + i]);
+  __syncthreads();
+  uint64_t carry = 0;
+  for (uint32_t base = 0; base < B; base += BLK) {
+    uint32_t b = base + tid;
+    uint64_t c = b < B ? s_bin[b] : 0;
+    uint64_t tot;
+    uint64_t p = block_exclusive_scan<BLK>(c, sm, tot);
+    if (b < B) rec_off[b] = carry + p;
+    carry += tot;
+  }
+  if (tid == 0) {
+    rec_off[B] = carry;
+    *n_bins_eff = (uint32_t)lut[NUM_BUCKETS - 1] + 1;
+  }
+}
+
+}  // namespace
+
+void launch_pack(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, cudaStream_t s) {
+  uint64_t n_nm = ceil_div(L, 64);
+  if (n_nm == 0) return;
+  pack_kernel<<<(unsigned)ceil_div(n_nm, 256), 256, 0, s>>>(ascii, L, W, NM, n_nm);
+  CF1_LAUNCH_CHECK();
+}
+
+void launch_superkmer_hist(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
+  launch_sk<false>(a, persistent_ctas, s);
+}
+void launch_superkmer_emit(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
+  launch_sk<true>(a, persistent_ctas, s);
+}
+
+void launch_partition(const uint32_t *hist, uint32_t num_bins, uint16_t *lut, uint64_t *rec_off, uint32_t *n_bins_eff,
+                      cudaStream_t s) {
+  partition_kernel<<<1, 1024, 0, s>>>(hist, num_bins, lut, rec_off, n_bins_eff);
+  CF1_LAUNCH_CHECK();
+}
+
+}  // namespace cf1

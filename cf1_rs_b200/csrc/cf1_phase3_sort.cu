@@ -1,0 +1,289 @@
+// Phase 3a on the device: expand every routed super k-mer into canonical
+// k-mers, sort each bin, keep one copy of each key (src/mphf.rs:284-363:
+// decode, canonicalise, radix sort, dedup per bin).
+#include "cf1_device_util.cuh"
+#include "cf1_internal.cuh"
+
+namespace cf1 {
+
+namespace {
+
+constexpr int RS_BLOCK = 256;
+constexpr int RS_ITEMS = 16;
+constexpr uint32_t RS_TILE = RS_BLOCK * RS_ITEMS;  // 4096 keys
+constexpr int RS_BITS = 8;
+constexpr uint32_t RS_DIGITS = 1u << RS_BITS;
+constexpr int RS_NW = RS_BLOCK / 32;
+
+CF1_D uint64_t ceil_div_dev(uint64_t n) { return (n + 31) / 32; }
+
+__global__ void record_len_kernel(const uint64_t *records, uint64_t n, uint32_t *len) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) len[i] = rec_n(records[i]);
+}
+
+// Warp-cooperative expansion: a warp takes 32 records, and its lanes walk the
+// records' k-mers in one flattened index space, so output stores are
+// contiguous whatever the record lengths.
+template <class KeyT>
+__global__ void __launch_bounds__(256) expand_kernel(const uint64_t *records, uint64_t n_rec, const uint64_t *kpre,
+                                                     const uint64_t *W, int k, KeyT *keys, uint64_t n_keys,
+                                                     uint64_t L, uint32_t *queue, uint32_t *err) {
+  const unsigned lane = lane_id();
+  const uint64_t n_chunks = ceil_div_dev(n_rec);
+  uint64_t chunk = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (;;) {
+    if (queue) {
+      uint32_t c = 0;
+      if (lane == 0) c = atomicAdd(queue, 1u);
+      chunk = __shfl_sync(FULL, c, 0);
+    }
+    if (chunk >= n_chunks) break;
+    uint64_t r = chunk * 32 + lane;
+    bool valid = r < n_rec;
+    uint64_t rec = valid ? records[r] : 0;
+    uint32_t n = valid ? rec_n(rec) : 0;
+    uint64_t pos = rec_pos(rec);
+    uint64_t off = valid ? kpre[r] : 0;
+    uint32_t incl = warp_inclusive_scan(n);
+    uint32_t total = __shfl_sync(FULL, incl, 31);
+    uint32_t excl = incl - n;
+    for (uint32_t base = 0; base < total; base += 32) {
+      uint32_t j = base + lane;
+      int lo = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        uint32_t v = __shfl_sync(FULL, incl, lo + step - 1);
+        if (v <= j) lo += step;
+      }
+      uint64_t opos = __shfl_sync(FULL, pos, lo);
+      uint32_t oex = __shfl_sync(FULL, excl, lo);
+      uint64_t ooff = __shfl_sync(FULL, off, lo);
+      if (j < total) {
+        uint32_t t = j - oex;
+        if (ooff + t < n_keys && opos + t + k <= L) {
+          KeyT fw = KOps<KeyT>::extract(W, opos + t, k);
+          KeyT rc = KOps<KeyT>::rc(fw, k);
+          keys[ooff + t] = kmin(fw, rc);
+        } else {
+          atomicOr(err, (uint32_t)DEV_OVERFLOW);
+        }
+      }
+    }
+    if (!queue) break;
+  }
+}
+
+// Per tile digit counts, stored segment-major then digit-major so that one
+// exclusive scan over the array yields every (segment, digit, tile) output
+// position: previous segments' sizes + smaller digits of this segment +
+// earlier tiles of this digit.
+template <class KeyT>
+__global__ void __launch_bounds__(RS_BLOCK) rs_hist_kernel(const KeyT *keys, const uint64_t *seg_off,
+                                                           const uint32_t *tile_off, uint32_t nseg, int shift,
+                                                           uint32_t *H) {
+  __shared__ uint32_t h[RS_DIGITS];
+  const uint32_t t = blockIdx.x;
+  const uint32_t total = tile_off[nseg];
+  if (t >= total) {
+    for (uint32_t d = threadIdx.x; d < RS_DIGITS; d += RS_BLOCK) H[(uint64_t)t * RS_DIGITS + d] = 0;
+    return;
+  }
+  for (uint32_t d = threadIdx.x; d < RS_DIGITS; d += RS_BLOCK) h[d] = 0;
+  __syncthreads();
+  TileSpan sp = tile_span(seg_off, tile_off, nseg, t, RS_TILE);
+  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += RS_BLOCK)
+    atomicAdd(&h[KOps<KeyT>::digit(keys[i], shift, RS_DIGITS - 1)], 1u);
+  __syncthreads();
+  for (uint32_t d = threadIdx.x; d < RS_DIGITS; d += RS_BLOCK)
+    H[(uint64_t)sp.first_tile * RS_DIGITS + (uint64_t)d * sp.ntiles + (t - sp.first_tile)] = h[d];
+}
+
+// Stable scatter of one tile: keys are taken in rounds of RS_BLOCK (round r,
+// thread i holds tile element r*RS_BLOCK + i), ranked inside each warp with
+// match_any, and the per (round, warp, digit) counts are turned into
+// per-digit offsets by one pass per digit over the shared table.
+template <class KeyT>
+__global__ void __launch_bounds__(RS_BLOCK) rs_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
+                                                              const uint32_t *tile_off, uint32_t nseg, int shift,
+                                                              const uint64_t *Hs) {
+  extern __shared__ uint16_t cnt[];  // [RS_ITEMS][RS_NW][RS_DIGITS]
+  __shared__ uint64_t s_base[RS_DIGITS];
+  const uint32_t t = blockIdx.x;
+  if (t >= tile_off[nseg]) return;
+  TileSpan sp = tile_span(seg_off, tile_off, nseg, t, RS_TILE);
+  const unsigned tid = threadIdx.x, warp = tid >> 5;
+  {
+    uint32_t *c32 = reinterpret_cast<uint32_t *>(cnt);
+    for (uint32_t i = tid; i < RS_ITEMS * RS_NW * RS_DIGITS / 2; i += RS_BLOCK) c32[i] = 0;
+  }
+  for (uint32_t d = tid; d < RS_DIGITS; d += RS_BLOCK)
+    s_base[d] = Hs[(uint64_t)sp.first_tile * RS_DIGITS + (uint64_t)d * sp.ntiles + (t - sp.first_tile)];
+  __syncthreads();
+  KeyT key[RS_ITEMS];
+  uint32_t dg[RS_ITEMS];
+  uint32_t wr[RS_ITEMS];
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (int r = 0; r < RS_ITEMS; r++) {
+    uint64_t i = sp.start + (uint64_t)r * RS_BLOCK + tid;
+    bool act = i < sp.end;
+    key[r] = act ? in[i] : KeyT();
+    dg[r] = act ? KOps<KeyT>::digit(key[r], shift, RS_DIGITS - 1) : 0xFFFFFFFFu;
+    unsigned peers = __match_any_sync(FULL, dg[r]);
+    wr[r] = __popc(peers & lt);
+    if (act && wr[r] == 0) cnt[(r * RS_NW + warp) * RS_DIGITS + dg[r]] = (uint16_t)__popc(peers);
+  }
+  __syncthreads();
+  for (uint32_t d = tid; d < RS_DIGITS; d += RS_BLOCK) {
+    uint32_t run = 0;
+    for (int r = 0; r < RS_ITEMS; r++)
+      for (int w = 0; w < RS_NW; w++) {
+        uint16_t &c = cnt[(r * RS_NW + w) * RS_DIGITS + d];
+        uint32_t v = c;
+        c = (uint16_t)run;
+        run += v;
+      }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < RS_ITEMS; r++) {
+    if (dg[r] != 0xFFFFFFFFu) {
+      uint64_t pos = s_base[dg[r]] + cnt[(r * RS_NW + warp) * RS_DIGITS + dg[r]] + wr[r];
+      out[pos] = key[r];
+    }
+  }
+}
+
+// ---- segmented unique ----
+template <class KeyT>
+__global__ void __launch_bounds__(RS_BLOCK) uq_count_kernel(const KeyT *keys, const uint64_t *seg_off,
+                                                            const uint32_t *tile_off, uint32_t nseg,
+                                                            uint32_t *tile_cnt) {
+  __shared__ uint32_t sm[RS_NW];
+  const uint32_t t = blockIdx.x;
+  if (t >= tile_off[nseg]) {
+    if (threadIdx.x == 0) tile_cnt[t] = 0;
+    return;
+  }
+  TileSpan sp = tile_span(seg_off, tile_off, nseg, t, RS_TILE);
+  const uint64_t seg_start = seg_off[sp.seg];
+  uint32_t c = 0;
+  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += RS_BLOCK)
+    c += (i == seg_start || keys[i] != keys[i - 1]) ? 1u : 0u;
+  uint32_t tot = block_sum<RS_BLOCK>(c, sm);
+  if (threadIdx.x == 0) tile_cnt[t] = tot;
+}
+
+template <class KeyT>
+__global__ void __launch_bounds__(RS_BLOCK) uq_write_kernel(const KeyT *keys, const uint64_t *seg_off,
+                                                            const uint32_t *tile_off, uint32_t nseg,
+                                                            const uint64_t *tile_out, KeyT *out) {
+  __shared__ uint32_t sm[RS_NW];
+  const uint32_t t = blockIdx.x;
+  if (t >= tile_off[nseg]) return;
+  TileSpan sp = tile_span(seg_off, tile_off, nseg, t, RS_TILE);
+  const uint64_t seg_start = seg_off[sp.seg];
+  uint64_t i0 = sp.start + (uint64_t)threadIdx.x * RS_ITEMS;
+  uint32_t flags = 0, c = 0;
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; j++) {
+    uint64_t i = i0 + j;
+    bool f = i < sp.end && (i == seg_start || keys[i] != keys[i - 1]);
+    flags |= (uint32_t)f << j;
+    c += f;
+  }
+  uint32_t tot;
+  uint32_t pre = block_exclusive_scan<RS_BLOCK>(c, sm, tot);
+  uint64_t o = tile_out[t] + pre;
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; j++)
+    if ((flags >> j) & 1) out[o++] = keys[i0 + j];
+}
+
+__global__ void seg_out_off_kernel(const uint32_t *tile_off, uint32_t nseg, const uint64_t *tile_out, uint64_t *out_off) {
+  uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b <= nseg) out_off[b] = tile_out[tile_off[b]];
+}
+
+}  // namespace
+
+void record_kmer_prefix(const uint64_t *records, uint64_t n_rec, uint64_t *kpre, DevBuf &lens, DevBuf &scratch,
+                        cudaStream_t s) {
+  uint32_t *len = lens.get<uint32_t>(n_rec + 1);
+  if (n_rec) {
+    record_len_kernel<<<(unsigned)ceil_div(n_rec, 256), 256, 0, s>>>(records, n_rec, len);
+    CF1_LAUNCH_CHECK();
+  }
+  exclusive_scan_u32(len, kpre, n_rec, scratch, s);
+}
+
+template <class KeyT>
+void launch_expand(const uint64_t *records, uint64_t n_rec, const uint64_t *kpre, const uint64_t *W, int k, KeyT *keys,
+                   uint64_t n_keys, uint64_t L, uint32_t *queue, uint32_t *err, int persistent_ctas, cudaStream_t s) {
+  if (n_rec == 0) return;
+  uint64_t warps = ceil_div(n_rec, 32);
+  unsigned grid = persistent_ctas > 0 ? (unsigned)persistent_ctas : (unsigned)ceil_div(warps, 8);
+  expand_kernel<KeyT><<<grid, 256, 0, s>>>(records, n_rec, kpre, W, k, keys, n_keys, L,
+                                           persistent_ctas > 0 ? queue : nullptr, err);
+  CF1_LAUNCH_CHECK();
+}
+
+template <class KeyT>
+void segmented_sort(KeyT *keys, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int key_bits, SortScratch<KeyT> &sc,
+                    cudaStream_t s) {
+  if (n == 0) return;
+  uint32_t ub_tiles = (uint32_t)(ceil_div(n, RS_TILE) + nseg);
+  uint32_t *tile_off = sc.tile_off.template get<uint32_t>(nseg + 1);
+  segment_tiles(seg_off, nseg, RS_TILE, tile_off, s);
+  KeyT *alt = sc.alt.template get<KeyT>(n + 1);
+  uint32_t *H = sc.hist.template get<uint32_t>((uint64_t)ub_tiles * RS_DIGITS);
+  uint64_t *Hs = sc.hscan.template get<uint64_t>((uint64_t)ub_tiles * RS_DIGITS + 1);
+  size_t smem = (size_t)RS_ITEMS * RS_NW * RS_DIGITS * sizeof(uint16_t);
+  CF1_CUDA(cudaFuncSetAttribute(rs_scatter_kernel<KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  KeyT *src = keys, *dst = alt;
+  int passes = (key_bits + RS_BITS - 1) / RS_BITS;
+  for (int p = 0; p < passes; p++) {
+    int shift = p * RS_BITS;
+    rs_hist_kernel<KeyT><<<ub_tiles, RS_BLOCK, 0, s>>>(src, seg_off, tile_off, nseg, shift, H);
+    CF1_LAUNCH_CHECK();
+    exclusive_scan_u32(H, Hs, (uint64_t)ub_tiles * RS_DIGITS, sc.scan_tmp, s);
+    rs_scatter_kernel<KeyT><<<ub_tiles, RS_BLOCK, smem, s>>>(src, dst, seg_off, tile_off, nseg, shift, Hs);
+    CF1_LAUNCH_CHECK();
+    KeyT *t = src; src = dst; dst = t;
+  }
+  if (src != keys) CF1_CUDA(cudaMemcpyAsync(keys, src, n * sizeof(KeyT), cudaMemcpyDeviceToDevice, s));
+}
+
+template <class KeyT>
+void segmented_unique(const KeyT *keys, uint64_t n, const uint64_t *seg_off, uint32_t nseg, KeyT *out, uint64_t *out_off,
+                      SortScratch<KeyT> &sc, cudaStream_t s) {
+  uint32_t ub_tiles = (uint32_t)(ceil_div(n, RS_TILE) + nseg);
+  uint32_t *tile_off = sc.tile_off.template get<uint32_t>(nseg + 1);
+  segment_tiles(seg_off, nseg, RS_TILE, tile_off, s);
+  uint32_t *tc = sc.tile_cnt.template get<uint32_t>(ub_tiles + 1);
+  uint64_t *to = sc.tile_out.template get<uint64_t>(ub_tiles + 2);
+  if (ub_tiles) {
+    uq_count_kernel<KeyT><<<ub_tiles, RS_BLOCK, 0, s>>>(keys, seg_off, tile_off, nseg, tc);
+    CF1_LAUNCH_CHECK();
+  }
+  exclusive_scan_u32(tc, to, ub_tiles, sc.scan_tmp, s);
+  if (ub_tiles) {
+    uq_write_kernel<KeyT><<<ub_tiles, RS_BLOCK, 0, s>>>(keys, seg_off, tile_off, nseg, to, out);
+    CF1_LAUNCH_CHECK();
+  }
+  seg_out_off_kernel<<<(unsigned)ceil_div(nseg + 1, 256), 256, 0, s>>>(tile_off, nseg, to, out_off);
+  CF1_LAUNCH_CHECK();
+}
+
+#define CF1_INST(KT)                                                                                                 \
+  template void launch_expand<KT>(const uint64_t *, uint64_t, const uint64_t *, const uint64_t *, int, KT *,        \
+                                  uint64_t, uint64_t, uint32_t *, uint32_t *, int, cudaStream_t);                   \
+  template void segmented_sort<KT>(KT *, uint64_t, const uint64_t *, uint32_t, int, SortScratch<KT> &, cudaStream_t); \
+  template void segmented_unique<KT>(const KT *, uint64_t, const uint64_t *, uint32_t, KT *, uint64_t *,            \
+                                     SortScratch<KT> &, cudaStream_t);
+CF1_INST(uint64_t)
+CF1_INST(Key2)
+#undef CF1_INST
+
+}  // namespace cf1

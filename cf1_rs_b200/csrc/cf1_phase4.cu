@@ -1,0 +1,205 @@
+// Phase 4 on the device: DFA vertex classification (src/classify.rs:34-601).
+//
+// The reference walks every placeholder-free run of every record and, per
+// k-mer, queries the MPHF and compare-and-swaps the vertex state
+// (src/classify.rs:106-118, 385-518; src/state_vector.rs:47-70).  Here the
+// same per-occurrence step runs over the routed super k-mers, bin after bin,
+// so one bin's MPHF blocks and state words are what the SMs touch at a time.
+// Each occurrence reads its true neighbours from the resident sequence, so the
+// k-mer's (front, back) contribution is exactly the reference's; the state
+// word is updated by a 64-bit atomicCAS loop on the reference layout (12 five-
+// bit states per word, LSB first).  The DFA is a per-side join, so the final
+// words do not depend on the order of the updates.
+#include "cf1_device_util.cuh"
+#include "cf1_internal.cuh"
+#include "cf1_mphf.cuh"
+#include "cf1_phase4.cuh"
+
+namespace cf1 {
+
+namespace {
+
+constexpr int CL_BLOCK = 256;
+
+// Joins contribution c into slot's state (src/state_vector.rs:47-70 CAS loop).
+// Each failed CAS means another thread changed the word; a word changes at
+// most 12 states x 3 steps, so 64 attempts always suffice.
+CF1_D void state_join_cas(unsigned long long *states, uint64_t slot, uint32_t c, uint32_t *err, uint32_t &retries) {
+  uint64_t wi = slot / 12;
+  uint32_t sh = (uint32_t)(slot - wi * 12) * 5;
+  unsigned long long *p = states + wi;
+  unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(p);
+  for (int it = 0; it < 64; it++) {
+    uint32_t cur = (uint32_t)(old >> sh) & 31u;
+    uint32_t nv = join_state(cur, c);
+    if (nv == cur) return;
+    unsigned long long nw = (old & ~(31ull << sh)) | ((unsigned long long)nv << sh);
+    unsigned long long prev = atomicCAS(p, old, nw);
+    if (prev == old) return;
+    old = prev;
+    retries++;
+  }
+  atomicOr(err, (uint32_t)DEV_CAS_LIMIT);
+}
+
+template <class KeyT>
+__global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a) {
+  const unsigned lane = lane_id();
+  const uint64_t n_chunks = (a.n_rec + 31) / 32;
+  uint64_t chunk = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t retries = 0;
+  const int k = a.k;
+  for (;;) {
+    if (a.queue) {
+      uint32_t c = 0;
+      if (lane == 0) c = atomicAdd(a.queue, 1u);
+      chunk = __shfl_sync(FULL, c, 0);
+    }
+    if (chunk >= n_chunks) break;
+    uint64_t r = chunk * 32 + lane;
+    bool valid = r < a.n_rec;
+    uint64_t rec = valid ? a.records[r] : 0;
+    uint32_t n = valid ? rec_n(rec) : 0;
+    uint32_t incl = warp_inclusive_scan(n);
+    uint32_t total = __shfl_sync(FULL, incl, 31);
+    uint32_t excl = incl - n;
+    for (uint32_t base = 0; base < total; base += 32) {
+      uint32_t j = base + lane;
+      int lo = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        uint32_t v = __shfl_sync(FULL, incl, lo + step - 1);
+        if (v <= j) lo += step;
+      }
+      uint64_t orec = __shfl_sync(FULL, rec, lo);
+      uint32_t oex = __shfl_sync(FULL, excl, lo);
+      uint64_t p = rec_pos(orec) + (j - oex);
+      if (j < total && p + k > a.L) {
+        atomicOr(a.err, (uint32_t)DEV_OVERFLOW);
+      } else if (j < total) {
+        uint32_t bin = rec_bin(orec);
+        KeyT fw = KOps<KeyT>::extract(a.W, p, k);
+        KeyT rc = KOps<KeyT>::rc(fw, k);
+        bool hp = p > 0 && !is_n(a.NM, p - 1);
+        bool hn = p + k < a.L && !is_n(a.NM, p + k);
+        uint32_t pb = hp ? base_at(a.W, p - 1) : 0;
+        uint32_t nb = hn ? base_at(a.W, p + k) : 0;
+        uint32_t c = contribution(fw, rc, hp, pb, hn, nb, k);
+        uint64_t slot = mphf_slot(a.mphf, bin, kmin(fw, rc));
+        if (slot == SLOT_NONE) atomicOr(a.err, (uint32_t)DEV_MPHF_MISS);
+        else state_join_cas(a.states, slot, c, a.err, retries);
+      }
+    }
+    if (!a.queue) break;
+  }
+  retries = warp_sum(retries);
+  if (lane == 0 && retries) atomicAdd(a.cas_retries, (unsigned long long)retries);
+}
+
+template <class KeyT>
+CF1_D KeyT load_key(const uint64_t *w, uint64_t i);
+template <>
+CF1_D uint64_t load_key<uint64_t>(const uint64_t *w, uint64_t i) { return w[i]; }
+template <>
+CF1_D Key2 load_key<Key2>(const uint64_t *w, uint64_t i) { return Key2{w[2 * i], w[2 * i + 1]}; }
+
+template <class KeyT>
+CF1_D void store_key(uint64_t *w, uint64_t i, const KeyT &k);
+template <>
+CF1_D void store_key<uint64_t>(uint64_t *w, uint64_t i, const uint64_t &k) { w[i] = k; }
+template <>
+CF1_D void store_key<Key2>(uint64_t *w, uint64_t i, const Key2 &k) {
+  w[2 * i] = k.lo;
+  w[2 * i + 1] = k.hi;
+}
+
+template <class KeyT>
+__global__ void dump_kernel(MphfView<KeyT> m, uint32_t nbins, uint64_t n, const unsigned long long *states,
+                            uint64_t *keys_out, uint8_t *states_out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t bin = upper_segment(m.dist_off, nbins, i);
+  KeyT key = m.keys[i];
+  uint64_t slot = mphf_slot(m, bin, key);
+  uint8_t st = 0xFF;
+  if (slot != SLOT_NONE && slot < n) st = (uint8_t)((states[slot / 12] >> (5 * (slot % 12))) & 31);
+  store_key<KeyT>(keys_out, i, key);
+  states_out[i] = st;
+}
+
+template <class KeyT>
+__global__ void verify_mark_kernel(MphfView<KeyT> m, uint32_t nbins, uint64_t n, uint32_t *seen, uint32_t *err) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t bin = upper_segment(m.dist_off, nbins, i);
+  uint64_t slot = mphf_slot(m, bin, m.keys[i]);
+  if (slot == SLOT_NONE || slot >= n) atomicOr(err, (uint32_t)DEV_BIJECTION);
+  else atomicAdd(&seen[slot], 1u);
+}
+
+__global__ void verify_check_kernel(const uint32_t *seen, uint64_t n, uint32_t *err) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && seen[i] != 1u) atomicOr(err, (uint32_t)DEV_BIJECTION);
+}
+
+template <class KeyT>
+__global__ void query_kernel(MphfView<KeyT> m, const uint16_t *lut, int k, int mlen, const uint64_t *in, uint64_t n,
+                             uint64_t *out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  KeyT key = load_key<KeyT>(in, i);
+  uint64_t mz = kmer_minimizer(key, k, mlen);
+  uint32_t bin = lut[mix_bucket((uint32_t)mz)];
+  uint64_t slot = mphf_slot(m, bin, key);
+  out[i] = slot == SLOT_NONE ? 0 : slot;  // absent keys: unwrap_or(0), src/mphf.rs:269
+}
+
+}  // namespace
+
+template <class KeyT>
+void launch_classify(const ClassifyArgs<KeyT> &a, int persistent_ctas, cudaStream_t s) {
+  if (a.n_rec == 0) return;
+  uint64_t warps = (a.n_rec + 31) / 32;
+  unsigned grid = persistent_ctas > 0 ? (unsigned)persistent_ctas : (unsigned)ceil_div(warps, CL_BLOCK / 32);
+  classify_kernel<KeyT><<<grid, CL_BLOCK, 0, s>>>(a);
+  CF1_LAUNCH_CHECK();
+}
+
+template <class KeyT>
+void launch_dump(const MphfView<KeyT> &m, uint32_t nbins, uint64_t n, const unsigned long long *states, uint64_t *keys_out,
+                 uint8_t *states_out, cudaStream_t s) {
+  if (!n) return;
+  dump_kernel<KeyT><<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(m, nbins, n, states, keys_out, states_out);
+  CF1_LAUNCH_CHECK();
+}
+
+template <class KeyT>
+void launch_verify(const MphfView<KeyT> &m, uint32_t nbins, uint64_t n, uint32_t *seen, uint32_t *err, cudaStream_t s) {
+  if (!n) return;
+  CF1_CUDA(cudaMemsetAsync(seen, 0, n * 4, s));
+  verify_mark_kernel<KeyT><<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(m, nbins, n, seen, err);
+  CF1_LAUNCH_CHECK();
+  verify_check_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(seen, n, err);
+  CF1_LAUNCH_CHECK();
+}
+
+template <class KeyT>
+void launch_query(const MphfView<KeyT> &m, const uint16_t *lut, int k, int mlen, const uint64_t *in, uint64_t n,
+                  uint64_t *out, cudaStream_t s) {
+  if (!n) return;
+  query_kernel<KeyT><<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(m, lut, k, mlen, in, n, out);
+  CF1_LAUNCH_CHECK();
+}
+
+#define CF1_INST(KT)                                                                                             \
+  template void launch_classify<KT>(const ClassifyArgs<KT> &, int, cudaStream_t);                               \
+  template void launch_dump<KT>(const MphfView<KT> &, uint32_t, uint64_t, const unsigned long long *, uint64_t *, \
+                                uint8_t *, cudaStream_t);                                                       \
+  template void launch_verify<KT>(const MphfView<KT> &, uint32_t, uint64_t, uint32_t *, uint32_t *, cudaStream_t); \
+  template void launch_query<KT>(const MphfView<KT> &, const uint16_t *, int, int, const uint64_t *, uint64_t,   \
+                                 uint64_t *, cudaStream_t);
+CF1_INST(uint64_t)
+CF1_INST(Key2)
+#undef CF1_INST
+
+}  // namespace cf1

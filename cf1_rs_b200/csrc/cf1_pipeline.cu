@@ -1,0 +1,376 @@
+// Orchestration of phases 1-4 (src/pipeline.rs:66-105) and the C ABI.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+#include "cf1_context.cuh"
+#include "cf1_device_util.cuh"
+#include "cf1_mphf.cuh"
+#include "cf1_phase4.cuh"
+#include "cf1_pipeline.cuh"
+
+using cf1::DevBuf;
+using cf1::Error;
+using cf1::Key2;
+
+namespace cf1 {
+
+void PinnedBuf::reserve(size_t bytes, size_t keep) {
+  if (bytes <= cap) return;
+  size_t ncap = std::max(bytes, cap + cap / 2);
+  uint8_t *np = nullptr;
+  CF1_CUDA(cudaHostAlloc((void **)&np, ncap, cudaHostAllocDefault));
+  if (p) {
+    if (keep) std::memcpy(np, p, keep);
+    cudaFreeHost(p);
+  }
+  p = np;
+  cap = ncap;
+}
+
+namespace {
+
+// Small device counters of one run.
+struct Small {
+  unsigned long long n_kmers;
+  unsigned long long cas_retries;
+  uint32_t err;
+  uint32_t n_bins_eff;
+  uint32_t queues[8];
+};
+
+__global__ void seg_gather_kernel(const uint64_t *kpre, const uint64_t *rec_off, uint32_t nbins, uint64_t *seg) {
+  uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b <= nbins) seg[b] = kpre[rec_off[b]];
+}
+
+template <class KeyT>
+Backend<KeyT> &backend(cf1gpu_ctx *c) {
+  return ctx_backend<KeyT>(c);
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0;
+  CF1_CUDA(cudaEventElapsedTime(&ms, a, b));
+  return ms;
+}
+
+void check_device_errors(uint32_t err) {
+  if (err & DEV_CAS_LIMIT) throw Error(CF1GPU_ERR_DEVICE_TIMEOUT, "phase 4: a state CAS loop passed its bound");
+  if (err & DEV_WAIT_LIMIT) throw Error(CF1GPU_ERR_DEVICE_TIMEOUT, "a bounded device wait gave up");
+  if (err & DEV_OVERFLOW) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "a device buffer bound was hit");
+  if (err & DEV_MPHF_MISS) throw Error(CF1GPU_ERR_BIJECTION, "phase 4: a k-mer was not found by the MPHF");
+  if (err & DEV_BIJECTION) throw Error(CF1GPU_ERR_BIJECTION, "MPHF is not a bijection onto [0, n)");
+}
+
+template <class KeyT>
+MphfView<KeyT> make_view(cf1gpu_ctx *c) {
+  Backend<KeyT> &be = backend<KeyT>(c);
+  MphfView<KeyT> v;
+  v.keys = c->d_dist.as<const KeyT>();
+  v.dist_off = c->d_dist_off.as<const uint64_t>();
+  v.bb = be.bb.view();
+  v.learned = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED;
+  v.li = be.li.view(c->k);
+  return v;
+}
+
+template <class KeyT>
+void run_impl(cf1gpu_ctx *c) {
+  cudaStream_t s = c->stream;
+  Backend<KeyT> &be = backend<KeyT>(c);
+  const uint64_t L = c->L;
+  const int k = c->k;
+  const uint32_t B = c->opts.num_bins;
+  const bool batched = c->opts.batched != 0;
+  c->nbins = B;
+  const uint64_t launches0 = g_launches.load();
+  Small *sm = c->d_small.get<Small>(1);
+  CF1_CUDA(cudaMemsetAsync(sm, 0, sizeof(Small), s));
+  CF1_CUDA(cudaEventRecord(c->ev[0], s));
+
+  // ---- phase 1: pack, minimizer histogram, partition
+  uint64_t n_nm = ceil_div(L, 64);
+  uint64_t *W = c->d_W.get<uint64_t>(2 * n_nm + 4);
+  uint64_t *NM = c->d_NM.get<uint64_t>(n_nm + 2);
+  CF1_CUDA(cudaMemsetAsync(W + 2 * n_nm, 0, 4 * sizeof(uint64_t), s));
+  CF1_CUDA(cudaMemsetAsync(NM + n_nm, 0xFF, 2 * sizeof(uint64_t), s));
+  launch_pack(c->d_ascii.as<uint8_t>(), L, W, NM, s);
+  uint32_t *hist = c->d_hist.get<uint32_t>(NUM_BUCKETS);
+  CF1_CUDA(cudaMemsetAsync(hist, 0, NUM_BUCKETS * sizeof(uint32_t), s));
+  SuperkmerArgs a{};
+  a.W = W;
+  a.NM = NM;
+  a.L = L;
+  a.k = k;
+  a.m = c->m;
+  a.w = c->w;
+  a.tile = c->tune.sk_tile;
+  a.n_tiles = L >= (uint64_t)k ? ceil_div(L - k + 1, a.tile) : 0;
+  a.hist = hist;
+  a.n_kmers = &sm->n_kmers;
+  a.err = &sm->err;
+  int pctas = batched ? (c->tune.persistent_ctas > 0 ? c->tune.persistent_ctas : 4 * c->num_sms) : 0;
+  a.tile_counter = batched ? &sm->queues[0] : nullptr;
+  launch_superkmer_hist(a, pctas, s);
+  uint16_t *lut = c->d_lut.get<uint16_t>(NUM_BUCKETS);
+  uint64_t *rec_off = c->d_rec_off.get<uint64_t>(B + 1);
+  launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
+  Small hs;
+  CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaMemcpyAsync(&c->n_super, rec_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  c->n_occ = hs.n_kmers;
+  c->n_bins_eff = hs.n_bins_eff;
+  CF1_CUDA(cudaEventRecord(c->ev[1], s));
+
+  // ---- phase 2: route super k-mers into bins
+  const uint64_t NS = c->n_super;
+  uint64_t *records = c->d_records.get<uint64_t>(NS + 1);
+  CF1_CUDA(cudaMemsetAsync(records, 0, (NS + 1) * sizeof(uint64_t), s));
+  uint32_t *cursor = c->d_cursor.get<uint32_t>(B);
+  CF1_CUDA(cudaMemsetAsync(cursor, 0, B * sizeof(uint32_t), s));
+  a.lut = lut;
+  a.num_bins = B;
+  a.rec_off = rec_off;
+  a.bin_cursor = cursor;
+  a.records = records;
+  a.tile_counter = batched ? &sm->queues[1] : nullptr;
+  launch_superkmer_emit(a, pctas, s);
+  uint64_t *kpre = c->d_kpre.get<uint64_t>(NS + 1);
+  record_kmer_prefix(records, NS, kpre, c->d_lens, c->d_scan, s);
+  CF1_CUDA(cudaEventRecord(c->ev[2], s));
+
+  // ---- phase 3a: expand, sort per bin, unique
+  const uint64_t NO = c->n_occ;
+  KeyT *keys = c->d_keys.get<KeyT>(NO + 1);
+  launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[2] : nullptr, &sm->err, pctas, s);
+  uint64_t *seg = c->d_seg.get<uint64_t>(B + 1);
+  seg_gather_kernel<<<(unsigned)ceil_div(B + 1, 256), 256, 0, s>>>(kpre, rec_off, B, seg);
+  CF1_LAUNCH_CHECK();
+  segmented_sort<KeyT>(keys, NO, seg, B, 2 * k, be.sort, s);
+  KeyT *dist = c->d_dist.get<KeyT>(NO + 1);
+  uint64_t *dist_off = c->d_dist_off.get<uint64_t>(B + 1);
+  segmented_unique<KeyT>(keys, NO, seg, B, dist, dist_off, be.sort, s);
+  CF1_CUDA(cudaMemcpyAsync(&c->n_distinct, dist_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  CF1_CUDA(cudaEventRecord(c->ev[3], s));
+
+  // ---- phase 3b: MPHF
+  // the sort's buffers (NO keys each) are free now: BBHash levels use them
+  KeyT *ws1 = be.sort.alt.template as<KeyT>();
+  if (c->opts.mphf_mode == CF1GPU_MPHF_LEARNED) {
+    be.li.build(dist, dist_off, B, k, c->learned, s);
+    be.bb.build(dist, dist_off, B, be.li.fallback_sel(), s, keys, ws1, NO + 1);
+  } else {
+    be.bb.build(dist, dist_off, B, nullptr, s, keys, ws1, NO + 1);
+  }
+  CF1_CUDA(cudaEventRecord(c->ev[4], s));
+
+  // ---- phase 4: classification
+  const uint64_t nwords = ceil_div(c->n_distinct, 12);
+  unsigned long long *states = c->d_states.get<unsigned long long>(nwords + 1);
+  CF1_CUDA(cudaMemsetAsync(states, 0, (nwords + 1) * sizeof(unsigned long long), s));
+  ClassifyArgs<KeyT> ca;
+  ca.records = records;
+  ca.n_rec = NS;
+  ca.W = W;
+  ca.NM = NM;
+  ca.L = L;
+  ca.k = k;
+  ca.mphf = make_view<KeyT>(c);
+  ca.states = states;
+  ca.queue = batched ? &sm->queues[3] : nullptr;
+  ca.err = &sm->err;
+  ca.cas_retries = &sm->cas_retries;
+  CF1_CUDA(cudaEventRecord(c->ev[5], s));
+  launch_classify<KeyT>(ca, batched ? 8 * c->num_sms : 0, s);
+  CF1_CUDA(cudaEventRecord(c->ev[6], s));
+  CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  check_device_errors(hs.err);
+  c->cas_retries = hs.cas_retries;
+
+  cf1gpu_stats &st = c->stats;
+  double h2d = st.ms_h2d;
+  std::memset(&st, 0, sizeof(st));
+  st.ms_h2d = h2d;
+  st.n_bases = c->n_bases;
+  st.n_records = c->n_records;
+  st.n_short = c->short_seqs.size();
+  st.n_superkmers = NS;
+  st.n_kmer_occurrences = NO;
+  st.n_distinct = c->n_distinct;
+  st.n_bins = c->n_bins_eff;
+  st.n_state_words = nwords;
+  st.bbhash_levels = be.bb.levels;
+  st.mphf_bytes = be.bb.bytes + (c->opts.mphf_mode == CF1GPU_MPHF_LEARNED ? be.li.stats.bytes : 0);
+  st.learned_bins = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED ? be.li.stats.learned_bins : 0;
+  st.fallback_bins = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED ? be.li.stats.fallback_bins : 0;
+  st.learned_max_err = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED ? be.li.stats.max_err : 0;
+  st.classify_cas_retries = c->cas_retries;
+  st.n_kernel_launches = g_launches.load() - launches0;
+  st.ms_phase1 = elapsed(c->ev[0], c->ev[1]);
+  st.ms_phase2 = elapsed(c->ev[1], c->ev[2]);
+  st.ms_phase3_sort = elapsed(c->ev[2], c->ev[3]);
+  st.ms_phase3_mphf = elapsed(c->ev[3], c->ev[4]);
+  st.ms_phase4 = elapsed(c->ev[4], c->ev[6]);
+  st.ms_classify_kernel = elapsed(c->ev[5], c->ev[6]);
+  st.ms_total = elapsed(c->ev[0], c->ev[6]);
+}
+
+template <class KeyT>
+void dump_impl(cf1gpu_ctx *c, uint64_t *keys, uint8_t *states) {
+  cudaStream_t s = c->stream;
+  uint64_t n = c->n_distinct;
+  uint64_t *dk = c->d_qout.get<uint64_t>(n * cf1::KOps<KeyT>::WORDS + 1);
+  uint8_t *ds = c->d_qin.get<uint8_t>(n + 1);
+  launch_dump<KeyT>(make_view<KeyT>(c), c->nbins, n, c->d_states.as<const unsigned long long>(), dk, ds, s);
+  CF1_CUDA(cudaMemcpyAsync(keys, dk, n * cf1::KOps<KeyT>::WORDS * 8, cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaMemcpyAsync(states, ds, n, cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class KeyT>
+void verify_impl(cf1gpu_ctx *c) {
+  cudaStream_t s = c->stream;
+  uint64_t n = c->n_distinct;
+  Small *sm = c->d_small.get<Small>(1);
+  CF1_CUDA(cudaMemsetAsync(&sm->err, 0, sizeof(uint32_t), s));
+  uint32_t *seen = c->d_seen.get<uint32_t>(n + 1);
+  launch_verify<KeyT>(make_view<KeyT>(c), c->nbins, n, seen, &sm->err, s);
+  uint32_t err = 0;
+  CF1_CUDA(cudaMemcpyAsync(&err, &sm->err, 4, cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  if (err) throw Error(CF1GPU_ERR_BIJECTION, "MPHF is not a bijection onto [0, total_kmers)");
+}
+
+template <class KeyT>
+void query_impl(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots) {
+  cudaStream_t s = c->stream;
+  constexpr int KW = cf1::KOps<KeyT>::WORDS;
+  uint64_t *din = c->d_qin.get<uint64_t>(n * KW + 1);
+  uint64_t *dout = c->d_qout.get<uint64_t>(n + 1);
+  CF1_CUDA(cudaMemcpyAsync(din, keys, n * KW * 8, cudaMemcpyHostToDevice, s));
+  launch_query<KeyT>(make_view<KeyT>(c), c->d_lut.as<const uint16_t>(), c->k, c->m, din, n, dout, s);
+  CF1_CUDA(cudaMemcpyAsync(slots, dout, n * 8, cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+}
+
+void append_record(cf1gpu_ctx *c, const uint8_t *seq, size_t len) {
+  c->host.reserve(c->L + len + 1, c->L);
+  if (len) std::memcpy(c->host.p + c->L, seq, len);
+  c->host.p[c->L + len] = 'N';
+  c->L += len + 1;
+}
+
+std::string first_token(const char *name, size_t n) {
+  size_t i = 0;
+  while (i < n && (name[i] == ' ' || name[i] == '\t' || name[i] == '\n' || name[i] == '\r')) i++;
+  size_t j = i;
+  while (j < n && !(name[j] == ' ' || name[j] == '\t' || name[j] == '\n' || name[j] == '\r')) j++;
+  return std::string(name + i, j - i);
+}
+
+}  // namespace
+
+// ---- entry points used by the C ABI (and by the C++ host mirror) ----
+void run_resident(cf1gpu_ctx *c) {
+  if (!c->uploaded) throw Error(CF1GPU_ERR_STATE, "no input on the device: call cf1gpu_upload first");
+  if (c->wide) run_impl<Key2>(c);
+  else run_impl<uint64_t>(c);
+  c->ran = true;
+}
+
+void upload(cf1gpu_ctx *c) {
+  cudaStream_t s = c->stream;
+  uint8_t *d = c->d_ascii.get<uint8_t>(c->L + 16);
+  CF1_CUDA(cudaEventRecord(c->ev[8], s));
+  if (c->L) CF1_CUDA(cudaMemcpyAsync(d, c->host.p, c->L, cudaMemcpyHostToDevice, s));
+  CF1_CUDA(cudaEventRecord(c->ev[9], s));
+  CF1_CUDA(cudaEventSynchronize(c->ev[9]));
+  float ms = 0;
+  CF1_CUDA(cudaEventElapsedTime(&ms, c->ev[8], c->ev[9]));
+  c->stats.ms_h2d = ms;
+  c->uploaded = true;
+}
+
+void add_record(cf1gpu_ctx *c, const char *name, size_t name_len, const uint8_t *seq, size_t len) {
+  c->n_records++;
+  c->n_bases += len;
+  c->uploaded = false;
+  if (len < (size_t)c->k) {  // src/classify.rs:550-561
+    if (c->opts.track_short_seqs) c->short_seqs.emplace_back(name ? first_token(name, name_len) : std::string(), len);
+    return;
+  }
+  append_record(c, seq, len);
+}
+
+void add_records(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, size_t n) {
+  // Records of k bases or more are copied into the pinned buffer by several
+  // threads; shorter ones only update the short-sequence list.
+  std::vector<uint64_t> dst(n + 1);
+  uint64_t pos = c->L;
+  for (size_t i = 0; i < n; i++) {
+    uint64_t len = off[i + 1] - off[i];
+    dst[i] = pos;
+    c->n_records++;
+    c->n_bases += len;
+    if (len < (uint64_t)c->k) {
+      if (c->opts.track_short_seqs) c->short_seqs.emplace_back(std::string(), len);
+      dst[i] = ~0ull;
+      continue;
+    }
+    pos += len + 1;
+  }
+  c->host.reserve(pos + 1, c->L);
+  uint8_t *h = c->host.p;
+  uint64_t total = pos - c->L;
+  unsigned nt = total > (64ull << 20) ? std::max(1u, std::min(16u, std::thread::hardware_concurrency())) : 1;
+  auto work = [&](unsigned t) {
+    // record i goes to thread t when its destination start falls in t's share
+    uint64_t lo = c->L + total * t / nt, hi = c->L + total * (t + 1) / nt;
+    for (size_t i = 0; i < n; i++) {
+      if (dst[i] == ~0ull) continue;
+      uint64_t len = off[i + 1] - off[i];
+      uint64_t a = std::max(dst[i], lo), b = std::min(dst[i] + len + 1, hi);
+      if (a >= b) continue;
+      uint64_t e = std::min(b, dst[i] + len);
+      if (a < e) std::memcpy(h + a, seqs + off[i] + (a - dst[i]), e - a);
+      if (b == dst[i] + len + 1) h[dst[i] + len] = 'N';
+    }
+  };
+  if (nt == 1) work(0);
+  else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; t++) th.emplace_back(work, t);
+    for (auto &x : th) x.join();
+  }
+  c->L = pos;
+  c->uploaded = false;
+}
+
+void dump_states(cf1gpu_ctx *c, uint64_t *keys, uint8_t *states) {
+  if (c->wide) dump_impl<Key2>(c, keys, states);
+  else dump_impl<uint64_t>(c, keys, states);
+}
+
+void verify_bijection(cf1gpu_ctx *c) {
+  if (c->wide) verify_impl<Key2>(c);
+  else verify_impl<uint64_t>(c);
+}
+
+void query(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots) {
+  if (c->wide) query_impl<Key2>(c, keys, n, slots);
+  else query_impl<uint64_t>(c, keys, n, slots);
+}
+
+void learned_summary(const cf1gpu_ctx *c, double out3[3]) {
+  const LearnedStats &ls = c->wide ? c->b128.li.stats : c->b64.li.stats;
+  out3[0] = ls.mean_err;
+  out3[1] = ls.mean_window;
+  out3[2] = ls.train_loss;
+}
+
+}  // namespace cf1

@@ -1,0 +1,186 @@
+/*
+ * cf1gpu.h -- C ABI of the B200 (sm_100a) k-mer state path of cf1-rs
+ * (phases 1-4: minimizer histogram, super k-mer routing into bins, per-bin
+ * dedup + minimal perfect hash, DFA vertex classification into the packed
+ * 5-bit state vector).
+ *
+ * All paths cited below are files of the cf1-rs reference crate.
+ *
+ * The seam this replaces is `run_pipeline::<K>` (src/pipeline.rs:66-118),
+ * lines 76-105: count_minimizer_histogram (src/minimizer.rs:27-98),
+ * partition_minimizers (src/minimizer.rs:116-144), route_superkmers
+ * (src/superkmer.rs:21-101), Mphf::<K>::build (src/mphf.rs:32-43),
+ * AtomicStateVector::new (src/state_vector.rs:17-26) and classify_vertices
+ * (src/classify.rs:524-601).  What phase 5 (src/output.rs) needs afterwards is
+ * (1) Mphf::hash / bucket_id / total_kmers (src/mphf.rs:268-280), served here
+ * by cf1gpu_query on the device and by cf1gpu_export_mphf +
+ * cf1gpu_mphf_host_query on the host; (2) the AtomicStateVector words in the
+ * reference bit layout (12 five-bit states per u64, LSB first,
+ * src/state_vector.rs:36-70), served by cf1gpu_copy_states; (3) the
+ * short-sequence list (src/classify.rs:550-561), served by
+ * cf1gpu_short_seq_count / cf1gpu_short_seq.
+ *
+ * Ownership: the context owns all device memory and pinned staging buffers.
+ * Output buffers are caller-allocated.  Input bytes are copied during the
+ * call, so the caller may free them on return.  Keys of k > 32 pass as
+ * (lo, hi) u64 pairs, the order of KmerBits::word(.., 0/1)
+ * (src/kmer.rs:426-432); keys of k <= 32 pass as one u64.
+ *
+ * Errors: every int-returning call returns CF1GPU_OK (0) or a negative
+ * status; cf1gpu_last_error gives the message.  No call aborts the process
+ * or traps the device.  A context is not thread-safe for mutation; after a
+ * run, cf1gpu_query / cf1gpu_copy_states may be called from one thread at a
+ * time, and exported MPHF images are immutable and may be queried from any
+ * number of host threads.
+ */
+#ifndef CF1GPU_H
+#define CF1GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CF1GPU_OK 0
+#define CF1GPU_ERR_INVALID_ARG (-1)   /* bad k, bins, null pointer, size mismatch */
+#define CF1GPU_ERR_OOM (-2)           /* device or pinned host allocation failed */
+#define CF1GPU_ERR_CUDA (-3)          /* a CUDA runtime call failed */
+#define CF1GPU_ERR_DEVICE_TIMEOUT (-4) /* a bounded device wait gave up */
+#define CF1GPU_ERR_BIJECTION (-5)     /* MPHF is not a bijection onto [0, n) */
+#define CF1GPU_ERR_QUEUE_OVERRUN (-6) /* a device work queue or buffer overflowed */
+#define CF1GPU_ERR_STATE (-7)         /* call made in the wrong order */
+#define CF1GPU_ERR_IO (-8)            /* input file could not be read */
+
+/* MPHF backends (the reference uses ph::fmph, src/mphf.rs:16). */
+#define CF1GPU_MPHF_BBHASH 0   /* per-bin GPU BBHash (gamma 2) */
+#define CF1GPU_MPHF_LEARNED 1  /* per-bin learned index, BBHash fallback */
+
+typedef struct cf1gpu_ctx cf1gpu_ctx;
+
+typedef struct cf1gpu_opts {
+  uint32_t k;                 /* odd, 1..63 (src/params.rs:167-170) */
+  uint32_t num_bins;          /* --num-bins (src/params.rs:58-59), 1..4096 */
+  int32_t device;             /* CUDA device ordinal */
+  uint32_t mphf_mode;         /* CF1GPU_MPHF_* */
+  uint32_t batched;           /* 1: persistent queue kernels + CUDA graph replay */
+  uint32_t track_short_seqs;  /* --track-short-seqs (src/params.rs:45-47) */
+  const char *tuner_cache_path; /* autotuner cache file, NULL = built-in defaults */
+  uint32_t learned_max_err;   /* learned index: per-bin error bound above which the bin falls back to BBHash (0 = default 1024) */
+  int32_t learned_train_steps; /* learned index root training steps: 0 = default (300), < 0 = no training (identity root) */
+  uint32_t learned_leaf_size; /* learned index target keys per leaf (0 = default 32) */
+  uint32_t sk_tile;           /* k-mer positions per minimizer tile: 1024, 2048 or 4096 (0 = tuner / default) */
+  uint32_t reserved[4];
+} cf1gpu_opts;
+
+typedef struct cf1gpu_stats {
+  uint64_t n_bases;            /* bases added (all records) */
+  uint64_t n_records;          /* records added */
+  uint64_t n_short;            /* records shorter than k */
+  uint64_t n_superkmers;       /* phase-1/2 super k-mers */
+  uint64_t n_kmer_occurrences; /* valid k-mer windows */
+  uint64_t n_distinct;         /* distinct canonical k-mers (Mphf::total_kmers) */
+  uint64_t n_bins;             /* bins after partitioning (src/minimizer.rs:137-141) */
+  uint64_t n_state_words;      /* ceil(n_distinct / 12) */
+  uint64_t mphf_bytes;         /* device bytes of the MPHF */
+  uint64_t bbhash_levels;      /* deepest BBHash level used */
+  uint64_t learned_bins;       /* bins served by the learned index */
+  uint64_t fallback_bins;      /* bins served by BBHash in learned mode */
+  uint64_t learned_max_err;    /* largest leaf error bound among learned bins */
+  uint64_t classify_cas_retries; /* failed CAS attempts in phase 4 */
+  uint64_t n_kernel_launches;  /* kernels this library launched during the last run */
+  uint64_t reserved_u[5];
+  double ms_h2d;               /* host->device copy of the input */
+  double ms_phase1;            /* pack + minimizer histogram + partition */
+  double ms_phase2;            /* super k-mer routing */
+  double ms_phase3_sort;       /* k-mer expansion + per-bin sort + unique */
+  double ms_phase3_mphf;       /* MPHF construction (+ bijection judge) */
+  double ms_phase4;            /* classification */
+  double ms_total;             /* device time of phases 1-4 (excludes h2d) */
+  double ms_classify_kernel;   /* the classification kernel alone */
+  double reserved_d[4];
+} cf1gpu_stats;
+
+/* Fills defaults: k 31, 128 bins, device 0, BBHash, not batched. */
+void cf1gpu_default_opts(cf1gpu_opts *opts);
+
+/* Params::from_resolved checks (src/params.rs:154-197) + device set-up. */
+int cf1gpu_create(const cf1gpu_opts *opts, cf1gpu_ctx **out);
+
+/* One input record in input order (the host parses FASTA/FASTQ, as needletail
+ * does at src/classify.rs:541-546).  `name` may be NULL; its first
+ * whitespace-delimited token is kept for short-sequence tracking. */
+int cf1gpu_add_record(cf1gpu_ctx *ctx, const char *name, size_t name_len, const uint8_t *seq, size_t len);
+
+/* Many records at once: record i is seqs[offsets[i] .. offsets[i+1]). */
+int cf1gpu_add_records(cf1gpu_ctx *ctx, const uint8_t *seqs, const uint64_t *offsets, size_t n_records);
+
+/* Reads every record of a FASTA/FASTQ file (plain or gzip). */
+int cf1gpu_add_fasta(cf1gpu_ctx *ctx, const char *path);
+
+/* Drops all added records and results (keeps device buffers for reuse). */
+int cf1gpu_reset_input(cf1gpu_ctx *ctx);
+
+/* Copies the added records to the device (part of cf1gpu_run_phases_1_4). */
+int cf1gpu_upload(cf1gpu_ctx *ctx);
+
+/* Phases 1-4 over the records already on the device (no host copies). */
+int cf1gpu_run_resident(cf1gpu_ctx *ctx);
+
+/* cf1gpu_upload + cf1gpu_run_resident: pipeline.rs:76-105 in one call. */
+int cf1gpu_run_phases_1_4(cf1gpu_ctx *ctx);
+
+int cf1gpu_get_stats(const cf1gpu_ctx *ctx, cf1gpu_stats *out);
+
+/* Mphf::total_kmers (src/mphf.rs:278-280). */
+uint64_t cf1gpu_total_kmers(const cf1gpu_ctx *ctx);
+
+/* The state vector words (src/state_vector.rs:7-71 layout); n_words must be
+ * ceil(total_kmers / 12). */
+int cf1gpu_copy_states(cf1gpu_ctx *ctx, uint64_t *dst, size_t n_words);
+
+/* Mphf::hash for a batch of canonical k-mers (src/mphf.rs:268-270): the
+ * slot in [0, total_kmers); absent keys give 0, like unwrap_or(0). */
+int cf1gpu_query(cf1gpu_ctx *ctx, const uint64_t *keys, size_t n, uint64_t *slots);
+
+/* Every distinct canonical k-mer with its state (for parity checks): keys in
+ * storage order (bins in order, each bin sorted), n must be total_kmers. */
+int cf1gpu_dump_states(cf1gpu_ctx *ctx, uint64_t *keys, uint8_t *states, size_t n);
+
+/* Judge: queries every distinct key on the device and checks that the slots
+ * form a bijection onto [0, total_kmers).  0 when they do. */
+int cf1gpu_verify_bijection(cf1gpu_ctx *ctx);
+
+/* Short sequences (src/classify.rs:550-561), in input order. */
+size_t cf1gpu_short_seq_count(const cf1gpu_ctx *ctx);
+int cf1gpu_short_seq(const cf1gpu_ctx *ctx, size_t i, char *name_buf, size_t name_cap, uint64_t *len);
+
+/* Flat host image of the MPHF.  Call with dst NULL to get the size. */
+int cf1gpu_export_mphf(cf1gpu_ctx *ctx, void *dst, size_t *bytes);
+
+/* Mphf::hash on the host over an exported image (thread-safe, no device). */
+int cf1gpu_mphf_host_query(const void *image, size_t bytes, const uint64_t *keys, size_t n, uint64_t *slots);
+
+/* Learned-index statistics of the last run (learned mode): mean leaf error
+ * bound and mean search window over the keys of learned bins, mean final
+ * training loss over bins.  out3 = {mean_err, mean_window, train_loss}. */
+int cf1gpu_learned_stats(const cf1gpu_ctx *ctx, double out3[3]);
+
+/* Diagnostics: full-batch MSE loss and gradient of a learned-index root
+ * (1 -> 16 ReLU -> 1, params = w1[16] b1[16] w2[16] b2) over n samples,
+ * computed on `device` by the code the training kernel runs. */
+int cf1gpu_learned_grad(int device, const float *params, const float *x, const float *t, size_t n, float *grad,
+                        float *loss);
+
+const char *cf1gpu_last_error(const cf1gpu_ctx *ctx);
+void cf1gpu_destroy(cf1gpu_ctx *ctx);
+
+/* Library build identification (e.g. "sm_100a"). */
+const char *cf1gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CF1GPU_H */

@@ -1,0 +1,938 @@
+// cf1 oracle -- TEST INFRASTRUCTURE ONLY.
+//
+// A CPU restatement of the cf1-rs k-mer state path (phases 1-4) used as the
+// checker for the CUDA library and as the timed CPU baseline ("port").  Only
+// tests, the smoke check and the bench's CPU-baseline / reference arm load it.
+// The product library never links, loads or calls anything in this file.
+//
+// Parity status.  The reference (Rust) cannot be built in this environment (no
+// cargo/rustc), so nothing here is checked against reference *runs*.  The
+// k-mer, DNA, state-codec and state-vector functions are pinned against every
+// known-answer test the reference holds (src/dna.rs:107-134, src/kmer.rs:505-592,
+// src/state.rs:300-349, src/state_vector.rs:77-114), ported as unit tests in
+// tests/test_oracle_kat.py.  Whole-pipeline classification has no reference
+// golden output; it is cross-checked by two independent oracles that must agree:
+//   (1) cfo_run(method=0): a direct restatement of src/classify.rs (CAS loops on
+//       the 12-per-word state vector; slot map = rank in the sorted distinct set);
+//   (2) cfo_run(method=1): a per-occurrence "side join" fold (each occurrence
+//       contributes an (in, out) side pair, states are the join over occurrences).
+//
+// Binning spec.  Phase-1/2 bins in the reference come from simd-minimizers 2.3.1
+// and xxhash-rust 0.8.15 (src/minimizer.rs:18-21,104; src/superkmer.rs:119-121),
+// which are not vendored.  Bins only partition work (no reference test pins them),
+// so the GPU path uses its own canonical-minimizer spec; cfo_superkmers /
+// cfo_histogram / cfo_partition restate *that* spec (the partition itself follows
+// src/minimizer.rs:116-172 exactly) so the GPU phase-1/2 kernels can be checked
+// bit for bit.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+typedef unsigned __int128 u128;
+
+namespace {
+
+// ---------------------------------------------------------------- dna.rs ----
+// MAPPED_BASE (src/dna.rs:64-75): A/a=0 C/c=1 G/g=2 T/t=3, everything else 4.
+// IS_PLACEHOLDER (src/dna.rs:81-92): true for anything not in ACGTacgt.
+struct DnaTables {
+  uint8_t mapped[256];
+  bool placeholder[256];
+  uint8_t rc_byte[256];  // src/kmer.rs:7-21 REVERSE_COMPLEMENT_BYTE, derived
+  DnaTables() {
+    for (int i = 0; i < 256; i++) { mapped[i] = 4; placeholder[i] = true; }
+    const char up[4] = {'A', 'C', 'G', 'T'}, lo[4] = {'a', 'c', 'g', 't'};
+    for (int b = 0; b < 4; b++) {
+      mapped[(uint8_t)up[b]] = (uint8_t)b; mapped[(uint8_t)lo[b]] = (uint8_t)b;
+      placeholder[(uint8_t)up[b]] = false; placeholder[(uint8_t)lo[b]] = false;
+    }
+    // A byte holds 4 bases, base i at bits 2i..2i+1.  Its reverse complement
+    // reverses the base order and complements each base (COMPLEMENTED_BASE,
+    // src/dna.rs:77: A<->T, C<->G, i.e. 3-b).
+    for (int v = 0; v < 256; v++) {
+      int out = 0;
+      for (int i = 0; i < 4; i++) {
+        int base = (v >> (2 * i)) & 3;
+        out |= (3 - base) << (2 * (3 - i));
+      }
+      rc_byte[v] = (uint8_t)out;
+    }
+  }
+};
+const DnaTables T;
+
+inline uint8_t complement(uint8_t b) { return (uint8_t)(3 - b); }  // dna.rs:13-15,77
+
+// --------------------------------------------------------------- kmer.rs ----
+// Kmer<K> storage (src/kmer.rs:24-39, 390-460): u64 for K<=32, u128 for K<=63;
+// word 0 is the low 64 bits.  The first base sits in the most significant used
+// bits (src/kmer.rs:377-382).  Ordering compares the high word first
+// (src/kmer.rs:72-89), i.e. plain unsigned integer order.
+struct KSpec {
+  int k;
+  int nwords;       // K.div_ceil(32)          (src/kmer.rs:104)
+  uint64_t clear_msn_mask;  // src/kmer.rs:105
+  int msn_shift;    // 2*((K-1)%32)            (src/kmer.rs:107)
+  explicit KSpec(int k_) : k(k_) {
+    nwords = (k + 31) / 32;
+    msn_shift = 2 * ((k - 1) % 32);
+    clear_msn_mask = ~(3ull << msn_shift);
+  }
+};
+
+inline uint64_t word(u128 s, int idx) { return idx == 0 ? (uint64_t)s : (uint64_t)(s >> 64); }
+inline void set_word(u128 &s, int idx, uint64_t v) {
+  if (idx == 0) s = (s & ((u128)~0ull << 64)) | (u128)v;
+  else s = (s & (u128)~0ull) | ((u128)v << 64);
+}
+
+inline uint64_t encode_word(const uint8_t *label, int n) {  // src/kmer.rs:379-388
+  uint64_t acc = 0;
+  for (int i = 0; i < n; i++) acc = (acc << 2) | T.mapped[label[i]];
+  return acc;
+}
+
+u128 from_ascii(const KSpec &ks, const uint8_t *seq, uint64_t offset) {  // kmer.rs:110-131
+  const uint8_t *label = seq + offset;
+  u128 s = 0;
+  int packed_word_count = ks.k / 32;
+  for (int d = 0; d < packed_word_count; d++) {
+    int start = ks.k - (d << 5) - 32;
+    set_word(s, d, encode_word(label + start, 32));
+  }
+  int rem = ks.k & 31;
+  if (rem > 0) set_word(s, ks.nwords - 1, encode_word(label, rem));
+  return s;
+}
+
+void left_shift(const KSpec &ks, u128 &s) {  // src/kmer.rs:291-304
+  for (int idx = ks.nwords - 1; idx >= 1; idx--) {
+    uint64_t curr = word(s, idx), prev = word(s, idx - 1);
+    set_word(s, idx, (curr << 2) | (prev >> 62));
+  }
+  set_word(s, 0, word(s, 0) << 2);
+}
+
+void left_shift_by(const KSpec &ks, u128 &s, int b) {  // src/kmer.rs:306-325
+  if (b == 0) return;
+  int nb = 2 * b;
+  uint64_t mask_msns = ((1ull << nb) - 1) << (64 - nb);
+  for (int idx = ks.nwords - 1; idx >= 1; idx--) {
+    uint64_t curr = word(s, idx), prev = word(s, idx - 1);
+    set_word(s, idx, (curr << nb) | ((prev & mask_msns) >> (64 - nb)));
+  }
+  set_word(s, 0, word(s, 0) << nb);
+}
+
+void right_shift(const KSpec &ks, u128 &s) {  // src/kmer.rs:328-341
+  for (int idx = 0; idx < ks.nwords - 1; idx++) {
+    uint64_t curr = word(s, idx), next = word(s, idx + 1);
+    set_word(s, idx, (curr >> 2) | ((next & 3ull) << 62));
+  }
+  set_word(s, ks.nwords - 1, word(s, ks.nwords - 1) >> 2);
+}
+
+// Byte-table reverse complement over the little-endian storage bytes
+// (src/kmer.rs:161-200).
+u128 reverse_complement(const KSpec &ks, u128 s) {
+  uint8_t data[16], rcb[16];
+  std::memcpy(data, &s, 16);  // little-endian host: byte 0 = low byte of word 0
+  std::memset(rcb, 0, 16);
+  int packed_byte_count = ks.k / 4;
+  for (int i = 0; i < packed_byte_count; i++) rcb[packed_byte_count - 1 - i] = T.rc_byte[data[i]];
+  u128 rc;
+  std::memcpy(&rc, rcb, 16);
+  int rem = ks.k % 4;
+  if (rem == 0) return rc;
+  // rcb[packed_byte_count] is already 0 (src/kmer.rs:182-184).
+  left_shift_by(ks, rc, rem);
+  uint8_t partial = data[packed_byte_count];
+  std::memcpy(rcb, &rc, 16);
+  for (int i = 0; i < rem; i++) {
+    uint8_t base = (partial >> (2 * i)) & 3;
+    rcb[0] |= (uint8_t)(complement(base) << (2 * (rem - 1 - i)));
+  }
+  std::memcpy(&rc, rcb, 16);
+  return rc;
+}
+
+inline u128 canonical_with_rc(u128 a, u128 rc) { return a <= rc ? a : rc; }  // kmer.rs:213-219
+inline u128 canonical(const KSpec &ks, u128 a) { return canonical_with_rc(a, reverse_complement(ks, a)); }
+
+inline uint8_t front(const KSpec &ks, u128 s) { return (word(s, ks.nwords - 1) >> ks.msn_shift) & 3; }  // kmer.rs:227-230
+inline uint8_t back(u128 s) { return word(s, 0) & 3; }  // kmer.rs:233-236
+
+void roll_to_next_kmer(const KSpec &ks, u128 &s, uint8_t base, u128 &rc) {  // kmer.rs:240-262
+  set_word(s, ks.nwords - 1, word(s, ks.nwords - 1) & ks.clear_msn_mask);
+  left_shift(ks, s);
+  set_word(s, 0, word(s, 0) | base);
+  right_shift(ks, rc);
+  set_word(rc, ks.nwords - 1, word(rc, ks.nwords - 1) | ((uint64_t)complement(base) << ks.msn_shift));
+}
+
+// Correct decode of K bases at a base offset from MSB-first 2-bit bytes
+// (the contract of src/kmer.rs:133-158 for every K<=63).
+u128 from_packed_2bit(const KSpec &ks, const uint8_t *packed, uint64_t base_offset) {
+  u128 v = 0;
+  for (int i = 0; i < ks.k; i++) {
+    uint64_t p = base_offset + i;
+    v = (v << 2) | ((packed[p / 4] >> (6 - 2 * (p % 4))) & 3);
+  }
+  return v;
+}
+
+// The reference's literal arithmetic (src/kmer.rs:136-158) with release-build
+// wrapping: a u128 accumulator over bytes_needed bytes, then a shift whose
+// amount wraps mod 2^64 and is masked to 7 bits.  For K=63 with
+// base_offset%4 in {2,3}, bytes_needed is 17, the first byte is shifted out and
+// the k-mer decodes wrong.  Kept only to document that defect in a test.
+u128 from_packed_2bit_reference_arith(const KSpec &ks, const uint8_t *packed, uint64_t base_offset) {
+  uint64_t byte_start = base_offset / 4, sub_offset = base_offset % 4;
+  uint64_t total_bases = sub_offset + (uint64_t)ks.k;
+  uint64_t bytes_needed = (total_bases + 3) / 4;
+  u128 val = 0;
+  for (uint64_t i = 0; i < bytes_needed; i++) val = (val << 8) | packed[byte_start + i];
+  uint64_t sh = (uint64_t)((16 - bytes_needed) * 8 + 2 * sub_offset);  // wraps as usize
+  val <<= (sh & 127);
+  u128 result = val >> ((128 - 2 * ks.k) & 127);
+  u128 s = 0;
+  set_word(s, 0, (uint64_t)result);
+  if (ks.nwords > 1) set_word(s, 1, (uint64_t)(result >> 64));
+  return s;
+}
+
+// -------------------------------------------------------------- state.rs ----
+enum StateClass { SISO = 0, MISO = 1, SIMO = 2, MIMO = 3 };  // src/state.rs:6-11
+struct Vertex { int cls; uint8_t front, back; bool visited, outputted; };  // src/state.rs:15-21
+
+uint8_t from_vertex(const Vertex &v) {  // src/state.rs:92-113
+  if (!v.visited) return 0;
+  if (!v.outputted) {
+    switch (v.cls) {
+      case SISO: return (uint8_t)(0x10 | (v.front << 2) | v.back);
+      case MISO: return (uint8_t)(0x04 | v.back);
+      case SIMO: return (uint8_t)(0x08 | v.front);
+      default: return 0x03;
+    }
+  }
+  switch (v.cls) {
+    case SISO: return 0x0C;
+    case MISO: return 0x0D;
+    case SIMO: return 0x0E;
+    default: return 0x0F;
+  }
+}
+
+struct StateTables {  // src/state.rs:148-298
+  Vertex decode[32];
+  int cls[32];
+  uint8_t outputted[32];
+  StateTables() {
+    for (int i = 0; i < 32; i++) { decode[i] = Vertex{SISO, 0, 0, false, false}; cls[i] = SISO; outputted[i] = 0; }
+    decode[3] = Vertex{MIMO, 0, 0, true, false};
+    for (int i = 0; i < 4; i++) {
+      decode[4 + i] = Vertex{MISO, 0, (uint8_t)i, true, false};
+      decode[8 + i] = Vertex{SIMO, (uint8_t)i, 0, true, false};
+    }
+    decode[12] = Vertex{SISO, 0, 0, true, true};
+    decode[13] = Vertex{MISO, 0, 0, true, true};
+    decode[14] = Vertex{SIMO, 0, 0, true, true};
+    decode[15] = Vertex{MIMO, 0, 0, true, true};
+    for (int c = 16; c < 32; c++) decode[c] = Vertex{SISO, (uint8_t)((c >> 2) & 3), (uint8_t)(c & 3), true, false};
+    cls[3] = MIMO;
+    for (int i = 4; i < 8; i++) cls[i] = MISO;
+    for (int i = 8; i < 12; i++) cls[i] = SIMO;
+    cls[12] = SISO; cls[13] = MISO; cls[14] = SIMO; cls[15] = MIMO;
+    outputted[3] = 0x0F;
+    for (int i = 4; i < 8; i++) outputted[i] = 0x0D;
+    for (int i = 8; i < 12; i++) outputted[i] = 0x0E;
+    outputted[12] = 0x0C; outputted[13] = 0x0D; outputted[14] = 0x0E; outputted[15] = 0x0F;
+    for (int i = 16; i < 32; i++) outputted[i] = 0x0C;
+  }
+};
+const StateTables ST;
+
+inline bool is_visited(uint8_t s) { return s != 0; }                             // state.rs:121-124
+inline bool is_dead_end(uint8_t s) { return is_visited(s) && ST.cls[s] == MIMO; }  // state.rs:127-130
+inline uint8_t with_class(uint8_t s, int cls) {  // State::from_vertex(&Vertex{state_class, ..vertex})
+  Vertex v = ST.decode[s];
+  v.cls = cls;
+  return from_vertex(v);
+}
+
+// -------------------------------------------------------- state_vector.rs ----
+// 12 five-bit states per u64, index i in word i/12 at shift 5*(i%12)
+// (src/state_vector.rs:7-71).
+struct AtomicStateVector {
+  std::vector<std::atomic<uint64_t>> data;
+  uint64_t len;
+  explicit AtomicStateVector(uint64_t n) : data((n + 11) / 12), len(n) {
+    for (auto &w : data) w.store(0, std::memory_order_relaxed);
+  }
+  uint8_t get(uint64_t i) const {  // src/state_vector.rs:36-42
+    uint64_t w = data[i / 12].load(std::memory_order_acquire);
+    return (uint8_t)((w >> (5 * (i % 12))) & 0x1F);
+  }
+  bool compare_and_swap(uint64_t i, uint8_t expected, uint8_t nv) {  // src/state_vector.rs:47-70
+    unsigned shift = 5 * (i % 12);
+    uint64_t mask = 0x1Full << shift;
+    auto &a = data[i / 12];
+    for (;;) {
+      uint64_t cur = a.load(std::memory_order_acquire);
+      if (((cur >> shift) & 0x1F) != expected) return false;
+      uint64_t nw = (cur & ~mask) | ((uint64_t)nv << shift);
+      if (a.compare_exchange_weak(cur, nw, std::memory_order_acq_rel, std::memory_order_relaxed)) return true;
+    }
+  }
+};
+
+// ------------------------------------------------------- exact slot map ----
+// Stand-in for Mphf::hash (src/mphf.rs:268-270): an injective map from the
+// distinct canonical k-mers onto [0, n) -- here the rank in sorted order.
+// Absent keys map to 0, like `unwrap_or(0)`.
+struct ExactMap {
+  std::vector<u128> keys;  // sorted, distinct
+  uint64_t hash(u128 key) const {
+    auto it = std::lower_bound(keys.begin(), keys.end(), key);
+    if (it == keys.end() || *it != key) return 0;
+    return (uint64_t)(it - keys.begin());
+  }
+};
+
+// -------------------------------------------------------------- classify.rs ----
+struct DirectedKmer {  // src/directed_kmer.rs:12-64
+  u128 kmer, rc, can;
+  bool fwd;
+  void init(const KSpec &ks, u128 k) {
+    kmer = k; rc = reverse_complement(ks, k); can = canonical_with_rc(kmer, rc); fwd = (kmer == can);
+  }
+  void roll(const KSpec &ks, uint8_t next_char) {
+    roll_to_next_kmer(ks, kmer, T.mapped[next_char], rc);
+    can = canonical_with_rc(kmer, rc);
+    fwd = (kmer == can);
+  }
+};
+
+struct Classifier {  // src/classify.rs:17-519
+  const KSpec &ks;
+  const ExactMap &mphf;
+  AtomicStateVector &states;
+  int K;
+  Classifier(const KSpec &s, const ExactMap &m, AtomicStateVector &v) : ks(s), mphf(m), states(v), K(s.k) {}
+
+  void process_substring(const uint8_t *seq, uint64_t seq_len, uint64_t left_end, uint64_t right_end) {  // 34-43
+    uint64_t kmer_idx = left_end;
+    while (kmer_idx <= right_end) {
+      kmer_idx = search_valid_kmer(seq, kmer_idx, right_end);
+      if (kmer_idx > right_end) break;
+      kmer_idx = process_contiguous_subseq(seq, seq_len, right_end, kmer_idx);
+    }
+  }
+  uint64_t search_valid_kmer(const uint8_t *seq, uint64_t start, uint64_t right_end) {  // 46-61
+    while (start <= right_end) {
+      bool valid = true;
+      for (int j = 0; j < K; j++) {
+        if (T.placeholder[seq[start + j]]) { start = start + j + 1; valid = false; break; }
+      }
+      if (valid) return start;
+    }
+    return right_end + 1;
+  }
+  uint64_t process_contiguous_subseq(const uint8_t *seq, uint64_t seq_len, uint64_t right_end, uint64_t start_idx) {  // 65-141
+    uint64_t kmer_idx = start_idx;
+    DirectedKmer curr; curr.init(ks, from_ascii(ks, seq, kmer_idx));
+    bool no_left = kmer_idx == 0 || T.placeholder[seq[kmer_idx - 1]];
+    bool no_right = kmer_idx + K == seq_len || T.placeholder[seq[kmer_idx + K]];
+    if (no_left && no_right) {
+      while (!process_isolated_kmer(curr)) {}
+    } else {
+      if (no_right) {
+        while (!process_rightmost_kmer(curr, seq[kmer_idx - 1])) {}
+        return kmer_idx + K;
+      }
+      DirectedKmer next = curr;
+      next.roll(ks, seq[kmer_idx + K]);
+      if (no_left) {
+        while (!process_leftmost_kmer(curr, next, seq[kmer_idx + K])) {}
+      } else {
+        while (!process_internal_kmer(curr, next, seq[kmer_idx - 1], seq[kmer_idx + K])) {}
+      }
+      kmer_idx += 1;
+      while (kmer_idx < right_end && !T.placeholder[seq[kmer_idx + K]]) {
+        curr = next;
+        next.roll(ks, seq[kmer_idx + K]);
+        while (!process_internal_kmer(curr, next, seq[kmer_idx - 1], seq[kmer_idx + K])) {}
+        kmer_idx += 1;
+      }
+      if (kmer_idx <= right_end) {
+        curr = next;
+        if (kmer_idx + K == seq_len || T.placeholder[seq[kmer_idx + K]]) {
+          while (!process_rightmost_kmer(curr, seq[kmer_idx - 1])) {}
+        } else {
+          next.roll(ks, seq[kmer_idx + K]);
+          while (!process_internal_kmer(curr, next, seq[kmer_idx - 1], seq[kmer_idx + K])) {}
+        }
+      } else {
+        kmer_idx -= 1;
+      }
+    }
+    return kmer_idx + K;
+  }
+  bool process_isolated_kmer(const DirectedKmer &km) {  // 147-158
+    uint64_t idx = mphf.hash(km.can);
+    uint8_t state = states.get(idx);
+    if (is_dead_end(state)) return true;
+    return states.compare_and_swap(idx, state, from_vertex(Vertex{MIMO, 0, 0, true, false}));
+  }
+  bool process_loop(const DirectedKmer &km, const DirectedKmer &next, uint8_t prev_char) {  // 160-177
+    if (prev_char == 0 || km.kmer == next.kmer) {
+      uint64_t idx = mphf.hash(km.can);
+      uint8_t state = states.get(idx);
+      return states.compare_and_swap(idx, state, from_vertex(Vertex{MIMO, 0, 0, true, false}));
+    }
+    return process_rightmost_kmer(km, prev_char);
+  }
+  bool process_leftmost_kmer(const DirectedKmer &km, const DirectedKmer &next, uint8_t next_char) {  // 179-285
+    uint64_t idx = mphf.hash(km.can);
+    uint8_t state = states.get(idx);
+    if (is_dead_end(state)) return true;
+    if (km.can == next.can) return process_loop(km, next, 0);
+    uint8_t old_state = state, ns;
+    uint8_t next_base = T.mapped[next_char];
+    if (km.fwd) {
+      if (!is_visited(state)) ns = from_vertex(Vertex{MISO, 0, next_base, true, false});
+      else {
+        Vertex v = ST.decode[state];
+        if (v.cls == SISO) ns = with_class(state, v.back == next_base ? MISO : MIMO);
+        else if (v.cls == MISO) ns = v.back != next_base ? with_class(state, MIMO) : old_state;
+        else ns = with_class(state, MIMO);
+      }
+    } else {
+      uint8_t cn = complement(next_base);
+      if (!is_visited(state)) ns = from_vertex(Vertex{SIMO, cn, 0, true, false});
+      else {
+        Vertex v = ST.decode[state];
+        if (v.cls == SISO) ns = with_class(state, v.front == cn ? SIMO : MIMO);
+        else if (v.cls == MISO) ns = with_class(state, MIMO);
+        else ns = v.front != cn ? with_class(state, MIMO) : old_state;
+      }
+    }
+    if (ns == old_state) return true;
+    return states.compare_and_swap(idx, old_state, ns);
+  }
+  bool process_rightmost_kmer(const DirectedKmer &km, uint8_t prev_char) {  // 287-383
+    uint64_t idx = mphf.hash(km.can);
+    uint8_t state = states.get(idx);
+    if (is_dead_end(state)) return true;
+    uint8_t old_state = state, ns;
+    uint8_t prev_base = T.mapped[prev_char];
+    if (km.fwd) {
+      if (!is_visited(state)) ns = from_vertex(Vertex{SIMO, prev_base, 0, true, false});
+      else {
+        Vertex v = ST.decode[state];
+        if (v.cls == SISO) ns = with_class(state, v.front == prev_base ? SIMO : MIMO);
+        else if (v.cls == MISO) ns = with_class(state, MIMO);
+        else ns = v.front != prev_base ? with_class(state, MIMO) : old_state;
+      }
+    } else {
+      uint8_t cp = complement(prev_base);
+      if (!is_visited(state)) ns = from_vertex(Vertex{MISO, 0, cp, true, false});
+      else {
+        Vertex v = ST.decode[state];
+        if (v.cls == SISO) ns = with_class(state, v.back == cp ? MISO : MIMO);
+        else if (v.cls == MISO) ns = v.back != cp ? with_class(state, MIMO) : old_state;
+        else ns = with_class(state, MIMO);
+      }
+    }
+    if (ns == old_state) return true;
+    return states.compare_and_swap(idx, old_state, ns);
+  }
+  bool process_internal_kmer(const DirectedKmer &km, const DirectedKmer &next, uint8_t prev_char, uint8_t next_char) {  // 385-518
+    uint64_t idx = mphf.hash(km.can);
+    uint8_t state = states.get(idx);
+    if (is_dead_end(state)) return true;
+    if (km.can == next.can) return process_loop(km, next, prev_char);
+    uint8_t old_state = state, ns;
+    uint8_t pb = T.mapped[prev_char], nb = T.mapped[next_char];
+    uint8_t f, b;  // expected front/back in canonical orientation
+    if (km.fwd) { f = pb; b = nb; } else { f = complement(nb); b = complement(pb); }
+    if (!is_visited(state)) ns = from_vertex(Vertex{SISO, f, b, true, false});
+    else {
+      Vertex v = ST.decode[state];
+      if (v.cls == SISO) {
+        if (v.front == f && v.back == b) return true;
+        else if (v.front != f && v.back != b) ns = with_class(state, MIMO);
+        else if (v.front != f) ns = with_class(state, MISO);
+        else ns = with_class(state, SIMO);
+      } else if (v.cls == MISO) {
+        ns = v.back != b ? with_class(state, MIMO) : old_state;
+      } else {
+        ns = v.front != f ? with_class(state, MIMO) : old_state;
+      }
+    }
+    if (ns == old_state) return true;
+    return states.compare_and_swap(idx, old_state, ns);
+  }
+};
+
+// ----------------------------------------------------- side-join oracle ----
+// Independent second oracle.  Each valid k-mer occurrence contributes an
+// (in, out) side pair in canonical orientation; a missing neighbour (record
+// end or placeholder) is "multi".  States are the per-side join over all
+// occurrences: equal sides stay, different sides become multi.  Encoding:
+// (M,M)=3, (M,b)=4|b, (f,M)=8|f, (f,b)=16|f<<2|b (src/state.rs:92-113).
+const uint8_t SIDE_M = 4;
+inline uint8_t encode_sides(uint8_t f, uint8_t b) {
+  if (f == SIDE_M && b == SIDE_M) return 3;
+  if (f == SIDE_M) return (uint8_t)(4 | b);
+  if (b == SIDE_M) return (uint8_t)(8 | f);
+  return (uint8_t)(16 | (f << 2) | b);
+}
+inline void decode_sides(uint8_t s, uint8_t &f, uint8_t &b) {
+  if (s == 3) { f = SIDE_M; b = SIDE_M; }
+  else if (s >= 4 && s < 8) { f = SIDE_M; b = s & 3; }
+  else if (s >= 8 && s < 12) { f = s & 3; b = SIDE_M; }
+  else { f = (s >> 2) & 3; b = s & 3; }
+}
+inline uint8_t join_side(uint8_t a, uint8_t b) { return a == b ? a : SIDE_M; }
+inline uint8_t join_state(uint8_t s, uint8_t c) {
+  if (s == 0) return c;
+  uint8_t f1, b1, f2, b2;
+  decode_sides(s, f1, b1); decode_sides(c, f2, b2);
+  return encode_sides(join_side(f1, f2), join_side(b1, b2));
+}
+
+// ------------------------------------------------------------- sorting ----
+void radix_sort_u64(std::vector<uint64_t> &v, int nthreads) {
+  // Parallel LSD radix sort, 8-bit digits, skipping digits that are constant.
+  size_t n = v.size();
+  if (n < 2) return;
+  std::vector<uint64_t> tmp(n);
+  uint64_t orv = 0;
+  for (uint64_t x : v) orv |= x;
+  int nt = std::max(1, nthreads);
+  std::vector<std::vector<size_t>> hist(nt, std::vector<size_t>(256));
+  for (int shift = 0; shift < 64; shift += 8) {
+    if (((orv >> shift) & 0xFF) == 0) continue;
+    size_t chunk = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; t++) th.emplace_back([&, t] {
+      auto &h = hist[t]; std::fill(h.begin(), h.end(), 0);
+      size_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+      for (size_t i = a; i < b; i++) h[(v[i] >> shift) & 0xFF]++;
+    });
+    for (auto &x : th) x.join();
+    th.clear();
+    size_t off = 0;
+    for (int d = 0; d < 256; d++)
+      for (int t = 0; t < nt; t++) { size_t c = hist[t][d]; hist[t][d] = off; off += c; }
+    for (int t = 0; t < nt; t++) th.emplace_back([&, t] {
+      auto &h = hist[t];
+      size_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+      for (size_t i = a; i < b; i++) tmp[h[(v[i] >> shift) & 0xFF]++] = v[i];
+    });
+    for (auto &x : th) x.join();
+    v.swap(tmp);
+  }
+}
+
+// ------------------------------------------------------------- pipeline ----
+struct Input {
+  const uint8_t *seq;
+  const uint64_t *off;  // n_rec + 1 offsets into seq
+  uint64_t n_rec;
+};
+
+struct Result {
+  int k;
+  std::vector<u128> keys;     // sorted distinct canonical k-mers
+  std::vector<uint8_t> states;  // per distinct key
+  std::vector<uint64_t> state_words;  // 12-per-word vector in rank-slot order
+  std::vector<uint64_t> short_idx, short_len;
+  uint64_t n_occ = 0;
+  double t_keys = 0, t_sort = 0, t_classify = 0;
+};
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+template <class F>
+void parallel_for(uint64_t n, int nthreads, F f) {
+  std::atomic<uint64_t> next(0);
+  std::vector<std::thread> th;
+  int nt = std::max(1, nthreads);
+  for (int t = 0; t < nt; t++) th.emplace_back([&] {
+    for (;;) { uint64_t i = next.fetch_add(1); if (i >= n) break; f(i); }
+  });
+  for (auto &x : th) x.join();
+}
+
+// Phase-3 semantics (src/mphf.rs:323-363): the distinct canonical k-mers of
+// every placeholder-free window of every record of length >= k.
+void collect_distinct(const KSpec &ks, const Input &in, int nthreads, Result &r) {
+  double t0 = now_s();
+  int K = ks.k;
+  std::vector<std::vector<u128>> per(in.n_rec);
+  std::atomic<uint64_t> occ(0);
+  parallel_for(in.n_rec, nthreads, [&](uint64_t i) {
+    const uint8_t *s = in.seq + in.off[i];
+    uint64_t len = in.off[i + 1] - in.off[i];
+    if (len < (uint64_t)K) return;
+    auto &out = per[i];
+    uint64_t run = 0;
+    u128 fw = 0, rc = 0;
+    for (uint64_t p = 0; p < len; p++) {
+      if (T.placeholder[s[p]]) { run = 0; continue; }
+      run++;
+      if (run == (uint64_t)K) { fw = from_ascii(ks, s, p + 1 - K); rc = reverse_complement(ks, fw); }
+      else if (run > (uint64_t)K) roll_to_next_kmer(ks, fw, T.mapped[s[p]], rc);
+      if (run >= (uint64_t)K) out.push_back(canonical_with_rc(fw, rc));
+    }
+    occ += out.size();
+  });
+  r.n_occ = occ.load();
+  double t1 = now_s();
+  r.t_keys = t1 - t0;
+  if (K <= 32) {
+    std::vector<uint64_t> all;
+    all.reserve(r.n_occ);
+    for (auto &v : per) { for (u128 x : v) all.push_back((uint64_t)x); std::vector<u128>().swap(v); }
+    radix_sort_u64(all, nthreads);
+    all.erase(std::unique(all.begin(), all.end()), all.end());
+    r.keys.resize(all.size());
+    for (size_t i = 0; i < all.size(); i++) r.keys[i] = all[i];
+  } else {
+    std::vector<u128> all;
+    all.reserve(r.n_occ);
+    for (auto &v : per) { all.insert(all.end(), v.begin(), v.end()); std::vector<u128>().swap(v); }
+    std::sort(all.begin(), all.end());
+    all.erase(std::unique(all.begin(), all.end()), all.end());
+    r.keys.swap(all);
+  }
+  r.t_sort = now_s() - t1;
+}
+
+const uint64_t CHUNK_KMERS = 4000000;  // src/classify.rs:13
+
+// classify_vertices (src/classify.rs:524-601): records in input order; records
+// shorter than k are tracked; records under CHUNK_KMERS bases are one task,
+// longer ones are cut into CHUNK_KMERS-k-mer chunks over the shared buffer.
+void classify_direct(const KSpec &ks, const Input &in, int nthreads, Result &r) {
+  double t0 = now_s();
+  ExactMap map;
+  map.keys.swap(r.keys);
+  AtomicStateVector states(map.keys.size());
+  Classifier cls(ks, map, states);
+  uint64_t K = ks.k;
+  struct Task { uint64_t rec, left, right; };
+  std::vector<Task> tasks;
+  for (uint64_t i = 0; i < in.n_rec; i++) {
+    uint64_t len = in.off[i + 1] - in.off[i];
+    if (len < K) { r.short_idx.push_back(i); r.short_len.push_back(len); continue; }
+    uint64_t right_end = len - K;
+    if (len < CHUNK_KMERS) tasks.push_back({i, 0, right_end});
+    else for (uint64_t left = 0; left <= right_end; left += CHUNK_KMERS)
+      tasks.push_back({i, left, std::min(left + CHUNK_KMERS - 1, right_end)});
+  }
+  parallel_for(tasks.size(), nthreads, [&](uint64_t t) {
+    const Task &tk = tasks[t];
+    cls.process_substring(in.seq + in.off[tk.rec], in.off[tk.rec + 1] - in.off[tk.rec], tk.left, tk.right);
+  });
+  r.keys.swap(map.keys);
+  r.states.resize(r.keys.size());
+  r.state_words.resize(states.data.size());
+  for (size_t i = 0; i < r.state_words.size(); i++) r.state_words[i] = states.data[i].load();
+  for (size_t i = 0; i < r.keys.size(); i++) r.states[i] = states.get(i);
+  r.t_classify = now_s() - t0;
+}
+
+// Per-occurrence side pair (derived from src/classify.rs:65-518): isolated ->
+// (M,M); rightmost -> fwd (prev,M) / bwd (M,c(prev)); self loop (canonical of
+// this == canonical of next): leftmost or direct repeat -> (M,M), inverted
+// repeat -> as rightmost; leftmost -> fwd (M,next) / bwd (c(next),M);
+// internal -> fwd (prev,next) / bwd (c(next),c(prev)).
+uint8_t contribution(const KSpec &ks, u128 fw, u128 rc, bool has_prev, uint8_t prev, bool has_next, uint8_t next) {
+  u128 can = canonical_with_rc(fw, rc);
+  bool fwd = (fw == can);
+  if (!has_prev && !has_next) return 3;
+  auto rightmost = [&]() { return fwd ? encode_sides(prev, SIDE_M) : encode_sides(SIDE_M, complement(prev)); };
+  if (!has_next) return rightmost();
+  u128 nf = fw, nr = rc;
+  roll_to_next_kmer(ks, nf, next, nr);
+  if (canonical_with_rc(nf, nr) == can) {
+    if (!has_prev || nf == fw) return 3;
+    return rightmost();
+  }
+  if (!has_prev) return fwd ? encode_sides(SIDE_M, next) : encode_sides(complement(next), SIDE_M);
+  return fwd ? encode_sides(prev, next) : encode_sides(complement(next), complement(prev));
+}
+
+void classify_join(const KSpec &ks, const Input &in, int nthreads, Result &r) {
+  double t0 = now_s();
+  uint64_t K = ks.k;
+  std::vector<std::vector<std::pair<u128, uint8_t>>> per(in.n_rec);
+  for (uint64_t i = 0; i < in.n_rec; i++) {
+    uint64_t len = in.off[i + 1] - in.off[i];
+    if (len < K) { r.short_idx.push_back(i); r.short_len.push_back(len); }
+  }
+  parallel_for(in.n_rec, nthreads, [&](uint64_t i) {
+    const uint8_t *s = in.seq + in.off[i];
+    uint64_t len = in.off[i + 1] - in.off[i];
+    if (len < K) return;
+    for (uint64_t p = 0; p + K <= len; p++) {
+      bool ok = true;
+      for (uint64_t j = 0; j < K; j++) if (T.placeholder[s[p + j]]) { ok = false; break; }
+      if (!ok) continue;
+      u128 fw = from_ascii(ks, s, p), rc = reverse_complement(ks, fw);
+      bool hp = p > 0 && !T.placeholder[s[p - 1]];
+      bool hn = p + K < len && !T.placeholder[s[p + K]];
+      uint8_t c = contribution(ks, fw, rc, hp, hp ? T.mapped[s[p - 1]] : 0, hn, hn ? T.mapped[s[p + K]] : 0);
+      per[i].push_back({canonical_with_rc(fw, rc), c});
+    }
+  });
+  std::vector<std::pair<u128, uint8_t>> all;
+  for (auto &v : per) { all.insert(all.end(), v.begin(), v.end()); std::vector<std::pair<u128, uint8_t>>().swap(v); }
+  r.n_occ = all.size();
+  std::sort(all.begin(), all.end(), [](const std::pair<u128, uint8_t> &a, const std::pair<u128, uint8_t> &b) { return a.first < b.first; });
+  r.keys.clear(); r.states.clear();
+  for (size_t i = 0; i < all.size();) {
+    size_t j = i;
+    uint8_t s = 0;
+    while (j < all.size() && all[j].first == all[i].first) { s = join_state(s, all[j].second); j++; }
+    r.keys.push_back(all[i].first);
+    r.states.push_back(s);
+    i = j;
+  }
+  r.state_words.assign((r.keys.size() + 11) / 12, 0);
+  for (size_t i = 0; i < r.keys.size(); i++) r.state_words[i / 12] |= (uint64_t)r.states[i] << (5 * (i % 12));
+  r.t_classify = now_s() - t0;
+}
+
+// ------------------------------------------------------- binning spec ----
+// Canonical minimizers over m-mers (m odd, m <= 15 so a canonical m-mer fits in
+// 30 bits).  Order key of an m-mer: (h(c) << 32) | c with c = min(fwd, rc) and
+// h a bijective 32-bit mixer, so no two distinct m-mers tie.  A k-mer's
+// minimizer is the least order key over its w = k-m+1 m-mers; it is the same
+// for a k-mer and its reverse complement.  Histogram bucket of a minimizer:
+// the top 16 bits of a second bijective mixer of c.
+inline uint32_t mix_order(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return x;
+}
+inline uint32_t mix_bucket(uint32_t x) {
+  x ^= 0x5bd1e995u;
+  x ^= x >> 16; x *= 0x21f0aaadu; x ^= x >> 15; x *= 0x735a2d97u; x ^= x >> 15;
+  return x >> 16;
+}
+inline uint32_t mmer_rc(uint32_t x, int m) {
+  uint32_t r = 0;
+  for (int i = 0; i < m; i++) { r = (r << 2) | (3 - (x & 3)); x >>= 2; }
+  return r;
+}
+
+struct SuperKmer { uint64_t pos; uint32_t n; uint32_t bucket; };
+
+// Super k-mers of the concatenated sequence: k-mer start positions are cut into
+// tiles of `tile` positions; inside a tile a super k-mer is a maximal run of
+// consecutive valid k-mers with the same minimizer.
+void superkmers(const uint8_t *seq, uint64_t L, int k, int m, uint32_t tile, std::vector<SuperKmer> &out) {
+  if (L < (uint64_t)k) return;
+  uint64_t nk = L - k + 1;
+  int w = k - m + 1;
+  std::vector<uint64_t> ord(L - m + 1);
+  uint32_t mmask = (m == 16) ? 0xFFFFFFFFu : ((1u << (2 * m)) - 1);
+  uint32_t fw = 0;
+  for (uint64_t q = 0; q < L; q++) {
+    fw = ((fw << 2) | (T.mapped[seq[q]] & 3)) & mmask;
+    if (q + 1 >= (uint64_t)m) {
+      uint32_t c = std::min(fw, mmer_rc(fw, m));
+      ord[q + 1 - m] = ((uint64_t)mix_order(c) << 32) | c;
+    }
+  }
+  // next placeholder at or after position p
+  std::vector<uint64_t> nextN(L + 1);
+  nextN[L] = L;
+  for (uint64_t p = L; p-- > 0;) nextN[p] = T.placeholder[seq[p]] ? p : nextN[p + 1];
+  auto valid = [&](uint64_t p) { return nextN[p] >= p + (uint64_t)k; };
+  auto mz = [&](uint64_t p) { uint64_t v = ~0ull; for (int j = 0; j < w; j++) v = std::min(v, ord[p + j]); return v; };
+  for (uint64_t t0 = 0; t0 < nk; t0 += tile) {
+    uint64_t t1 = std::min(nk, t0 + tile);
+    uint64_t p = t0;
+    while (p < t1) {
+      if (!valid(p)) { p++; continue; }
+      uint64_t z = mz(p), q = p + 1;
+      while (q < t1 && valid(q) && mz(q) == z) q++;
+      out.push_back({p, (uint32_t)(q - p), mix_bucket((uint32_t)z)});
+      p = q;
+    }
+  }
+}
+
+// Greedy count-balanced partition (src/minimizer.rs:116-144) and the
+// bucket -> bin table (src/minimizer.rs:156-172).
+void partition(const uint64_t *hist, uint32_t num_buckets, uint32_t num_bins, uint16_t *lut, uint32_t *bins_out) {
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < num_buckets; i++) total += hist[i];
+  uint64_t target = total / num_bins;
+  std::vector<uint16_t> boundaries;
+  uint64_t cur = 0;
+  for (uint32_t b = 0; b < num_buckets; b++) {
+    cur += hist[b];
+    if (cur >= target && boundaries.size() < num_bins - 1) { boundaries.push_back((uint16_t)b); cur -= target; }
+  }
+  uint16_t bin = 0;
+  size_t bi = 0;
+  for (uint32_t b = 0; b < num_buckets; b++) {
+    if (bi < boundaries.size() && (uint16_t)b > boundaries[bi]) { bin++; bi++; }
+    lut[b] = bin;
+  }
+  *bins_out = (uint32_t)boundaries.size() + 1;
+}
+
+}  // namespace
+
+// ================================================================ C ABI ====
+extern "C" {
+
+// --- dna / kmer (src/dna.rs, src/kmer.rs) ---
+uint8_t cfo_mapped_base(uint8_t c) { return T.mapped[c]; }
+int cfo_is_placeholder(uint8_t c) { return T.placeholder[c] ? 1 : 0; }
+uint8_t cfo_complement_base(uint8_t b) { return complement(b); }
+uint8_t cfo_rc_byte(uint8_t v) { return T.rc_byte[v]; }
+
+static inline void put(u128 v, uint64_t out[2]) { out[0] = (uint64_t)v; out[1] = (uint64_t)(v >> 64); }
+static inline u128 get(const uint64_t in[2]) { return ((u128)in[1] << 64) | in[0]; }
+
+void cfo_kmer_from_ascii(int k, const uint8_t *seq, uint64_t offset, uint64_t out[2]) { put(from_ascii(KSpec(k), seq, offset), out); }
+void cfo_kmer_reverse_complement(int k, const uint64_t in[2], uint64_t out[2]) { put(reverse_complement(KSpec(k), get(in)), out); }
+void cfo_kmer_canonical(int k, const uint64_t in[2], uint64_t out[2]) { put(canonical(KSpec(k), get(in)), out); }
+int cfo_kmer_front(int k, const uint64_t in[2]) { return front(KSpec(k), get(in)); }
+int cfo_kmer_back(int k, const uint64_t in[2]) { (void)k; return back(get(in)); }
+void cfo_kmer_roll(int k, uint64_t kmer[2], uint64_t rc[2], uint8_t base) {
+  KSpec ks(k); u128 a = get(kmer), b = get(rc);
+  roll_to_next_kmer(ks, a, base, b);
+  put(a, kmer); put(b, rc);
+}
+void cfo_kmer_label(int k, const uint64_t in[2], char *out) {  // src/kmer.rs:277-288
+  KSpec ks(k); u128 c = get(in);
+  for (int i = k - 1; i >= 0; i--) { out[i] = "ACGT"[(uint64_t)c & 3]; right_shift(ks, c); }
+  out[k] = 0;
+}
+int cfo_kmer_cmp(int k, const uint64_t a[2], const uint64_t b[2]) { (void)k; u128 x = get(a), y = get(b); return x < y ? -1 : (x > y ? 1 : 0); }
+void cfo_kmer_from_packed_2bit(int k, const uint8_t *packed, uint64_t base_offset, uint64_t out[2]) { put(from_packed_2bit(KSpec(k), packed, base_offset), out); }
+void cfo_kmer_from_packed_2bit_reference_arith(int k, const uint8_t *packed, uint64_t base_offset, uint64_t out[2]) {
+  put(from_packed_2bit_reference_arith(KSpec(k), packed, base_offset), out);
+}
+
+// --- state.rs ---
+uint8_t cfo_state_from_vertex(int cls, int front_, int back_, int visited, int outputted) {
+  return from_vertex(Vertex{cls, (uint8_t)front_, (uint8_t)back_, visited != 0, outputted != 0});
+}
+void cfo_state_decode(uint8_t code, int out5[5]) {
+  const Vertex &v = ST.decode[code & 31];
+  out5[0] = v.cls; out5[1] = v.front; out5[2] = v.back; out5[3] = v.visited; out5[4] = v.outputted;
+}
+int cfo_state_class(uint8_t code) { return ST.cls[code & 31]; }
+int cfo_state_is_dead_end(uint8_t code) { return is_dead_end(code & 31) ? 1 : 0; }
+uint8_t cfo_state_outputted(uint8_t code) { return ST.outputted[code & 31]; }
+uint8_t cfo_state_join(uint8_t s, uint8_t c) { return join_state(s, c); }
+
+// --- state_vector.rs ---
+void *cfo_asv_new(uint64_t len) { return new AtomicStateVector(len); }
+void cfo_asv_free(void *h) { delete (AtomicStateVector *)h; }
+uint8_t cfo_asv_get(void *h, uint64_t i) { return ((AtomicStateVector *)h)->get(i); }
+int cfo_asv_cas(void *h, uint64_t i, uint8_t expected, uint8_t nv) { return ((AtomicStateVector *)h)->compare_and_swap(i, expected, nv) ? 1 : 0; }
+uint64_t cfo_asv_word(void *h, uint64_t w) { return ((AtomicStateVector *)h)->data[w].load(); }
+uint64_t cfo_asv_num_words(void *h) { return ((AtomicStateVector *)h)->data.size(); }
+
+// --- phases 1-4 ---
+// method 0: direct restatement of classify.rs; method 1: side-join fold.
+void *cfo_run(int k, const uint8_t *seq, const uint64_t *rec_off, uint64_t n_rec, int nthreads, int method) {
+  if (k < 1 || k > 63 || (k % 2) == 0) return nullptr;  // src/params.rs:167-170
+  KSpec ks(k);
+  Input in{seq, rec_off, n_rec};
+  Result *r = new Result();
+  r->k = k;
+  if (method == 0) {
+    collect_distinct(ks, in, nthreads, *r);
+    classify_direct(ks, in, nthreads, *r);
+  } else {
+    classify_join(ks, in, nthreads, *r);
+  }
+  return r;
+}
+void cfo_free(void *h) { delete (Result *)h; }
+uint64_t cfo_n_distinct(void *h) { return ((Result *)h)->keys.size(); }
+uint64_t cfo_n_occ(void *h) { return ((Result *)h)->n_occ; }
+void cfo_copy_keys(void *h, uint64_t *out) {  // (lo, hi) pairs when k > 32, else one word per key
+  Result *r = (Result *)h;
+  size_t n = r->keys.size();
+  if (r->k <= 32) for (size_t i = 0; i < n; i++) out[i] = (uint64_t)r->keys[i];
+  else for (size_t i = 0; i < n; i++) { out[2 * i] = (uint64_t)r->keys[i]; out[2 * i + 1] = (uint64_t)(r->keys[i] >> 64); }
+}
+void cfo_copy_states(void *h, uint8_t *out) { Result *r = (Result *)h; std::memcpy(out, r->states.data(), r->states.size()); }
+uint64_t cfo_num_state_words(void *h) { return ((Result *)h)->state_words.size(); }
+void cfo_copy_state_words(void *h, uint64_t *out) { Result *r = (Result *)h; std::memcpy(out, r->state_words.data(), r->state_words.size() * 8); }
+uint64_t cfo_n_short(void *h) { return ((Result *)h)->short_idx.size(); }
+void cfo_copy_short(void *h, uint64_t *idx, uint64_t *len) {
+  Result *r = (Result *)h;
+  for (size_t i = 0; i < r->short_idx.size(); i++) { idx[i] = r->short_idx[i]; len[i] = r->short_len[i]; }
+}
+void cfo_times(void *h, double out3[3]) { Result *r = (Result *)h; out3[0] = r->t_keys; out3[1] = r->t_sort; out3[2] = r->t_classify; }
+
+// --- binning spec ---
+int cfo_minimizer_len(int k) {  // src/params.rs:221-228
+  int m = std::min(k / 2, 15);
+  if (m % 2 == 0) m = std::max(m - 1, 1);
+  return m;
+}
+uint32_t cfo_mix_order(uint32_t x) { return mix_order(x); }
+uint32_t cfo_mix_bucket(uint32_t x) { return mix_bucket(x); }
+// Returns the number of super k-mers; fills up to cap entries of pos/n/bucket.
+uint64_t cfo_superkmers(const uint8_t *seq, uint64_t L, int k, uint32_t tile, uint64_t *pos, uint32_t *n, uint32_t *bucket, uint64_t cap) {
+  std::vector<SuperKmer> v;
+  superkmers(seq, L, k, cfo_minimizer_len(k), tile, v);
+  for (size_t i = 0; i < v.size() && i < cap; i++) { pos[i] = v[i].pos; n[i] = v[i].n; bucket[i] = v[i].bucket; }
+  return v.size();
+}
+void cfo_partition(const uint64_t *hist, uint32_t num_buckets, uint32_t num_bins, uint16_t *lut, uint32_t *bins_out) {
+  partition(hist, num_buckets, num_bins, lut, bins_out);
+}
+
+// Learned-index root (1 -> H ReLU -> 1, H = 16): full-batch mean squared
+// error and its gradient in double precision, for checking the device's
+// training kernels.  params = w1[H] b1[H] w2[H] b2.
+void cfo_mlp_grad(const float *params, const float *x, const float *t, uint64_t n, double *grad, double *loss) {
+  const int H = 16;
+  for (int p = 0; p < 3 * H + 1; p++) grad[p] = 0;
+  double l = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    double z[H], a[H];
+    double y = params[3 * H];
+    for (int j = 0; j < H; j++) {
+      z[j] = (double)params[j] * x[i] + params[H + j];
+      a[j] = z[j] > 0 ? z[j] : 0;
+      y += (double)params[2 * H + j] * a[j];
+    }
+    double e = y - t[i];
+    l += e * e / (double)n;
+    double dy = 2 * e / (double)n;
+    grad[3 * H] += dy;
+    for (int j = 0; j < H; j++) {
+      grad[2 * H + j] += dy * a[j];
+      double dz = z[j] > 0 ? dy * params[2 * H + j] : 0;
+      grad[j] += dz * x[i];
+      grad[H + j] += dz;
+    }
+  }
+  *loss = l;
+}
+
+}  // extern "C"

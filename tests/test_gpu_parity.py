@@ -1,0 +1,166 @@
+"""GPU parity: per-k-mer states of the CUDA path (through the C ABI) equal the
+oracle's, bit for bit, keyed by canonical k-mer."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import cf1_rs_b200 as cg
+from oracle import oracle as o
+from tests.gpu_util import assert_parity, gpu_run, sort_by_key
+from tests.inputs import random_records
+
+pytestmark = pytest.mark.gpu
+
+KS = [1, 3, 5, 7, 9, 15, 21, 31, 33, 45, 61, 63]
+
+
+@pytest.mark.parametrize("mode", ["bbhash", "learned"])
+@pytest.mark.parametrize("k", KS)
+def test_edge_case_records(k, mode):
+    recs = random_records(1000 + k, k, n_records=60, max_len=4000)
+    seq, off = o.concat_records(recs)
+    g, _ = assert_parity(seq, off, k, mode=mode, num_bins=16, track_short_seqs=True)
+    g.close()
+
+
+@pytest.mark.parametrize("k", [31, 63])
+@pytest.mark.parametrize("mode", ["bbhash", "learned"])
+def test_batched_mode(k, mode):
+    recs = random_records(77 + k, k, n_records=200, max_len=6000)
+    seq, off = o.concat_records(recs)
+    assert_parity(seq, off, k, mode=mode, batched=True, num_bins=64)[0].close()
+
+
+@pytest.mark.parametrize("bins", [1, 2, 7, 128, 4096])
+def test_bin_counts(bins):
+    recs = random_records(5, 31, n_records=80, max_len=5000)
+    seq, off = o.concat_records(recs)
+    g, _ = assert_parity(seq, off, 31, num_bins=bins)
+    assert 1 <= g.stats()["n_bins"] <= bins
+    g.close()
+
+
+@pytest.mark.parametrize("tile", [1024, 2048, 4096])
+def test_superkmers_match_spec(tile):
+    k = 31
+    recs = random_records(11, k, n_records=50, max_len=8000)
+    seq, off = o.concat_records(recs)
+    g, ref = assert_parity(seq, off, k, sk_tile=tile, num_bins=32)
+    # the device concatenates records of >= k bases, one placeholder after each
+    cat = b"".join(r + b"N" for r in recs if len(r) >= k)
+    pos, n, _ = o.superkmers(np.frombuffer(cat, np.uint8), k, tile)
+    s = g.stats()
+    assert s["n_superkmers"] == len(pos)
+    assert s["n_kmer_occurrences"] == int(n.sum()) == ref.n_occ
+    g.close()
+
+
+@pytest.mark.parametrize("mode", ["bbhash", "learned"])
+@pytest.mark.parametrize("k", [31, 63])
+def test_query_state_words_and_host_image(k, mode):
+    recs = random_records(21, k, n_records=40, max_len=5000)
+    seq, off = o.concat_records(recs)
+    g, ref = assert_parity(seq, off, k, mode=mode, num_bins=32)
+    keys, st = g.dump_states()
+    slots = g.query(keys)
+    n = g.total_kmers()
+    assert np.array_equal(np.sort(slots), np.arange(n, dtype=np.uint64))
+    words = g.states()
+    assert len(words) == (n + 11) // 12
+    from_words = (words[slots // 12] >> (5 * (slots % 12)).astype(np.uint64)) & np.uint64(31)
+    assert np.array_equal(from_words.astype(np.uint8), st)
+    img = g.export_mphf()
+    assert np.array_equal(cg.host_query(img, keys), slots)
+    g.close()
+
+
+def test_short_seqs_and_fasta():
+    k = 31
+    recs = [b"ACGT" * 5, b"ACGTTGCA" * 10, b"A" * 30, b"", b"GATTACA" * 20]
+    names = ["short1 desc", "long1", "short2\tx", "empty", "long2"]
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "in.fa")
+        with open(p, "w") as f:
+            for nm, r in zip(names, recs):
+                f.write(">" + nm + "\n")
+                s = r.decode()
+                for i in range(0, len(s), 7):
+                    f.write(s[i:i + 7] + "\n")
+        g = cg.Cf1Gpu(k=k, track_short_seqs=True)
+        g.add_fasta(p)
+        g.run()
+        assert g.short_seqs() == [("short1", 20), ("short2", 30), ("empty", 0)]
+        seq, off = o.concat_records(recs)
+        ref = o.run(k, seq, off)
+        keys, st = sort_by_key(*g.dump_states())
+        assert np.array_equal(keys, ref.keys) and np.array_equal(st, ref.states)
+        g.close()
+
+
+def test_deterministic_repeat_runs():
+    recs = random_records(3, 31, n_records=100, max_len=8000)
+    seq, off = o.concat_records(recs)
+    g = gpu_run(seq, off, 31, num_bins=64)
+    w1 = g.states().copy()
+    g.upload()
+    g.run_resident()
+    w2 = g.states()
+    assert np.array_equal(w1, w2)
+    g.close()
+
+
+@pytest.mark.parametrize("mode", ["bbhash", "learned"])
+def test_workload1_full_size(mode):
+    x = cg.SynthInput(1)
+    g, _ = assert_parity(x.seq, x.offsets, 31, mode=mode, num_bins=128)
+    g.close()
+
+
+@pytest.mark.parametrize("cfg,scale,k,flags", [
+    (2, 0.05, 31, dict(track_short_seqs=True)),
+    (3, 0.1, 31, dict()),
+    (4, 0.01, 63, dict()),
+    (5, 0.005, 31, dict(num_bins=256)),
+])
+@pytest.mark.parametrize("mode", ["bbhash", "learned"])
+def test_scaled_workloads(cfg, scale, k, flags, mode):
+    x = cg.SynthInput(cfg, scale=scale)
+    kw = dict(num_bins=128)
+    kw.update(flags)
+    g, _ = assert_parity(x.seq, x.offsets, k, mode=mode, **kw)
+    g.close()
+
+
+# ---- learned index: gradients against the CPU oracle, gain of the network ----
+def test_learned_gradients_match_cpu():
+    rng = np.random.default_rng(0)
+    for trial in range(5):
+        params = rng.normal(0, 0.7, 49).astype(np.float32)
+        n = int(rng.integers(1, 3000))
+        x = rng.random(n).astype(np.float32)
+        t = np.sort(rng.random(n)).astype(np.float32)
+        loss_g, grad_g = cg.learned_grad(params, x, t)
+        loss_c, grad_c = o.mlp_grad(params, x, t)
+        # fp32 device accumulation vs fp64 CPU: relative 1e-4 of the gradient scale
+        scale = max(1e-6, float(np.abs(grad_c).max()))
+        assert abs(loss_g - loss_c) <= 1e-4 * max(1.0, loss_c)
+        assert np.abs(grad_g - grad_c).max() <= 1e-4 * scale
+
+
+def test_learned_network_gain():
+    """The trained root shrinks the search windows of the index without it."""
+    x = cg.SynthInput(5, scale=0.005)
+    res = {}
+    for steps in (-1, 0):  # -1: identity root (no network), 0: default training
+        g = cg.Cf1Gpu(k=31, num_bins=64, mode="learned", learned_train_steps=steps, learned_max_err=1 << 30)
+        g.add_records(x.seq, x.offsets)
+        g.run()
+        g.verify_bijection()
+        res[steps] = (g.learned_stats(), sort_by_key(*g.dump_states()), g.stats())
+        g.close()
+    untrained, trained = res[-1][0], res[0][0]
+    assert trained["train_loss"] < untrained["train_loss"]
+    assert trained["mean_window"] < untrained["mean_window"]
+    assert np.array_equal(res[-1][1][0], res[0][1][0]) and np.array_equal(res[-1][1][1], res[0][1][1])
