@@ -223,9 +223,10 @@ class Cf1Gpu:
         return {n: getattr(s, n) for n in _STAT_U + _STAT_D}
 
     def learned_stats(self) -> dict:
-        out = (C.c_double * 3)()
+        out = (C.c_double * 5)()
         self._check(lib().cf1gpu_learned_stats(self.h, out))
-        return dict(mean_err=out[0], mean_window=out[1], train_loss=out[2])
+        return dict(mean_err=out[0], mean_window=out[1], train_loss=out[2], max_err_all=int(out[3]),
+                    judge_miss_bins=int(out[4]))
 
     def total_kmers(self) -> int:
         return int(lib().cf1gpu_total_kmers(self.h))

@@ -165,15 +165,13 @@ uint64_t d2h_u64(const uint64_t *p, cudaStream_t s) {
 
 template <class KeyT>
 BBHashBuild<KeyT>::~BBHashBuild() {
-  clear();
+  for (DevBuf *b : A) delete b;
+  for (DevBuf *b : R) delete b;
 }
 
 template <class KeyT>
 void BBHashBuild<KeyT>::clear() {
-  for (DevBuf *b : A) delete b;
-  for (DevBuf *b : R) delete b;
-  A.clear();
-  R.clear();
+  nwords.clear();
   levels = 0;
   bytes = 0;
 }
@@ -228,11 +226,13 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     CF1_LAUNCH_CHECK();
     exclusive_scan_u64(cnt, woff, nbins, scan_tmp_, s);
     uint64_t nw = d2h_u64(woff + nbins, s);
-    DevBuf *Ab = new DevBuf(), *Rb = new DevBuf();
-    A.push_back(Ab);
-    R.push_back(Rb);
-    uint64_t *Al = Ab->get<uint64_t>(nw);
-    uint64_t *Rl = Rb->get<uint64_t>(nw + 1);
+    if (A.size() <= l) {
+      A.push_back(new DevBuf());
+      R.push_back(new DevBuf());
+    }
+    nwords.push_back(nw);
+    uint64_t *Al = A[l]->get<uint64_t>(nw);
+    uint64_t *Rl = R[l]->get<uint64_t>(nw + 1);
     uint64_t *C = C_.get<uint64_t>(nw);
     uint32_t *pc = pc_.get<uint32_t>(nw);
     bytes += nw * 16 + 8;
@@ -288,7 +288,7 @@ BBView BBHashBuild<KeyT>::view() const {
 
 template <class KeyT>
 uint64_t BBHashBuild<KeyT>::level_words(uint32_t l) const {
-  return l < A.size() ? A[l]->cap / 8 : 0;
+  return l < nwords.size() ? nwords[l] : 0;
 }
 
 template struct BBHashBuild<uint64_t>;

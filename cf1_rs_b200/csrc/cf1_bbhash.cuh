@@ -6,7 +6,10 @@ namespace cf1 {
 
 template <class KeyT>
 struct BBHashBuild {
-  std::vector<DevBuf *> A, R;  // per level: bit array, rank prefix (words + 1)
+  // per level: bit array, rank prefix (words + 1); kept across builds and
+  // grown on demand, so a rebuild allocates nothing once sizes settle
+  std::vector<DevBuf *> A, R;
+  std::vector<uint64_t> nwords;  // words of each level in use
   uint32_t levels = 0, nbins = 0;
   uint64_t bytes = 0;
 

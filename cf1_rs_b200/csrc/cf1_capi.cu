@@ -243,9 +243,9 @@ int cf1gpu_mphf_host_query(const void *image, size_t bytes, const uint64_t *keys
   }
 }
 
-int cf1gpu_learned_stats(const cf1gpu_ctx *c, double out3[3]) {
-  if (!c || !out3) return CF1GPU_ERR_INVALID_ARG;
-  cf1::learned_summary(c, out3);
+int cf1gpu_learned_stats(const cf1gpu_ctx *c, double out5[5]) {
+  if (!c || !out5) return CF1GPU_ERR_INVALID_ARG;
+  cf1::learned_summary(c, out5);
   return CF1GPU_OK;
 }
 

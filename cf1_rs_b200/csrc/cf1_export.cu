@@ -60,7 +60,7 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   off = align8(off + (uint64_t)NL * sizeof(LevelEntry));
   std::vector<LevelEntry> lev(NL);
   for (uint32_t l = 0; l < NL; l++) {
-    uint64_t nw = be.bb.A[l]->cap / 8;
+    uint64_t nw = be.bb.level_words(l);
     lev[l].nwords = nw;
     lev[l].a_off = off;
     off = align8(off + nw * 8);

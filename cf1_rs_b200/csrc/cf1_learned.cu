@@ -9,7 +9,16 @@
 // A query evaluates the root, the leaf's line, and searches the sorted keys
 // in [pred - err, pred + err].  A judge pass queries every key; a bin with a
 // key outside its window, or with err above the threshold, is served by
-// BBHash instead.  Before training the root is the identity (y = x), which
+// BBHash instead.
+//
+// The hidden units are clipped ReLUs, clamp(w1 x + b1, 0, 1): a sum of
+// bounded non-decreasing ramps can follow any non-decreasing CDF, concave
+// ones included (canonical k-mers are denser at small values).  Training
+// projects the weights of both layers onto [0, inf) after every step.  With
+// non-negative weights every rounded fma and the clamp are non-decreasing,
+// so root(x) -- and the leaf index -- is non-decreasing in the key: the keys
+// routed to a leaf are one contiguous run of ranks, and a leaf's error bound
+// only measures how far the run bends from its line.  Before training the root is the identity (y = x), which
 // is the same index without the network: the comparison of the two is
 // reported in the stats.
 #include <cmath>
@@ -30,15 +39,15 @@ constexpr uint32_t LT_MAX_SAMPLES = 4096;
 constexpr int H = LI_HIDDEN;
 
 // Adds one sample's MSE term (weight `scale`) and its gradient to g.
-// Parameter layout: w1[0,H) b1[H,2H) w2[2H,3H) b2[3H].
+// Parameter layout: w1[0,H) b1[H,2H) w2[2H,3H) b2[3H]; hidden units are
+// clipped ReLUs clamp(w1 x + b1, 0, 1) (li_root_eval).
 CF1_HD void mlp_accumulate(const float *P, float x, float t, float scale, float *g, float &loss) {
   float z[H];
   float y = P[3 * H];
 #pragma unroll
   for (int j = 0; j < H; j++) {
     z[j] = f_fma(P[j], x, P[H + j]);
-    float a = z[j] > 0.f ? z[j] : 0.f;
-    y = f_fma(P[2 * H + j], a, y);
+    y = f_fma(P[2 * H + j], li_act(z[j]), y);
   }
   float e = y - t;
   loss += e * e * scale;
@@ -46,22 +55,71 @@ CF1_HD void mlp_accumulate(const float *P, float x, float t, float scale, float 
   g[3 * H] += dy;
 #pragma unroll
   for (int j = 0; j < H; j++) {
-    float a = z[j] > 0.f ? z[j] : 0.f;
-    g[2 * H + j] += dy * a;
-    float dz = z[j] > 0.f ? dy * P[2 * H + j] : 0.f;
+    g[2 * H + j] += dy * li_act(z[j]);
+    float dz = (z[j] > 0.f && z[j] < 1.f) ? dy * P[2 * H + j] : 0.f;
     g[j] += dz * x;
     g[H + j] += dz;
   }
 }
 
-// Identity initialisation: hidden unit j is relu(x - j/H); only unit 0 feeds
-// the output with weight 1, so root(x) = x for x in [0, 1].
+// Identity initialisation: hidden unit j ramps from 0 to 1 over
+// x in [j/H, (j+1)/H] (w1 = H, b1 = -j) and feeds the output with 1/H, so
+// root(x) = x on [0, 1] -- the index without a trained network.
 CF1_HD float init_param(int p) {
-  if (p < H) return 1.f;
-  if (p < 2 * H) return -(float)(p - H) / (float)H;
-  if (p == 2 * H) return 1.f;
+  if (p < H) return (float)H;
+  if (p < 2 * H) return -(float)(p - H);
+  if (p < 3 * H) return 1.f / (float)H;
   return 0.f;
 }
+
+// Trained parameters Q (2H+1): knot logits theta[H], output weights w2[H],
+// output bias b2.  The first layer is derived from the knots: widths
+// d = softmax(theta), knots t_j = sum_{i<j} d_i, w1_j = 1/d_j,
+// b1_j = -t_j/d_j, so unit j ramps over [t_j, t_j + d_j] and the ramps tile
+// [0, 1] without gaps (a gap would be a flat stretch of the root, sending
+// every key in it to one leaf).
+constexpr int LI_NQ = 2 * H + 1;
+
+// P (the MLP's w1 b1 w2 b2) from Q; d and t kept for the chain rule.
+CF1_D void derive_params(const float *Q, float *P, float *d, float *t) {
+  float m = Q[0];
+  for (int j = 1; j < H; j++) m = fmaxf(m, Q[j]);
+  float s = 0.f;
+  for (int j = 0; j < H; j++) {
+    d[j] = expf(Q[j] - m);
+    s += d[j];
+  }
+  float acc = 0.f;
+  for (int j = 0; j < H; j++) {
+    d[j] = d[j] / s;
+    t[j] = acc;
+    acc += d[j];
+    P[j] = 1.f / d[j];
+    P[H + j] = -t[j] / d[j];
+    P[2 * H + j] = Q[H + j];
+  }
+  P[3 * H] = Q[2 * H];
+}
+
+// dL/dQ from dL/dP (chain rule through w1 = 1/d, b1 = -t/d, the knot sums
+// and the softmax).
+CF1_D void grad_q(const float *G, const float *d, const float *t, float *GQ) {
+  float gd[H];
+  for (int j = 0; j < H; j++) gd[j] = -G[j] / (d[j] * d[j]) + G[H + j] * t[j] / (d[j] * d[j]);
+  float acc = 0.f;  // t_j = sum_{i<j} d_i: d_i collects dL/dt_j of every j > i
+  for (int j = H - 1; j >= 0; j--) {
+    gd[j] += acc;
+    acc += -G[H + j] / d[j];
+  }
+  float dot = 0.f;
+  for (int j = 0; j < H; j++) dot += d[j] * gd[j];
+  for (int j = 0; j < H; j++) GQ[j] = d[j] * (gd[j] - dot);
+  for (int j = 0; j < H; j++) GQ[H + j] = G[2 * H + j];
+  GQ[2 * H] = G[3 * H];
+}
+
+// Adam step size per group: logits O(1), output weights O(1/H).
+CF1_D float lr_scale_q(int q) { return q < H ? 1.f : 1.f / (float)H; }
 
 // Block reduction of the NPARAM gradient sums and the loss into red/sl.
 CF1_D void reduce_grads(float *g, float loss, float (*red)[LI_NPARAM + 1]) {
@@ -80,7 +138,7 @@ __global__ void __launch_bounds__(LT_BLOCK) li_train_kernel(const KeyT *keys, co
                                                            int k, int steps, float lr, uint32_t max_samples,
                                                            float *loss_out) {
   __shared__ float sx[LT_MAX_SAMPLES], st[LT_MAX_SAMPLES];
-  __shared__ float P[LI_NPARAM], M1[LI_NPARAM], M2[LI_NPARAM];
+  __shared__ float P[LI_NPARAM], Q[LI_NQ], GQ[LI_NQ], M1[LI_NQ], M2[LI_NQ], sd[H], stk[H];
   __shared__ float red[LT_NW][LI_NPARAM + 1];
   __shared__ float s_loss;
   const uint32_t b = blockIdx.x;
@@ -101,12 +159,14 @@ __global__ void __launch_bounds__(LT_BLOCK) li_train_kernel(const KeyT *keys, co
     sx[i] = f_mul(u64_to_f(h - hmin), inv);
     st[i] = (float)((double)r / (double)n);
   }
-  if (tid < LI_NPARAM) {
-    P[tid] = init_param(tid);
+  if (tid < LI_NQ) {
+    Q[tid] = tid < H ? 0.f : (tid < 2 * H ? 1.f / (float)H : 0.f);  // identity root
     M1[tid] = 0.f;
     M2[tid] = 0.f;
   }
   if (tid == 0) s_loss = 0.f;
+  __syncthreads();
+  if (tid == 0) derive_params(Q, P, sd, stk);
   __syncthreads();
   const float scale = S ? 1.f / (float)S : 0.f;
   const float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
@@ -119,23 +179,55 @@ __global__ void __launch_bounds__(LT_BLOCK) li_train_kernel(const KeyT *keys, co
     for (uint32_t i = tid; i < S; i += LT_BLOCK) mlp_accumulate(P, sx[i], st[i], scale, g, loss);
     reduce_grads(g, loss, red);
     __syncthreads();
-    if (tid < LI_NPARAM) {
-      float G = 0.f;
-      for (int w = 0; w < LT_NW; w++) G += red[w][tid];
-      b1t *= beta1;
-      b2t *= beta2;
-      M1[tid] = beta1 * M1[tid] + (1.f - beta1) * G;
-      M2[tid] = beta2 * M2[tid] + (1.f - beta2) * G * G;
-      float mh = M1[tid] / (1.f - b1t), vh = M2[tid] / (1.f - b2t);
-      P[tid] -= lr * mh / (sqrtf(vh) + eps);
-    }
-    if (tid == LI_NPARAM) {
+    if (tid == 0) {
+      float G[LI_NPARAM];
+      for (int p = 0; p < LI_NPARAM; p++) {
+        float v = 0.f;
+        for (int w = 0; w < LT_NW; w++) v += red[w][p];
+        G[p] = v;
+      }
+      grad_q(G, sd, stk, GQ);
       float l = 0.f;
       for (int w = 0; w < LT_NW; w++) l += red[w][LI_NPARAM];
       s_loss = l;
     }
     __syncthreads();
+    if (tid < LI_NQ) {
+      float G = GQ[tid];
+      b1t *= beta1;
+      b2t *= beta2;
+      M1[tid] = beta1 * M1[tid] + (1.f - beta1) * G;
+      M2[tid] = beta2 * M2[tid] + (1.f - beta2) * G * G;
+      float mh = M1[tid] / (1.f - b1t), vh = M2[tid] / (1.f - b2t);
+      float nq = Q[tid] - lr * lr_scale_q(tid) * mh / (sqrtf(vh) + eps);
+      // projection onto w2 >= 0 (w1 = 1/d > 0 already): non-decreasing root
+      if (tid >= H && tid < 2 * H && nq < 0.f) nq = 0.f;
+      Q[tid] = nq;
+    }
+    __syncthreads();
+    if (tid == 0) derive_params(Q, P, sd, stk);
+    __syncthreads();
   }
+  // Output fold: an affine map with a positive slope sends the bin's smallest
+  // key to 0 and its largest to just below 1, so the leaves cover the keys.
+  if (tid == 0 && n) {
+    LIRoot tmp;
+    for (int j = 0; j < H; j++) {
+      tmp.w1[j] = P[j];
+      tmp.b1[j] = P[H + j];
+      tmp.w2[j] = P[2 * H + j];
+    }
+    tmp.b2 = P[3 * H];
+    tmp.hmin = hmin;
+    tmp.inv_range = inv;
+    float y0 = li_root_eval(tmp, li_x(tmp, hmin)), y1 = li_root_eval(tmp, li_x(tmp, hmax));
+    if (y1 > y0) {
+      float a = 0.99999905f / (y1 - y0);
+      for (int j = 0; j < H; j++) P[2 * H + j] *= a;
+      P[3 * H] = a * P[3 * H] - a * y0;
+    }
+  }
+  __syncthreads();
   // final loss with the trained parameters
   {
     float g[LI_NPARAM];
@@ -412,6 +504,8 @@ void LearnedBuild<KeyT>::build(const KeyT *keys, const uint64_t *dist_off, uint3
   std::vector<LIRoot> r2(nbins);
   std::vector<unsigned long long> es(nbins);
   std::vector<float> hl(nbins);
+  std::vector<uint32_t> hmiss(nbins);
+  CF1_CUDA(cudaMemcpyAsync(hmiss.data(), miss, nbins * 4, cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaMemcpyAsync(r2.data(), roots, nbins * sizeof(LIRoot), cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaMemcpyAsync(es.data(), errsum, nbins * 8, cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaMemcpyAsync(hl.data(), loss, nbins * 4, cudaMemcpyDeviceToHost, s));
@@ -423,6 +517,8 @@ void LearnedBuild<KeyT>::build(const KeyT *keys, const uint64_t *dist_off, uint3
     if (!n) continue;
     nonempty++;
     lsum += hl[b];
+    stats.max_err_all = r2[b].max_err > stats.max_err_all ? r2[b].max_err : stats.max_err_all;
+    stats.judge_miss_bins += hmiss[b] ? 1 : 0;
     if (r2[b].use_learned) {
       stats.learned_bins++;
       stats.max_err = r2[b].max_err > stats.max_err ? r2[b].max_err : stats.max_err;

@@ -67,13 +67,12 @@ CF1_HD int64_t f_round(float x) {
 // scaled to [0, 1].
 CF1_HD float li_x(const LIRoot &r, uint64_t h) { return f_mul(u64_to_f(h - r.hmin), r.inv_range); }
 
+// Hidden activation: clipped ReLU, clamp(z, 0, 1).
+CF1_HD float li_act(float z) { return z > 0.f ? (z < 1.f ? z : 1.f) : 0.f; }
+
 CF1_HD float li_root_eval(const LIRoot &r, float x) {
   float y = r.b2;
-  for (int j = 0; j < LI_HIDDEN; j++) {
-    float z = f_fma(r.w1[j], x, r.b1[j]);
-    z = z > 0.f ? z : 0.f;
-    y = f_fma(r.w2[j], z, y);
-  }
+  for (int j = 0; j < LI_HIDDEN; j++) y = f_fma(r.w2[j], li_act(f_fma(r.w1[j], x, r.b1[j])), y);
   return y;
 }
 

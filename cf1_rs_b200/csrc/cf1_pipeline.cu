@@ -366,11 +366,13 @@ void query(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots) {
   else query_impl<uint64_t>(c, keys, n, slots);
 }
 
-void learned_summary(const cf1gpu_ctx *c, double out3[3]) {
+void learned_summary(const cf1gpu_ctx *c, double out5[5]) {
   const LearnedStats &ls = c->wide ? c->b128.li.stats : c->b64.li.stats;
-  out3[0] = ls.mean_err;
-  out3[1] = ls.mean_window;
-  out3[2] = ls.train_loss;
+  out5[0] = ls.mean_err;
+  out5[1] = ls.mean_window;
+  out5[2] = ls.train_loss;
+  out5[3] = (double)ls.max_err_all;
+  out5[4] = (double)ls.judge_miss_bins;
 }
 
 }  // namespace cf1

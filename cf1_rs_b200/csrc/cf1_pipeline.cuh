@@ -14,7 +14,7 @@ void run_resident(cf1gpu_ctx *c);
 void dump_states(cf1gpu_ctx *c, uint64_t *keys, uint8_t *states);
 void verify_bijection(cf1gpu_ctx *c);
 void query(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots);
-void learned_summary(const cf1gpu_ctx *c, double out3[3]);
+void learned_summary(const cf1gpu_ctx *c, double out5[5]);
 size_t export_mphf(cf1gpu_ctx *c, void *dst, size_t cap);
 void host_query(const void *image, size_t bytes, const uint64_t *keys, size_t n, uint64_t *slots);
 }  // namespace cf1

@@ -162,14 +162,16 @@ int cf1gpu_export_mphf(cf1gpu_ctx *ctx, void *dst, size_t *bytes);
 /* Mphf::hash on the host over an exported image (thread-safe, no device). */
 int cf1gpu_mphf_host_query(const void *image, size_t bytes, const uint64_t *keys, size_t n, uint64_t *slots);
 
-/* Learned-index statistics of the last run (learned mode): mean leaf error
- * bound and mean search window over the keys of learned bins, mean final
- * training loss over bins.  out3 = {mean_err, mean_window, train_loss}. */
-int cf1gpu_learned_stats(const cf1gpu_ctx *ctx, double out3[3]);
+/* Learned-index statistics of the last run (learned mode): out5 =
+ * {mean leaf error bound and mean search window over the keys of learned
+ * bins, mean final training loss over bins, largest leaf error over all
+ * bins, bins where the judge found a key outside its window}. */
+int cf1gpu_learned_stats(const cf1gpu_ctx *ctx, double out5[5]);
 
 /* Diagnostics: full-batch MSE loss and gradient of a learned-index root
- * (1 -> 16 ReLU -> 1, params = w1[16] b1[16] w2[16] b2) over n samples,
- * computed on `device` by the code the training kernel runs. */
+ * (1 -> 16 clipped-ReLU clamp(w1 x + b1, 0, 1) -> 1, params = w1[16] b1[16]
+ * w2[16] b2) over n samples, computed on `device` by the code the training
+ * kernel runs. */
 int cf1gpu_learned_grad(int device, const float *params, const float *x, const float *t, size_t n, float *grad,
                         float *loss);
 

@@ -906,9 +906,10 @@ void cfo_partition(const uint64_t *hist, uint32_t num_buckets, uint32_t num_bins
   partition(hist, num_buckets, num_bins, lut, bins_out);
 }
 
-// Learned-index root (1 -> H ReLU -> 1, H = 16): full-batch mean squared
-// error and its gradient in double precision, for checking the device's
-// training kernels.  params = w1[H] b1[H] w2[H] b2.
+// Learned-index root (1 -> H clipped-ReLU -> 1, H = 16; hidden unit j is
+// clamp(w1_j x + b1_j, 0, 1)): full-batch mean squared error and its gradient
+// in double precision, for checking the device's training kernels.
+// params = w1[H] b1[H] w2[H] b2.
 void cfo_mlp_grad(const float *params, const float *x, const float *t, uint64_t n, double *grad, double *loss) {
   const int H = 16;
   for (int p = 0; p < 3 * H + 1; p++) grad[p] = 0;
@@ -918,7 +919,7 @@ void cfo_mlp_grad(const float *params, const float *x, const float *t, uint64_t 
     double y = params[3 * H];
     for (int j = 0; j < H; j++) {
       z[j] = (double)params[j] * x[i] + params[H + j];
-      a[j] = z[j] > 0 ? z[j] : 0;
+      a[j] = z[j] > 0 ? (z[j] < 1 ? z[j] : 1) : 0;
       y += (double)params[2 * H + j] * a[j];
     }
     double e = y - t[i];
@@ -927,7 +928,7 @@ void cfo_mlp_grad(const float *params, const float *x, const float *t, uint64_t 
     grad[3 * H] += dy;
     for (int j = 0; j < H; j++) {
       grad[2 * H + j] += dy * a[j];
-      double dz = z[j] > 0 ? dy * params[2 * H + j] : 0;
+      double dz = (z[j] > 0 && z[j] < 1) ? dy * params[2 * H + j] : 0;
       grad[j] += dz * x[i];
       grad[H + j] += dz;
     }
