@@ -314,7 +314,9 @@ def gpu_arm(args):
                 "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "peak_kind": peak_kind,
                 "traffic": traffic.get("dram_bytes_per_launch_scaled") if traffic else None,
                 "algorithmic_bytes": b4}
-    # whole phases 1-4 (algorithmic bytes of SURVEY-style accounting)
+    # whole phases 1-4: input read once, records written + read, keys
+    # written + read by the sort, distinct keys written and read by the MPHF
+    # build, plus the classification bytes above
     s_bins = 8.0 * s["n_superkmers"]
     b14 = 0.25 * L + 2 * s_bins + 2 * w * n_occ + 2 * w * n_dist + b4
     pipe = {"achieved": b14 / (head["ms_per_step"] / 1e3) / 1e9, "unit": "GB/s", "algorithmic_bytes": b14,

@@ -226,7 +226,7 @@ class Cf1Gpu:
         out = (C.c_double * 5)()
         self._check(lib().cf1gpu_learned_stats(self.h, out))
         return dict(mean_err=out[0], mean_window=out[1], train_loss=out[2], max_err_all=int(out[3]),
-                    judge_miss_bins=int(out[4]))
+                    verify_miss_bins=int(out[4]))
 
     def total_kmers(self) -> int:
         return int(lib().cf1gpu_total_kmers(self.h))

@@ -7,7 +7,7 @@
 //   leaves: per leaf a line through its first and last key's (key, rank);
 //           err = max |prediction - rank| over the keys the root sends there.
 // A query evaluates the root, the leaf's line, and searches the sorted keys
-// in [pred - err, pred + err].  A judge pass queries every key; a bin with a
+// in [pred - err, pred + err].  A verification pass queries every key; a bin with a
 // key outside its window, or with err above the threshold, is served by
 // BBHash instead.
 //
@@ -381,9 +381,9 @@ __global__ void __launch_bounds__(LT_BLOCK) li_decide_kernel(const uint64_t *dis
   }
 }
 
-// The judge: every key of a learned bin must come back as its own rank.
+// Verification: every key of a learned bin must come back as its own rank.
 template <class KeyT>
-__global__ void __launch_bounds__(LT_BLOCK) li_judge_kernel(const KeyT *keys, const uint64_t *dist_off,
+__global__ void __launch_bounds__(LT_BLOCK) li_verify_kernel(const KeyT *keys, const uint64_t *dist_off,
                                                            const uint32_t *tile_off, uint32_t nbins, LIView v,
                                                            uint32_t *miss) {
   const uint32_t t = blockIdx.x;
@@ -496,7 +496,7 @@ void LearnedBuild<KeyT>::build(const KeyT *keys, const uint64_t *dist_off, uint3
   CF1_LAUNCH_CHECK();
   uint32_t *miss = lfirst;  // reuse: one flag per bin
   CF1_CUDA(cudaMemsetAsync(miss, 0, nbins * 4, s));
-  li_judge_kernel<KeyT><<<ub, LT_BLOCK, 0, s>>>(keys, dist_off, tile_off, nbins, view(k), miss);
+  li_verify_kernel<KeyT><<<ub, LT_BLOCK, 0, s>>>(keys, dist_off, tile_off, nbins, view(k), miss);
   CF1_LAUNCH_CHECK();
   li_fixup_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(roots, miss, sel, nbins);
   CF1_LAUNCH_CHECK();
@@ -518,7 +518,7 @@ void LearnedBuild<KeyT>::build(const KeyT *keys, const uint64_t *dist_off, uint3
     nonempty++;
     lsum += hl[b];
     stats.max_err_all = r2[b].max_err > stats.max_err_all ? r2[b].max_err : stats.max_err_all;
-    stats.judge_miss_bins += hmiss[b] ? 1 : 0;
+    stats.verify_miss_bins += hmiss[b] ? 1 : 0;
     if (r2[b].use_learned) {
       stats.learned_bins++;
       stats.max_err = r2[b].max_err > stats.max_err ? r2[b].max_err : stats.max_err;

@@ -17,7 +17,7 @@ struct LearnedOpts {
 struct LearnedStats {
   uint64_t learned_bins = 0, fallback_bins = 0, max_err = 0, leaves = 0, bytes = 0;
   uint64_t max_err_all = 0;     // largest leaf error over every non-empty bin
-  uint64_t judge_miss_bins = 0; // bins where some key fell outside its window
+  uint64_t verify_miss_bins = 0; // bins where some key fell outside its window
   double mean_err = 0;         // mean leaf error bound over keys of learned bins
   double mean_window = 0;      // mean search window (2*err+1) over keys of learned bins
   double train_loss = 0;       // mean final training loss over bins

@@ -372,7 +372,7 @@ void learned_summary(const cf1gpu_ctx *c, double out5[5]) {
   out5[1] = ls.mean_window;
   out5[2] = ls.train_loss;
   out5[3] = (double)ls.max_err_all;
-  out5[4] = (double)ls.judge_miss_bins;
+  out5[4] = (double)ls.verify_miss_bins;
 }
 
 }  // namespace cf1

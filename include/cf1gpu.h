@@ -95,7 +95,7 @@ typedef struct cf1gpu_stats {
   double ms_phase1;            /* pack + minimizer histogram + partition */
   double ms_phase2;            /* super k-mer routing */
   double ms_phase3_sort;       /* k-mer expansion + per-bin sort + unique */
-  double ms_phase3_mphf;       /* MPHF construction (+ bijection judge) */
+  double ms_phase3_mphf;       /* MPHF construction (+ bijection check) */
   double ms_phase4;            /* classification */
   double ms_total;             /* device time of phases 1-4 (excludes h2d) */
   double ms_classify_kernel;   /* the classification kernel alone */
@@ -165,7 +165,7 @@ int cf1gpu_mphf_host_query(const void *image, size_t bytes, const uint64_t *keys
 /* Learned-index statistics of the last run (learned mode): out5 =
  * {mean leaf error bound and mean search window over the keys of learned
  * bins, mean final training loss over bins, largest leaf error over all
- * bins, bins where the judge found a key outside its window}. */
+ * bins, bins where verification found a key outside its window}. */
 int cf1gpu_learned_stats(const cf1gpu_ctx *ctx, double out5[5]);
 
 /* Diagnostics: full-batch MSE loss and gradient of a learned-index root

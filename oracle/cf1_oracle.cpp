@@ -1,7 +1,8 @@
 // cf1 oracle -- TEST INFRASTRUCTURE ONLY.
 //
-// A CPU restatement of the cf1-rs k-mer state path (phases 1-4) used as the
-// checker for the CUDA library and as the timed CPU baseline ("port").  Only
+// A CPU restatement of the cf1-rs k-mer state path (phases 1-4) that the
+// CUDA library's results are compared against, and the timed CPU baseline
+// ("port").  Only
 // tests, the smoke check and the bench's CPU-baseline / reference arm load it.
 // The product library never links, loads or calls anything in this file.
 //
