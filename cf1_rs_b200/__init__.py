@@ -24,7 +24,9 @@ LIB_PATH = os.path.join(_HERE, "libcf1gpu.so")
 SYNTH_PATH = os.path.join(_HERE, "libcf1synth.so")
 
 OK = 0
-ERR_INVALID_ARG, ERR_OOM, ERR_CUDA, ERR_DEVICE_TIMEOUT, ERR_BIJECTION, ERR_QUEUE_OVERRUN, ERR_STATE, ERR_IO = range(-1, -9, -1)
+ERR_INVALID_ARG, ERR_OOM, ERR_CUDA, ERR_DEVICE_TIMEOUT, ERR_BIJECTION, ERR_QUEUE_OVERRUN, ERR_STATE, ERR_IO, \
+    ERR_TOO_LARGE = range(-1, -10, -1)
+NOALLOC_MAX_BASES = 1 << 20
 MPHF_BBHASH, MPHF_LEARNED = 0, 1
 
 
@@ -69,6 +71,7 @@ EXPORTED = [
     "cf1gpu_total_kmers", "cf1gpu_copy_states", "cf1gpu_query", "cf1gpu_dump_states", "cf1gpu_verify_bijection",
     "cf1gpu_short_seq_count", "cf1gpu_short_seq", "cf1gpu_export_mphf", "cf1gpu_mphf_host_query",
     "cf1gpu_learned_stats", "cf1gpu_learned_grad", "cf1gpu_last_error", "cf1gpu_destroy", "cf1gpu_version",
+    "cf1gpu_distinct_kmers_noalloc",
 ]
 
 
@@ -109,8 +112,18 @@ def lib():
     L.cf1gpu_destroy.argtypes = [vp]
     L.cf1gpu_destroy.restype = None
     L.cf1gpu_version.restype = C.c_char_p
+    L.cf1gpu_distinct_kmers_noalloc.argtypes = [C.c_int, C.c_uint32, vp, C.c_size_t, vp, C.c_size_t, vp, vp]
     _lib = L
     return L
+
+
+def distinct_kmers_noalloc(d_seq: int, length: int, k: int, d_keys_out: int, out_cap: int, d_n_out: int,
+                           stream: int = 0, device: int = 0) -> int:
+    """Distinct canonical k-mers of one device-resident record without any
+    device allocation by the library (cf1gpu_distinct_kmers_noalloc).  All
+    pointers are device addresses the caller owns; returns the status code."""
+    return lib().cf1gpu_distinct_kmers_noalloc(device, k, d_seq, length, d_keys_out, out_cap, d_n_out,
+                                               stream or None)
 
 
 def _p(a, t):

@@ -31,6 +31,7 @@ SOURCES = [
     "cf1_export.cu",
     "cf1_fasta.cu",
     "cf1_capi.cu",
+    "cf1_noalloc.cu",
 ]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []
 

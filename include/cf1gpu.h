@@ -52,6 +52,7 @@ extern "C" {
 #define CF1GPU_ERR_QUEUE_OVERRUN (-6) /* a device work queue or buffer overflowed */
 #define CF1GPU_ERR_STATE (-7)         /* call made in the wrong order */
 #define CF1GPU_ERR_IO (-8)            /* input file could not be read */
+#define CF1GPU_ERR_TOO_LARGE (-9)     /* input exceeds a fixed-capacity entry point's limit */
 
 /* MPHF backends (the reference uses ph::fmph, src/mphf.rs:16). */
 #define CF1GPU_MPHF_BBHASH 0   /* per-bin GPU BBHash (gamma 2) */
@@ -174,6 +175,31 @@ int cf1gpu_learned_stats(const cf1gpu_ctx *ctx, double out5[5]);
  * kernel runs. */
 int cf1gpu_learned_grad(int device, const float *params, const float *x, const float *t, size_t n, float *grad,
                         float *loss);
+
+/* Distinct canonical k-mers of one record, for callers that must not
+ * allocate device memory.  No counterpart in the reference (it has no
+ * device memory at all): this exists for host applications that own the
+ * device memory pool and give the library only their buffers, and for code
+ * running where a cudaMalloc would synchronise the device or is not allowed.
+ * It allocates nothing: its scratch is a fixed array inside the library
+ * (17 MiB, kept by every GPU that loads it until the process exits).
+ *
+ * d_seq: the record's ASCII bases in device memory, len <= 1048576 (1 Mi)
+ * bases -- longer records return CF1GPU_ERR_TOO_LARGE without running.
+ * k: odd, 1..31.  d_keys_out: device buffer of out_cap u64, out_cap >=
+ * len - k + 1; receives the distinct canonical k-mers of the record's
+ * placeholder-free windows, ascending (the phase-3 key set of
+ * src/mphf.rs:323-363 for this record).  d_n_out: device u64, their count.
+ * Work is queued on `stream` (a cudaStream_t, NULL = default stream);
+ * outputs are valid once the stream has run it.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with the device current; make that first call
+ * before any stream capture.  Calls share the array and it keeps the last
+ * call's contents (each call clears what it needs): calls that overlap on
+ * the GPU race and corrupt each other, so serialise them. */
+int cf1gpu_distinct_kmers_noalloc(int device, uint32_t k, const uint8_t *d_seq, size_t len, uint64_t *d_keys_out,
+                                  size_t out_cap, uint64_t *d_n_out, void *stream);
 
 const char *cf1gpu_last_error(const cf1gpu_ctx *ctx);
 void cf1gpu_destroy(cf1gpu_ctx *ctx);
