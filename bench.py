@@ -344,6 +344,8 @@ def gpu_arm(args):
         "forms": {f: {"value": v["value"], "ms_per_step": v["ms_per_step"],
                       "ms_classify_kernel": v["ms_classify_kernel"], "phases_ms": v["phases_ms"],
                       "bbhash_levels": int(v["stats"]["bbhash_levels"]), "mphf_bytes": int(v["stats"]["mphf_bytes"]),
+                      "sort": ("lsd" if v["stats"]["sort_msd_bits"] == 2**64 - 1
+                               else f"msd{v['stats']['sort_msd_bits']}"),
                       "learned_bins": int(v["stats"]["learned_bins"]), "fallback_bins": int(v["stats"]["fallback_bins"]),
                       "learned": v["learned"]} for f, v in forms.items()},
     }

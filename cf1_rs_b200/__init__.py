@@ -41,19 +41,19 @@ class Opts(C.Structure):
         ("k", C.c_uint32), ("num_bins", C.c_uint32), ("device", C.c_int32), ("mphf_mode", C.c_uint32),
         ("batched", C.c_uint32), ("track_short_seqs", C.c_uint32), ("tuner_cache_path", C.c_char_p),
         ("learned_max_err", C.c_uint32), ("learned_train_steps", C.c_int32), ("learned_leaf_size", C.c_uint32),
-        ("sk_tile", C.c_uint32), ("reserved", C.c_uint32 * 4),
+        ("sk_tile", C.c_uint32), ("sort_mode", C.c_uint32), ("reserved", C.c_uint32 * 3),
     ]
 
 
 _STAT_U = ["n_bases", "n_records", "n_short", "n_superkmers", "n_kmer_occurrences", "n_distinct", "n_bins",
            "n_state_words", "mphf_bytes", "bbhash_levels", "learned_bins", "fallback_bins", "learned_max_err",
-           "classify_cas_retries", "n_kernel_launches"]
+           "classify_cas_retries", "n_kernel_launches", "sort_msd_bits"]
 _STAT_D = ["ms_h2d", "ms_phase1", "ms_phase2", "ms_phase3_sort", "ms_phase3_mphf", "ms_phase4", "ms_total",
            "ms_classify_kernel"]
 
 
 class Stats(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in _STAT_U] + [("reserved_u", C.c_uint64 * 5)] + \
+    _fields_ = [(n, C.c_uint64) for n in _STAT_U] + [("reserved_u", C.c_uint64 * 4)] + \
                [(n, C.c_double) for n in _STAT_D] + [("reserved_d", C.c_double * 4)]
 
 
@@ -160,7 +160,8 @@ class Cf1Gpu:
 
     def __init__(self, k: int = 31, num_bins: int = 128, device: int = 0, mode: str = "bbhash",
                  batched: bool = False, track_short_seqs: bool = False, learned_max_err: int = 0,
-                 learned_train_steps: int = 0, learned_leaf_size: int = 0, sk_tile: int = 0):
+                 learned_train_steps: int = 0, learned_leaf_size: int = 0, sk_tile: int = 0,
+                 sort_mode: str = "msd"):
         L = lib()
         o = Opts()
         L.cf1gpu_default_opts(C.byref(o))
@@ -172,6 +173,7 @@ class Cf1Gpu:
         o.learned_train_steps = learned_train_steps
         o.learned_leaf_size = learned_leaf_size
         o.sk_tile = sk_tile
+        o.sort_mode = {"msd": 0, "lsd": 1}[sort_mode]
         h = C.c_void_p()
         st = L.cf1gpu_create(C.byref(o), C.byref(h))
         if st != OK:

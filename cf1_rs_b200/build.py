@@ -24,6 +24,7 @@ SOURCES = [
     "cf1_util.cu",
     "cf1_phase12.cu",
     "cf1_phase3_sort.cu",
+    "cf1_msdsort.cu",
     "cf1_bbhash.cu",
     "cf1_learned.cu",
     "cf1_phase4.cu",

@@ -91,6 +91,7 @@ int cf1gpu_create(const cf1gpu_opts *opts, cf1gpu_ctx **out) {
     if (opts->learned_train_steps > 0) c->learned.train_steps = opts->learned_train_steps;
     if (opts->learned_train_steps < 0) c->learned.train_steps = -1;
     if (opts->learned_leaf_size) c->learned.leaf_size = opts->learned_leaf_size;
+    c->force_lsd = opts->sort_mode == 1;
   });
   if (st != CF1GPU_OK) {
     delete c;

@@ -8,6 +8,7 @@
 #include "cf1_bbhash.cuh"
 #include "cf1_internal.cuh"
 #include "cf1_learned.cuh"
+#include "cf1_msdsort.cuh"
 
 namespace cf1 {
 
@@ -28,6 +29,7 @@ struct PinnedBuf {
 template <class KeyT>
 struct Backend {
   SortScratch<KeyT> sort;
+  MsdScratch msd;
   BBHashBuild<KeyT> bb;
   LearnedBuild<KeyT> li;
 };
@@ -68,6 +70,8 @@ struct cf1gpu_ctx {
 
   // results of the last run
   uint64_t n_super = 0, n_occ = 0, n_distinct = 0, n_bins_eff = 0, cas_retries = 0;
+  int msd_bits = 0;        // top bits split on by the MSD sort (-1: LSD path ran)
+  bool force_lsd = false;  // opts.sort_mode == 1
   uint32_t nbins = 0;
   cf1gpu_stats stats{};
 };

@@ -59,6 +59,43 @@ CF1_D T block_sum(T v, T *sm) {
   return tot;
 }
 
+// Order-preserving selection over [0, len) by a whole block: pred(i) picks
+// indices, emit(i, rank) receives each picked index with its rank among the
+// picked ones.  Each warp owns one contiguous slice and walks it 32
+// consecutive indices at a time, so consecutive lanes touch consecutive
+// elements (no shared-memory bank conflicts).  Returns the count; ends with
+// a barrier.  `sm` holds BLOCK/32 entries.
+template <int BLOCK, class Pred, class Emit>
+CF1_D uint32_t block_select(uint32_t len, Pred pred, Emit emit, uint32_t *sm) {
+  constexpr int NW = BLOCK / 32;
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  const uint32_t per = ((len + NW - 1) / NW + 31) & ~31u;
+  const uint32_t lo = warp * per, hi = lo + per < len ? lo + per : len;
+  uint32_t c = 0;
+  for (uint32_t base = lo; base < hi; base += 32) {
+    uint32_t i = base + lane;
+    c += __popc(__ballot_sync(FULL, i < hi && pred(i)));
+  }
+  if (lane == 0) sm[warp] = c;
+  __syncthreads();
+  uint32_t pre = 0, tot = 0;
+  for (int w = 0; w < NW; w++) {
+    uint32_t v = sm[w];
+    pre += (unsigned)w < warp ? v : 0;
+    tot += v;
+  }
+  const unsigned lt = lanemask_lt();
+  for (uint32_t base = lo; base < hi; base += 32) {
+    uint32_t i = base + lane;
+    bool f = i < hi && pred(i);
+    unsigned b = __ballot_sync(FULL, f);
+    if (f) emit(i, pre + __popc(b & lt));
+    pre += __popc(b);
+  }
+  __syncthreads();
+  return tot;
+}
+
 // Largest b in [0, nseg) with off[b] <= t, for nondecreasing off[0..nseg].
 template <class T>
 CF1_D uint32_t upper_segment(const T *off, uint32_t nseg, T t) {

@@ -1,0 +1,589 @@
+// Phase 3a, MSD form: sorted distinct canonical k-mers per bin.
+//
+//   1. one or two stable multisplit passes on the top P bits of the keys,
+//      segmented by bin (P chosen so a sub-bucket holds ~CAP/3 keys);
+//   2. one CTA per sub-bucket: counting sort on the next 10 bits in shared
+//      memory, insertion sort of the small buckets (bitonic sort of the whole
+//      sub-bucket if any bucket is large), adjacent-unique, distinct keys
+//      written back at the sub-bucket's start;
+//   3. a scan of the per-sub-bucket counts and a copy into the dense distinct
+//      array; a bin's first sub-bucket gives its slot offset.
+// A sub-bucket above CAP keys (long homopolymers, huge tandem arrays) makes
+// the caller fall back to the LSD path (cf1_phase3_sort.cu) for the run.
+#include "cf1_device_util.cuh"
+#include "cf1_internal.cuh"
+#include "cf1_msdsort.cuh"
+
+namespace cf1 {
+
+namespace {
+
+constexpr int MS_BLOCK = 256;
+constexpr int MS_ITEMS = 16;
+constexpr uint32_t MS_TILE = MS_BLOCK * MS_ITEMS;  // 4096 keys per pass tile
+constexpr int MS_NW = MS_BLOCK / 32;
+constexpr int CS_BLOCK = 256;
+constexpr int CS_BITS = 10;
+constexpr uint32_t CS_BUCKETS = 1u << CS_BITS;
+// Insertion sort up to this many keys per bucket.  Repeats put hundreds of
+// copies of one k-mer in a bucket; insertion sort passes over equal keys at
+// once, so large buckets of few distinct values stay cheap.
+constexpr uint32_t CS_SMALL = 512;
+constexpr uint32_t CS_DEDUP_MIN = 64;  // 64-bit sub-buckets above this size are deduplicated first
+
+template <class KeyT>
+constexpr uint32_t cs_cap() { return KOps<KeyT>::WORDS == 1 ? 8192u : 4096u; }
+
+// ---------------------------------------------------------------- multisplit pass
+template <class KeyT, int BITS>
+__global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, const uint64_t *seg_off,
+                                                           const uint32_t *tile_off, uint32_t nseg, int shift,
+                                                           uint32_t *H) {
+  constexpr uint32_t DIG = 1u << BITS;
+  __shared__ uint32_t h[DIG];
+  const uint32_t t = blockIdx.x;
+  if (t >= tile_off[nseg]) {
+    for (uint32_t d = threadIdx.x; d < DIG; d += MS_BLOCK) H[(uint64_t)t * DIG + d] = 0;
+    return;
+  }
+  for (uint32_t d = threadIdx.x; d < DIG; d += MS_BLOCK) h[d] = 0;
+  __syncthreads();
+  TileSpan sp = tile_span(seg_off, tile_off, nseg, t, MS_TILE);
+  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += MS_BLOCK)
+    atomicAdd(&h[KOps<KeyT>::digit(keys[i], shift, DIG - 1)], 1u);
+  __syncthreads();
+  for (uint32_t d = threadIdx.x; d < DIG; d += MS_BLOCK)
+    H[(uint64_t)sp.first_tile * DIG + (uint64_t)d * sp.ntiles + (t - sp.first_tile)] = h[d];
+}
+
+// Stable multisplit of one tile: warp w ranks the w-th 512-key slice of the
+// tile round by round (match_any inside a round, a running per-warp digit
+// count across rounds), a per-digit prefix over warps gives tile-local
+// positions, the tile is staged in shared memory in digit order, and each
+// digit's run is written out with consecutive threads on consecutive
+// addresses.
+template <class KeyT, int BITS>
+__global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
+                                                                 const uint32_t *tile_off, uint32_t nseg, int shift,
+                                                                 const uint64_t *Hs) {
+  constexpr uint32_t DIG = 1u << BITS;
+  extern __shared__ __align__(16) unsigned char ms_smem[];
+  KeyT *stage = reinterpret_cast<KeyT *>(ms_smem);                            // [MS_TILE]
+  uint32_t *whist = reinterpret_cast<uint32_t *>(stage + MS_TILE);           // [MS_NW][DIG]
+  uint32_t *lstart = whist + MS_NW * DIG;                                     // [DIG]
+  uint64_t *base = reinterpret_cast<uint64_t *>(lstart + DIG);                // [DIG]
+  __shared__ uint32_t sm[MS_BLOCK / 32];
+  const uint32_t t = blockIdx.x;
+  if (t >= tile_off[nseg]) return;
+  TileSpan sp = tile_span(seg_off, tile_off, nseg, t, MS_TILE);
+  const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  for (uint32_t i = tid; i < MS_NW * DIG; i += MS_BLOCK) whist[i] = 0;
+  for (uint32_t d = tid; d < DIG; d += MS_BLOCK)
+    base[d] = Hs[(uint64_t)sp.first_tile * DIG + (uint64_t)d * sp.ntiles + (t - sp.first_tile)];
+  __syncthreads();
+  const uint32_t n = (uint32_t)(sp.end - sp.start);
+  // per key: (rank in the warp's slice for its digit) << 8 | digit, or ~0
+  // for lanes past the tile; keys are read again when staged, which keeps
+  // the register count (and so the occupancy) down
+  uint32_t pk[MS_ITEMS];
+  const unsigned lt = lanemask_lt();
+  uint32_t *wh = whist + warp * DIG;
+#pragma unroll
+  for (int r = 0; r < MS_ITEMS; r++) {
+    uint32_t li = warp * (MS_ITEMS * 32) + r * 32 + lane;
+    bool act = li < n;
+    uint32_t d = act ? KOps<KeyT>::digit(in[sp.start + li], shift, DIG - 1) : 0xFFFFFFFFu;
+    unsigned peers = __match_any_sync(FULL, d);
+    unsigned leader = __ffs(peers) - 1;
+    uint32_t old = 0;
+    if (act && lane == leader) {
+      old = wh[d];
+      wh[d] = old + __popc(peers);
+    }
+    old = __shfl_sync(FULL, old, leader);
+    pk[r] = act ? ((old + __popc(peers & lt)) << 8) | d : 0xFFFFFFFFu;
+  }
+  __syncthreads();
+  // per digit: exclusive prefix over warps; tile total per digit
+  uint32_t tot_d = 0;
+  for (uint32_t d = tid; d < DIG; d += MS_BLOCK) {
+    uint32_t run = 0;
+    for (int w = 0; w < MS_NW; w++) {
+      uint32_t v = whist[w * DIG + d];
+      whist[w * DIG + d] = run;
+      run += v;
+    }
+    if (DIG == MS_BLOCK) tot_d = run;
+    else lstart[d] = run;
+  }
+  __syncthreads();
+  // tile-local start of each digit: exclusive scan over digits
+  if (DIG == MS_BLOCK) {
+    uint32_t tot;
+    uint32_t pre = block_exclusive_scan<MS_BLOCK>(tot_d, sm, tot);
+    lstart[tid] = pre;
+  } else if (tid == 0) {
+    uint32_t run = 0;
+    for (uint32_t d = 0; d < DIG; d++) {
+      uint32_t v = lstart[d];
+      lstart[d] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < MS_ITEMS; r++) {
+    if (pk[r] != 0xFFFFFFFFu) {
+      uint32_t d = pk[r] & 0xFF, li = warp * (MS_ITEMS * 32) + r * 32 + lane;
+      stage[lstart[d] + wh[d] + (pk[r] >> 8)] = in[sp.start + li];
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < n; i += MS_BLOCK) {
+    KeyT kk = stage[i];
+    uint32_t d = KOps<KeyT>::digit(kk, shift, DIG - 1);
+    out[base[d] + (i - lstart[d])] = kk;
+  }
+}
+
+// Sub-bucket starts after the last pass: sub-bucket (segment s, digit d)
+// begins at the scanned histogram entry of its first tile.
+template <int BITS>
+__global__ void ms_subbucket_kernel(const uint64_t *seg_off, const uint32_t *tile_off, uint32_t nseg,
+                                    const uint64_t *Hs, uint64_t *sb_off) {
+  constexpr uint32_t DIG = 1u << BITS;
+  uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t nsub = (uint64_t)nseg * DIG;
+  if (j > nsub) return;
+  if (j == nsub) {
+    sb_off[j] = seg_off[nseg];
+    return;
+  }
+  uint32_t s = (uint32_t)(j / DIG), d = (uint32_t)(j % DIG);
+  uint32_t ft = tile_off[s], nt = tile_off[s + 1] - ft;
+  sb_off[j] = nt ? Hs[(uint64_t)ft * DIG + (uint64_t)d * nt] : seg_off[s];
+}
+
+// ---------------------------------------------------------------- chunk sort
+template <class KeyT>
+CF1_D void cs_swap_if(KeyT &a, KeyT &b, bool up) {
+  if ((b < a) == up) {
+    KeyT t = a;
+    a = b;
+    b = t;
+  }
+}
+
+// Replaces T[a, a+n) by its distinct keys (any order) through an
+// open-addressing set in shared memory; returns their count, or ~0u when
+// they do not fit in three quarters of the set.  Every probe sequence is
+// bounded by the set size.
+CF1_D uint32_t cs_hash_dedup(uint64_t *T, uint64_t a, uint64_t n, uint64_t *S, uint32_t cap, uint32_t *s_cnt,
+                             uint32_t *sm) {
+  const unsigned tid = threadIdx.x;
+  const uint64_t EMPTY = ~0ull;  // above every key (keys use at most 62 bits)
+  uint32_t tsize = 64;           // a power of two >= 2n, at most cap
+  while (tsize < cap && (uint64_t)tsize < 2 * n) tsize <<= 1;
+  for (uint32_t i = tid; i < tsize; i += CS_BLOCK) S[i] = EMPTY;
+  if (tid == 0) *s_cnt = 0;
+  __syncthreads();
+  const uint32_t limit = tsize / 4 * 3;
+  for (uint64_t i = tid; i < n; i += CS_BLOCK) {
+    if (*reinterpret_cast<volatile uint32_t *>(s_cnt) > limit) break;
+    uint64_t key = T[a + i];
+    uint32_t h = (uint32_t)KOps<uint64_t>::hash(key, 0x5851F42D4C957F2Dull) & (tsize - 1);
+    for (uint32_t probe = 0; probe < tsize; probe++) {
+      unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long *>(S + h), EMPTY, key);
+      if (old == EMPTY) {
+        atomicAdd(s_cnt, 1u);
+        break;
+      }
+      if (old == key) break;
+      h = (h + 1) & (tsize - 1);
+    }
+  }
+  __syncthreads();
+  uint32_t d = *s_cnt;
+  if (d > limit) return ~0u;
+  // compact the occupied slots to T[a, a+d)
+  block_select<CS_BLOCK>(
+      tsize, [&](uint32_t i) { return S[i] != EMPTY; }, [&](uint32_t i, uint32_t r) { T[a + r] = S[i]; }, sm);
+  return d;
+}
+
+// Bucket of a key for the shared-memory counting sort: the bits
+// [s1, s1+b1) minus off1, followed by the bits [s2, s2+b2).  A plain
+// sub-bucket uses the next bits below its prefix (b2 = 0); a chunk of pieces
+// of a split sub-bucket uses the piece index relative to the chunk's first
+// piece, then further bits.
+struct CsDigit {
+  int s1, b1, s2, b2;
+  uint32_t off1;
+  template <class KeyT>
+  CF1_D uint32_t operator()(const KeyT &k) const {
+    uint32_t d1 = b1 ? KOps<KeyT>::digit(k, s1, (1u << b1) - 1) - off1 : 0u;
+    uint32_t d2 = b2 ? KOps<KeyT>::digit(k, s2, (1u << b2) - 1) : 0u;
+    return (d1 << b2) | d2;
+  }
+};
+
+struct CsShared {
+  uint32_t *hist, *cur, *sm;
+  int *big;
+};
+
+// Sorted distinct keys of src[0, m) (m <= CAP, keys all in [0, 1024) buckets
+// of dig) into out[0, tot); returns tot.  src is fully read into shared
+// memory before out is written, so they may overlap.  All threads call it.
+template <class KeyT>
+CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &dig, KeyT *S, const CsShared &sh,
+                                    KeyT *out) {
+  constexpr uint32_t CAP = cs_cap<KeyT>();
+  const unsigned tid = threadIdx.x;
+  for (uint32_t i = tid; i < CS_BUCKETS; i += CS_BLOCK) sh.hist[i] = 0;
+  if (tid == 0) *sh.big = 0;
+  __syncthreads();
+  for (uint32_t i = tid; i < m; i += CS_BLOCK) atomicAdd(&sh.hist[dig(src[i])], 1u);
+  __syncthreads();
+  {
+    constexpr int PER = CS_BUCKETS / CS_BLOCK;
+    uint32_t v[PER], s = 0;
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      v[q] = sh.hist[tid * PER + q];
+      s += v[q];
+    }
+    uint32_t tot;
+    uint32_t pre = block_exclusive_scan<CS_BLOCK>(s, sh.sm, tot);
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      sh.hist[tid * PER + q] = pre;
+      sh.cur[tid * PER + q] = pre;
+      pre += v[q];
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < m; i += CS_BLOCK) {
+    KeyT key = src[i];
+    S[atomicAdd(&sh.cur[dig(key)], 1u)] = key;
+  }
+  __syncthreads();
+  // insertion sort per bucket (bucket b spans [hist[b], cur[b]))
+  for (uint32_t b = tid; b < CS_BUCKETS; b += CS_BLOCK) {
+    uint32_t lo = sh.hist[b], hi = sh.cur[b];
+    if (hi - lo > CS_SMALL) {
+      *sh.big = 1;
+      continue;
+    }
+    for (uint32_t i = lo + 1; i < hi; i++) {
+      KeyT x = S[i];
+      uint32_t q = i;
+      while (q > lo && x < S[q - 1]) {
+        S[q] = S[q - 1];
+        q--;
+      }
+      S[q] = x;
+    }
+  }
+  __syncthreads();
+  if (*sh.big) {  // bitonic sort of the whole range, padded to a power of two
+    uint32_t P2 = 1;
+    while (P2 < m) P2 <<= 1;
+    for (uint32_t i = m + tid; i < P2; i += CS_BLOCK) S[i] = KOps<KeyT>::max_key();
+    __syncthreads();
+    for (uint32_t size = 2; size <= P2; size <<= 1) {
+      for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+        for (uint32_t i = tid; i < P2 / 2; i += CS_BLOCK) {
+          uint32_t lo = 2 * i - (i & (stride - 1));
+          cs_swap_if(S[lo], S[lo + stride], (lo & size) == 0);
+        }
+        __syncthreads();
+      }
+    }
+  }
+  // adjacent-unique
+  (void)CAP;
+  return block_select<CS_BLOCK>(
+      m, [&](uint32_t i) { return i == 0 || S[i] != S[i - 1]; }, [&](uint32_t i, uint32_t r) { out[r] = S[i]; },
+      sh.sm);
+}
+
+// Sorted distinct keys of one sub-bucket T[a, a+n), written back at a.
+// Sub-buckets above CAP keys: 64-bit keys are first reduced to one copy each
+// through a shared-memory set; if still above CAP, the sub-bucket is split on
+// its next `bits` bits into U[a, a+n) (the free ping-pong buffer), runs of
+// consecutive pieces up to CAP keys are sorted one after another, and their
+// distinct keys are appended at T[a].  Only a single piece above CAP keys
+// makes the kernel report the sub-bucket as oversized.
+template <class KeyT>
+__global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT *U, const uint64_t *sb_off,
+                                                                  uint64_t nsub, int shift, int bits, uint32_t *cnt,
+                                                                  uint32_t *oversize) {
+  constexpr uint32_t CAP = cs_cap<KeyT>();
+  extern __shared__ __align__(16) unsigned char cs_smem[];
+  KeyT *S = reinterpret_cast<KeyT *>(cs_smem);                    // [CAP]
+  uint32_t *hist = reinterpret_cast<uint32_t *>(S + CAP);         // [CS_BUCKETS]
+  uint32_t *cur = hist + CS_BUCKETS;                              // [CS_BUCKETS]
+  uint32_t *pstart = cur + CS_BUCKETS;                            // [CS_BUCKETS + 1]
+  uint16_t *cb = reinterpret_cast<uint16_t *>(pstart + CS_BUCKETS + 1);  // [CS_BUCKETS + 1]
+  __shared__ uint32_t sm[CS_BLOCK / 32];
+  __shared__ int s_big, s_nchunks, s_bad;
+  __shared__ uint32_t s_cnt;
+  const uint64_t j = blockIdx.x;
+  if (j >= nsub) return;
+  const uint64_t a = sb_off[j], n = sb_off[j + 1] - a;
+  const unsigned tid = threadIdx.x;
+  if (n == 0) {
+    if (tid == 0) cnt[j] = 0;
+    return;
+  }
+  CsShared sh{hist, cur, sm, &s_big};
+  CsDigit plain{shift, bits, 0, 0, 0u};
+  uint32_t m = (uint32_t)n;
+  // 64-bit keys: one copy of each key first.  Repeats put hundreds of copies
+  // of a k-mer in one bucket, where sorting copies would dominate the work.
+  if (n > CS_DEDUP_MIN && KOps<KeyT>::WORDS == 1) {
+    uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(T), a, n, reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
+    if (d != ~0u) m = d;
+  }
+  if (m <= CAP) {
+    uint32_t tot = cs_sort_unique_range<KeyT>(T + a, m, plain, S, sh, T + a);
+    if (tid == 0) cnt[j] = tot;
+    return;
+  }
+  // local split on the next `bits` bits into U[a, a+n)
+  const uint32_t npieces = 1u << bits, pmask = npieces - 1;
+  for (uint32_t i = tid; i <= CS_BUCKETS; i += CS_BLOCK) pstart[i] = 0;
+  __syncthreads();
+  for (uint64_t i = tid; i < n; i += CS_BLOCK) atomicAdd(&pstart[KOps<KeyT>::digit(T[a + i], shift, pmask)], 1u);
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t run = 0;
+    for (uint32_t p = 0; p < npieces; p++) {
+      uint32_t v = pstart[p];
+      pstart[p] = run;
+      run += v;
+    }
+    pstart[npieces] = run;
+    // greedy runs of consecutive pieces up to CAP keys
+    int nc = 0, bad = 0;
+    uint32_t acc = 0;
+    cb[0] = 0;
+    for (uint32_t p = 0; p < npieces; p++) {
+      uint32_t sz = pstart[p + 1] - pstart[p];
+      if (sz > CAP) {  // a piece of its own, deduplicated before sorting (64-bit keys)
+        if (KOps<KeyT>::WORDS != 1) bad = 1;
+        if (acc > 0) cb[++nc] = (uint16_t)p;
+        cb[++nc] = (uint16_t)(p + 1);
+        acc = 0;
+        continue;
+      }
+      if (acc + sz > CAP && acc > 0) {
+        cb[++nc] = (uint16_t)p;
+        acc = 0;
+      }
+      acc += sz;
+    }
+    if (acc == 0) nc--;  // the loop already closed the last run
+    cb[++nc] = (uint16_t)npieces;
+    s_nchunks = nc;
+    s_bad = bad;
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (tid == 0) {
+      cnt[j] = 0;
+      atomicOr(oversize, 1u);
+    }
+    return;
+  }
+  for (uint32_t p = tid; p < npieces; p += CS_BLOCK) cur[p] = pstart[p];
+  __syncthreads();
+  for (uint64_t i = tid; i < n; i += CS_BLOCK) {
+    KeyT key = T[a + i];
+    U[a + atomicAdd(&cur[KOps<KeyT>::digit(key, shift, pmask)], 1u)] = key;
+  }
+  __syncthreads();
+  uint32_t outc = 0;
+  for (int c = 0; c < s_nchunks; c++) {
+    uint32_t p0 = cb[c], p1 = cb[c + 1];
+    uint32_t span = p1 - p0;
+    int g = 0;
+    while ((1u << g) < span) g++;
+    int b2 = 10 - g;
+    if (b2 > shift) b2 = shift;
+    CsDigit dig{shift, bits, shift - b2, b2, p0};
+    uint32_t len = pstart[p1] - pstart[p0];
+    if (len > CS_DEDUP_MIN && KOps<KeyT>::WORDS == 1) {
+      uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(U), a + pstart[p0], len,
+                                 reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
+      if (d != ~0u) len = d;  // (a failed pass leaves U untouched)
+      if (len > CAP) {
+        if (tid == 0) {
+          cnt[j] = 0;
+          atomicOr(oversize, 1u);
+        }
+        return;
+      }
+    }
+    outc += cs_sort_unique_range<KeyT>(U + a + pstart[p0], len, dig, S, sh, T + a + outc);
+  }
+  if (tid == 0) cnt[j] = outc;
+}
+
+// One warp per sub-bucket: copy its distinct keys to the dense array.
+template <class KeyT>
+__global__ void cs_compact_kernel(const KeyT *T, const uint64_t *sb_off, const uint32_t *cnt, const uint64_t *out_off,
+                                  uint64_t nsub, KeyT *dist) {
+  uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (j >= nsub) return;
+  uint32_t c = cnt[j];
+  uint64_t a = sb_off[j], o = out_off[j];
+  for (uint32_t i = lane_id(); i < c; i += 32) dist[o + i] = T[a + i];
+}
+
+__global__ void cs_bin_off_kernel(const uint64_t *out_off, uint32_t nbins, uint64_t per_bin, uint64_t *dist_off) {
+  uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b <= nbins) dist_off[b] = out_off[(uint64_t)b * per_bin];
+}
+
+template <class KeyT, int BITS>
+void ms_pass(const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift,
+             MsdScratch &sc, cudaStream_t s) {
+  constexpr uint32_t DIG = 1u << BITS;
+  uint32_t ub = (uint32_t)(ceil_div(n, MS_TILE) + nseg);
+  uint32_t *tile_off = sc.tile_off.get<uint32_t>(nseg + 1);
+  segment_tiles(seg_off, nseg, MS_TILE, tile_off, s);
+  uint32_t *H = sc.hist.get<uint32_t>((uint64_t)ub * DIG);
+  uint64_t *Hs = sc.hscan.get<uint64_t>((uint64_t)ub * DIG + 1);
+  ms_hist_kernel<KeyT, BITS><<<ub, MS_BLOCK, 0, s>>>(in, seg_off, tile_off, nseg, shift, H);
+  CF1_LAUNCH_CHECK();
+  exclusive_scan_u32(H, Hs, (uint64_t)ub * DIG, sc.scan_tmp, s);
+  size_t smem = MS_TILE * sizeof(KeyT) + (MS_NW + 1) * DIG * sizeof(uint32_t) + DIG * sizeof(uint64_t);
+  CF1_CUDA(cudaFuncSetAttribute(ms_scatter_kernel<KeyT, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ms_scatter_kernel<KeyT, BITS><<<ub, MS_BLOCK, smem, s>>>(in, out, seg_off, tile_off, nseg, shift, Hs);
+  CF1_LAUNCH_CHECK();
+}
+
+template <class KeyT>
+void ms_pass_bits(int bits, const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift,
+                  MsdScratch &sc, cudaStream_t s) {
+  switch (bits) {
+    case 1: ms_pass<KeyT, 1>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    case 2: ms_pass<KeyT, 2>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    case 3: ms_pass<KeyT, 3>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    case 4: ms_pass<KeyT, 4>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    case 5: ms_pass<KeyT, 5>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    case 6: ms_pass<KeyT, 6>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    case 7: ms_pass<KeyT, 7>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    case 8: ms_pass<KeyT, 8>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    default: throw Error(-1, "MSD pass width must be 1..8 bits");
+  }
+}
+
+template <int BITS>
+void subbuckets(const uint64_t *seg_off, const uint32_t *tile_off, uint32_t nseg, const uint64_t *Hs,
+                uint64_t *sb_off, cudaStream_t s) {
+  uint64_t nsub = (uint64_t)nseg << BITS;
+  ms_subbucket_kernel<BITS><<<(unsigned)ceil_div(nsub + 1, 256), 256, 0, s>>>(seg_off, tile_off, nseg, Hs, sb_off);
+  CF1_LAUNCH_CHECK();
+}
+
+void subbuckets_bits(int bits, const uint64_t *seg_off, const uint32_t *tile_off, uint32_t nseg, const uint64_t *Hs,
+                     uint64_t *sb_off, cudaStream_t s) {
+  switch (bits) {
+    case 1: subbuckets<1>(seg_off, tile_off, nseg, Hs, sb_off, s); break;
+    case 2: subbuckets<2>(seg_off, tile_off, nseg, Hs, sb_off, s); break;
+    case 3: subbuckets<3>(seg_off, tile_off, nseg, Hs, sb_off, s); break;
+    case 4: subbuckets<4>(seg_off, tile_off, nseg, Hs, sb_off, s); break;
+    case 5: subbuckets<5>(seg_off, tile_off, nseg, Hs, sb_off, s); break;
+    case 6: subbuckets<6>(seg_off, tile_off, nseg, Hs, sb_off, s); break;
+    case 7: subbuckets<7>(seg_off, tile_off, nseg, Hs, sb_off, s); break;
+    case 8: subbuckets<8>(seg_off, tile_off, nseg, Hs, sb_off, s); break;
+    default: throw Error(-1, "MSD pass width must be 1..8 bits");
+  }
+}
+
+}  // namespace
+
+template <class KeyT>
+int msd_prefix_bits(uint64_t max_bin_keys) {
+  const uint64_t target = cs_cap<KeyT>() / 2;
+  int p = 0;
+  while (p < 16 && (max_bin_keys >> p) > target) p++;
+  return p;
+}
+
+template <class KeyT>
+bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
+                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s) {
+  // passes on the top P bits: P1 then P2 (P2 may be 0)
+  const int P1 = P > 8 ? (P + 1) / 2 : P, P2 = P - P1;
+  KeyT *T = keys;
+  uint64_t nsub = (uint64_t)nbins << P;
+  uint64_t *sb_off = sc.sb_off.get<uint64_t>(nsub + 1);
+  if (P == 0) {
+    CF1_CUDA(cudaMemcpyAsync(sb_off, seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+  } else if (n) {
+    ms_pass_bits<KeyT>(P1, keys, alt, n, seg_off, nbins, key_bits - P1, sc, s);
+    const uint64_t *seg2 = seg_off;
+    uint32_t nseg2 = nbins;
+    if (P2) {
+      // segments of pass 2: (bin, first digit), from pass 1's scanned histogram
+      uint64_t *sb1 = sc.sb_off1.get<uint64_t>(((uint64_t)nbins << P1) + 1);
+      subbuckets_bits(P1, seg_off, sc.tile_off.as<uint32_t>(), nbins, sc.hscan.as<uint64_t>(), sb1, s);
+      nseg2 = (uint32_t)((uint64_t)nbins << P1);
+      seg2 = sb1;
+      ms_pass_bits<KeyT>(P2, alt, keys, n, seg2, nseg2, key_bits - P1 - P2, sc, s);
+      T = keys;
+    } else {
+      T = alt;
+    }
+    subbuckets_bits(P2 ? P2 : P1, seg2, sc.tile_off.as<uint32_t>(), nseg2, sc.hscan.as<uint64_t>(), sb_off, s);
+  } else {
+    CF1_CUDA(cudaMemsetAsync(sb_off, 0, (nsub + 1) * sizeof(uint64_t), s));
+  }
+  uint32_t *cnt = sc.cnt.get<uint32_t>(nsub + 1);
+  uint32_t *over = sc.flag.get<uint32_t>(1);
+  CF1_CUDA(cudaMemsetAsync(over, 0, 4, s));
+  int rest = key_bits - P;
+  int bits = rest < CS_BITS ? rest : CS_BITS;
+  int shift = rest - bits;
+  if (bits <= 0) {
+    bits = 1;  // every key of a sub-bucket is equal: one bucket
+    shift = 0;
+  }
+  // S, hist, cur, pstart (u32) and the chunk bounds (u16)
+  size_t smem = cs_cap<KeyT>() * sizeof(KeyT) + (3 * CS_BUCKETS + 1) * sizeof(uint32_t) +
+                (CS_BUCKETS + 1) * sizeof(uint16_t);
+  CF1_CUDA(cudaFuncSetAttribute(cs_sort_unique_kernel<KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  KeyT *U = T == keys ? alt : keys;
+  if (nsub) {
+    cs_sort_unique_kernel<KeyT><<<(unsigned)nsub, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift,
+                                                                      rest > 0 ? bits : 0, cnt, over);
+    CF1_LAUNCH_CHECK();
+  }
+  uint32_t h_over = 0;
+  CF1_CUDA(cudaMemcpyAsync(&h_over, over, 4, cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  if (h_over) return false;
+  uint64_t *out_off = sc.out_off.get<uint64_t>(nsub + 1);
+  exclusive_scan_u32(cnt, out_off, nsub, sc.scan_tmp, s);
+  if (nsub) {
+    cs_compact_kernel<KeyT><<<(unsigned)ceil_div(nsub * 32, 256), 256, 0, s>>>(T, sb_off, cnt, out_off, nsub, dist);
+    CF1_LAUNCH_CHECK();
+  }
+  cs_bin_off_kernel<<<(unsigned)ceil_div(nbins + 1, 256), 256, 0, s>>>(out_off, nbins, 1ull << P, dist_off);
+  CF1_LAUNCH_CHECK();
+  return true;
+}
+
+#define CF1_INST(KT)                                                                                              \
+  template int msd_prefix_bits<KT>(uint64_t);                                                                     \
+  template bool msd_sort_unique<KT>(KT *, KT *, uint64_t, const uint64_t *, uint32_t, int, int, KT *, uint64_t *, \
+                                    MsdScratch &, cudaStream_t);
+CF1_INST(uint64_t)
+CF1_INST(Key2)
+#undef CF1_INST
+
+}  // namespace cf1

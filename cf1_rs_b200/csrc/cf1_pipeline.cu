@@ -149,10 +149,23 @@ void run_impl(cf1gpu_ctx *c) {
   uint64_t *seg = c->d_seg.get<uint64_t>(B + 1);
   seg_gather_kernel<<<(unsigned)ceil_div(B + 1, 256), 256, 0, s>>>(kpre, rec_off, B, seg);
   CF1_LAUNCH_CHECK();
-  segmented_sort<KeyT>(keys, NO, seg, B, 2 * k, be.sort, s);
   KeyT *dist = c->d_dist.get<KeyT>(NO + 1);
   uint64_t *dist_off = c->d_dist_off.get<uint64_t>(B + 1);
-  segmented_unique<KeyT>(keys, NO, seg, B, dist, dist_off, be.sort, s);
+  std::vector<uint64_t> hseg(B + 1);
+  CF1_CUDA(cudaMemcpyAsync(hseg.data(), seg, (B + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  uint64_t max_bin = 0;
+  for (uint32_t b = 0; b < B; b++) max_bin = std::max(max_bin, hseg[b + 1] - hseg[b]);
+  KeyT *alt = be.sort.alt.template get<KeyT>(NO + 1);
+  int P = c->force_lsd ? -1 : msd_prefix_bits<KeyT>(max_bin);
+  bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist, dist_off, be.msd, s);
+  c->msd_bits = done ? P : -1;
+  if (!done) {  // a sub-bucket overflowed shared memory: expand again, LSD path
+    if (P >= 0)
+      launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[4] : nullptr, &sm->err, pctas, s);
+    segmented_sort<KeyT>(keys, NO, seg, B, 2 * k, be.sort, s);
+    segmented_unique<KeyT>(keys, NO, seg, B, dist, dist_off, be.sort, s);
+  }
   CF1_CUDA(cudaMemcpyAsync(&c->n_distinct, dist_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaStreamSynchronize(s));
   CF1_CUDA(cudaEventRecord(c->ev[3], s));
@@ -211,6 +224,7 @@ void run_impl(cf1gpu_ctx *c) {
   st.learned_max_err = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED ? be.li.stats.max_err : 0;
   st.classify_cas_retries = c->cas_retries;
   st.n_kernel_launches = g_launches.load() - launches0;
+  st.sort_msd_bits = c->msd_bits >= 0 ? (uint64_t)c->msd_bits : ~0ull;
   st.ms_phase1 = elapsed(c->ev[0], c->ev[1]);
   st.ms_phase2 = elapsed(c->ev[1], c->ev[2]);
   st.ms_phase3_sort = elapsed(c->ev[2], c->ev[3]);

@@ -72,7 +72,9 @@ typedef struct cf1gpu_opts {
   int32_t learned_train_steps; /* learned index root training steps: 0 = default (300), < 0 = no training (identity root) */
   uint32_t learned_leaf_size; /* learned index target keys per leaf (0 = default 32) */
   uint32_t sk_tile;           /* k-mer positions per minimizer tile: 1024, 2048 or 4096 (0 = tuner / default) */
-  uint32_t reserved[4];
+  uint32_t sort_mode;         /* phase-3 sort: 0 = per-bin MSD + shared-memory sort (LSD when a sub-bucket
+                                 overflows), 1 = segmented LSD radix sort only */
+  uint32_t reserved[3];
 } cf1gpu_opts;
 
 typedef struct cf1gpu_stats {
@@ -91,7 +93,8 @@ typedef struct cf1gpu_stats {
   uint64_t learned_max_err;    /* largest leaf error bound among learned bins */
   uint64_t classify_cas_retries; /* failed CAS attempts in phase 4 */
   uint64_t n_kernel_launches;  /* kernels this library launched during the last run */
-  uint64_t reserved_u[5];
+  uint64_t sort_msd_bits;      /* top bits the MSD sort split bins on; UINT64_MAX when the LSD path ran */
+  uint64_t reserved_u[4];
   double ms_h2d;               /* host->device copy of the input */
   double ms_phase1;            /* pack + minimizer histogram + partition */
   double ms_phase2;            /* super k-mer routing */

@@ -42,6 +42,40 @@ def test_bin_counts(bins):
     g.close()
 
 
+@pytest.mark.parametrize("sort_mode", ["msd", "lsd"])
+@pytest.mark.parametrize("k", [15, 31, 33, 63])
+def test_sort_modes(k, sort_mode):
+    recs = random_records(300 + k, k, n_records=80, max_len=6000)
+    seq, off = o.concat_records(recs)
+    g, _ = assert_parity(seq, off, k, num_bins=8, sort_mode=sort_mode)
+    bits = g.stats()["sort_msd_bits"]
+    assert (bits == 2**64 - 1) if sort_mode == "lsd" else (bits < 64)
+    g.close()
+
+
+@pytest.mark.parametrize("k", [31, 63])
+def test_oversized_subbucket(k):
+    # a long homopolymer and a tandem repeat put tens of thousands of copies of
+    # a few k-mers in one sub-bucket, beyond the shared-memory sort's capacity:
+    # 64-bit keys are deduplicated through a shared-memory set first and stay
+    # on the MSD path; 128-bit keys fall back to the LSD path
+    recs = random_records(9, k, n_records=20, max_len=3000) + [b"A" * 30000, b"ACGT" * 9000]
+    seq, off = o.concat_records(recs)
+    g, _ = assert_parity(seq, off, k, num_bins=4)
+    bits = g.stats()["sort_msd_bits"]
+    assert (bits < 64) if k <= 32 else (bits == 2**64 - 1)
+    g.close()
+
+
+@pytest.mark.parametrize("bins", [1, 2])
+def test_msd_two_passes(bins):
+    # 5 M keys in one or two bins: the MSD split takes two multisplit passes
+    x = cg.SynthInput(1)
+    g, _ = assert_parity(x.seq, x.offsets, 31, num_bins=bins)
+    assert g.stats()["sort_msd_bits"] > 8
+    g.close()
+
+
 @pytest.mark.parametrize("tile", [1024, 2048, 4096])
 def test_superkmers_match_spec(tile):
     k = 31
