@@ -269,6 +269,10 @@ def gpu_arm(args):
     head_name = max(forms, key=lambda f: forms[f]["value"])
     head = forms[head_name]
     s = head["stats"]
+    for f in forms.values():  # one context at a time on the device
+        if f is not head and f["ctx"] is not None:
+            f["ctx"].close()
+            f["ctx"] = None
     # ---- end to end through the C ABI from host buffers
     e2e = None
     if not args.no_e2e:

@@ -65,6 +65,7 @@ struct cf1gpu_ctx {
   // device buffers
   cf1::DevBuf d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
       d_keys, d_dist, d_dist_off, d_states, d_scan, d_seen, d_qin, d_qout, d_queue;
+  uint64_t rec_cap_hint = 0;  // phase-1 record list size of the last run
   cf1::Backend<uint64_t> b64;
   cf1::Backend<cf1::Key2> b128;
 

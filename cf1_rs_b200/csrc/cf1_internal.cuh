@@ -88,19 +88,20 @@ struct SuperkmerArgs {
   uint32_t tile;          // k-mer positions per tile
   uint64_t n_tiles;
   uint32_t *tile_counter; // persistent mode: atomic work queue (zeroed); nullptr = one CTA per tile
-  // histogram mode
-  uint32_t *hist;         // [65536] super k-mers per bucket
-  unsigned long long *n_kmers;  // valid k-mer windows
-  // emit mode
-  const uint16_t *lut;    // bucket -> bin
-  uint32_t num_bins;
-  const uint64_t *rec_off;      // [num_bins+1]
-  uint32_t *bin_cursor;         // [num_bins] zeroed
-  uint64_t *records;
+  uint32_t *hist;         // [65536] super k-mers per bucket (zeroed)
+  unsigned long long *n_kmers;    // valid k-mer windows (zeroed)
+  uint64_t *rec_tmp;      // unordered super k-mers (rec_pack with bin 0) ...
+  uint16_t *rec_bucket;   // ... and their histogram buckets
+  unsigned long long *rec_count;  // records produced (zeroed); only the first rec_cap are stored
+  uint64_t rec_cap;
   uint32_t *err;
 };
-void launch_superkmer_hist(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s);
-void launch_superkmer_emit(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s);
+// Phase 1: minimizer histogram + unordered super k-mer list.
+void launch_superkmer_scan(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s);
+// Phase 2: route the list into per-bin ranges rec_off[0..num_bins] of records.
+void launch_bin_scatter(const uint64_t *rec_tmp, const uint16_t *rec_bucket, uint64_t n, const uint16_t *lut,
+                        uint32_t num_bins, const uint64_t *rec_off, uint32_t *cursor, uint64_t *records, uint32_t *err,
+                        cudaStream_t s);
 // Greedy partition of the histogram (src/minimizer.rs:116-172) into the
 // bucket->bin table, plus per-bin record offsets rec_off[0..num_bins].
 void launch_partition(const uint32_t *hist, uint32_t num_bins, uint16_t *lut, uint64_t *rec_off, uint32_t *n_bins_eff,

@@ -22,7 +22,7 @@ constexpr int MS_BLOCK = 256;
 constexpr int MS_ITEMS = 16;
 constexpr uint32_t MS_TILE = MS_BLOCK * MS_ITEMS;  // 4096 keys per pass tile
 constexpr int MS_NW = MS_BLOCK / 32;
-constexpr int CS_BLOCK = 256;
+constexpr int CS_BLOCK = 512;  // 16 warps: shared memory allows 2 CTAs per SM
 constexpr int CS_BITS = 10;
 constexpr uint32_t CS_BUCKETS = 1u << CS_BITS;
 // Insertion sort up to this many keys per bucket.  Repeats put hundreds of

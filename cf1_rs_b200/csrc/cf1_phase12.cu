@@ -73,23 +73,23 @@ __global__ void pack_kernel(const uint8_t *ascii, uint64_t L, uint64_t *W, uint6
 //   2. sliding-window minimum over w by log2(w) doubling passes;
 //   3. a k-mer is valid when its window holds no placeholder; a super k-mer
 //      starts at a valid k-mer whose predecessor in the tile is invalid or has
-//      another minimizer, and runs while the minimizer stays the same.
-template <int BLOCK, int ITEMS, bool EMIT>
+//      another minimizer, and runs while the minimizer stays the same;
+//   4. each super k-mer counts once in the histogram of its minimizer bucket
+//      (phase 1) and is written once, with its bucket, to an unordered record
+//      list that phase 2 routes by bin (a tile reserves its slots with one
+//      atomic add).
+template <int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
   constexpr uint32_t T = BLOCK * ITEMS;
   extern __shared__ uint64_t dyn[];
   uint64_t *bufA = dyn;
   uint64_t *bufB = dyn + T + 64;
-  uint32_t *s_cnt = reinterpret_cast<uint32_t *>(dyn + 2 * (T + 64));
-  uint32_t *s_base = s_cnt + (EMIT ? a.num_bins : 0);
   __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_base;
+  __shared__ uint32_t sm[BLOCK / 32];
   const int k = a.k, m = a.m, w = a.w;
   const unsigned tid = threadIdx.x;
   const uint64_t NK = a.L - (uint64_t)k + 1;
-  if (EMIT) {
-    for (uint32_t b = tid; b < a.num_bins; b += BLOCK) s_cnt[b] = 0;
-  }
-  __syncthreads();
   uint64_t tile = blockIdx.x;
   unsigned long long my_kmers = 0;
   for (;;) {
@@ -127,71 +127,101 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
     }
     __syncthreads();
     const uint64_t *z = dst;
-    uint32_t rp[ITEMS], rn[ITEMS], rb[ITEMS], rl[ITEMS];
+    uint32_t rn[ITEMS], rbk[ITEMS];
+    uint32_t mine = 0;
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
       uint32_t p = i * BLOCK + tid;
       rn[i] = 0;
-      rb[i] = 0;
-      rl[i] = 1;
-      rp[i] = p;
+      rbk[i] = 0;
       if (p < nk) {
         uint64_t v = z[p];
         if (v != ~0ull && (p == 0 || z[p - 1] != v)) {
           uint32_t e = p + 1;
           while (e < nk && z[e] == v) e++;
           rn[i] = e - p;
-          uint32_t bucket = mix_bucket((uint32_t)v);
-          if (!EMIT) {
-            atomicAdd(&a.hist[bucket], 1u);
-            my_kmers += rn[i];
-          } else {
-            uint32_t bin = a.lut[bucket];
-            rb[i] = bin;
-            rl[i] = atomicAdd(&s_cnt[bin], 1u);
-          }
+          rbk[i] = mix_bucket((uint32_t)v);
+          atomicAdd(&a.hist[rbk[i]], 1u);
+          my_kmers += rn[i];
+          mine++;
         }
       }
     }
-    if (EMIT) {
-      __syncthreads();
+    uint32_t tot;
+    uint32_t pre = block_exclusive_scan<BLOCK>(mine, sm, tot);
+    if (tid == 0) s_base = atomicAdd(a.rec_count, (unsigned long long)tot);
+    __syncthreads();
+    uint64_t o = s_base + pre;
 #pragma unroll
-      for (int i = 0; i < ITEMS; i++)
-        if (rn[i] && rl[i] == 0) s_base[rb[i]] = atomicAdd(&a.bin_cursor[rb[i]], s_cnt[rb[i]]);
-      __syncthreads();
-#pragma unroll
-      for (int i = 0; i < ITEMS; i++) {
-        if (rn[i]) {
-          uint64_t idx = a.rec_off[rb[i]] + s_base[rb[i]] + rl[i];
-          if (idx < a.rec_off[rb[i] + 1]) a.records[idx] = rec_pack(P0 + rp[i], rn[i], rb[i]);
-          else atomicOr(a.err, (uint32_t)DEV_OVERFLOW);
+    for (int i = 0; i < ITEMS; i++) {
+      if (rn[i]) {
+        if (o < a.rec_cap) {
+          a.rec_tmp[o] = rec_pack(P0 + i * BLOCK + tid, rn[i], 0);
+          a.rec_bucket[o] = (uint16_t)rbk[i];
         }
+        o++;
       }
-      __syncthreads();
-#pragma unroll
-      for (int i = 0; i < ITEMS; i++)
-        if (rn[i] && rl[i] == 0) s_cnt[rb[i]] = 0;
     }
     __syncthreads();
     if (!a.tile_counter) break;
   }
-  if (!EMIT) {
-    my_kmers = warp_sum(my_kmers);
-    if (lane_id() == 0 && my_kmers) atomicAdd(a.n_kmers, my_kmers);
-  }
+  my_kmers = warp_sum(my_kmers);
+  if (lane_id() == 0 && my_kmers) atomicAdd(a.n_kmers, my_kmers);
 }
 
 constexpr int SK_BLOCK = 256;
 
-template <bool EMIT>
+// Phase 2: every record of the unordered list goes to its bin's range
+// (records of a bin end up in no particular order).  A CTA takes BS_TILE
+// records, counts them per bin in shared memory, reserves each bin's slots
+// with one atomic add, and writes.
+constexpr int BS_BLOCK = 256;
+constexpr int BS_ITEMS = 16;
+__global__ void __launch_bounds__(BS_BLOCK) bin_scatter_kernel(const uint64_t *rec_tmp, const uint16_t *rec_bucket,
+                                                               uint64_t n, const uint16_t *lut, uint32_t num_bins,
+                                                               const uint64_t *rec_off, uint32_t *cursor,
+                                                               uint64_t *records, uint32_t *err) {
+  extern __shared__ uint32_t bs_smem[];
+  uint32_t *s_cnt = bs_smem;             // [num_bins]
+  uint32_t *s_base = bs_smem + num_bins;  // [num_bins]
+  const unsigned tid = threadIdx.x;
+  for (uint32_t b = tid; b < num_bins; b += BS_BLOCK) s_cnt[b] = 0;
+  __syncthreads();
+  const uint64_t r0 = (uint64_t)blockIdx.x * BS_BLOCK * BS_ITEMS;
+  uint32_t bin[BS_ITEMS], li[BS_ITEMS];
+#pragma unroll
+  for (int i = 0; i < BS_ITEMS; i++) {
+    uint64_t r = r0 + (uint64_t)i * BS_BLOCK + tid;
+    bin[i] = 0xFFFFFFFFu;
+    if (r < n) {
+      bin[i] = lut[rec_bucket[r]];
+      li[i] = atomicAdd(&s_cnt[bin[i]], 1u);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < BS_ITEMS; i++)
+    if (bin[i] != 0xFFFFFFFFu && li[i] == 0) s_base[bin[i]] = atomicAdd(&cursor[bin[i]], s_cnt[bin[i]]);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < BS_ITEMS; i++) {
+    if (bin[i] == 0xFFFFFFFFu) continue;
+    uint64_t r = r0 + (uint64_t)i * BS_BLOCK + tid;
+    uint64_t idx = rec_off[bin[i]] + s_base[bin[i]] + li[i];
+    uint64_t t = rec_tmp[r];
+    if (idx < rec_off[bin[i] + 1]) records[idx] = rec_pack(rec_pos(t), rec_n(t), bin[i]);
+    else atomicOr(err, (uint32_t)DEV_OVERFLOW);
+  }
+}
+
 void launch_sk(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
   if (a.n_tiles == 0) return;
-  size_t smem = 2 * (a.tile + 64) * sizeof(uint64_t) + (EMIT ? 2 * a.num_bins * sizeof(uint32_t) : 0);
+  size_t smem = 2 * (a.tile + 64) * sizeof(uint64_t);
   unsigned grid = persistent_ctas > 0 ? (unsigned)persistent_ctas : (unsigned)a.n_tiles;
   switch (a.tile) {
 #define CF1_SK_CASE(IT)                                                                              \
   case SK_BLOCK * IT: {                                                                            \
-    auto kern = superkmer_kernel<SK_BLOCK, IT, EMIT>;                                              \
+    auto kern = superkmer_kernel<SK_BLOCK, IT>;                                                    \
     CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
     kern<<<grid, SK_BLOCK, smem, s>>>(a);                                                          \
     break;                                                                                         \
@@ -283,11 +313,19 @@ void launch_pack(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, cu
   CF1_LAUNCH_CHECK();
 }
 
-void launch_superkmer_hist(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
-  launch_sk<false>(a, persistent_ctas, s);
+void launch_superkmer_scan(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
+  launch_sk(a, persistent_ctas, s);
 }
-void launch_superkmer_emit(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
-  launch_sk<true>(a, persistent_ctas, s);
+
+void launch_bin_scatter(const uint64_t *rec_tmp, const uint16_t *rec_bucket, uint64_t n, const uint16_t *lut,
+                        uint32_t num_bins, const uint64_t *rec_off, uint32_t *cursor, uint64_t *records, uint32_t *err,
+                        cudaStream_t s) {
+  if (n == 0) return;
+  size_t smem = 2 * num_bins * sizeof(uint32_t);
+  CF1_CUDA(cudaFuncSetAttribute(bin_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  bin_scatter_kernel<<<(unsigned)ceil_div(n, (uint64_t)BS_BLOCK * BS_ITEMS), BS_BLOCK, smem, s>>>(
+      rec_tmp, rec_bucket, n, lut, num_bins, rec_off, cursor, records, err);
+  CF1_LAUNCH_CHECK();
 }
 
 void launch_partition(const uint32_t *hist, uint32_t num_bins, uint16_t *lut, uint64_t *rec_off, uint32_t *n_bins_eff,

@@ -35,6 +35,7 @@ namespace {
 struct Small {
   unsigned long long n_kmers;
   unsigned long long cas_retries;
+  unsigned long long rec_count;
   uint32_t err;
   uint32_t n_bins_eff;
   uint32_t queues[8];
@@ -98,7 +99,6 @@ void run_impl(cf1gpu_ctx *c) {
   CF1_CUDA(cudaMemsetAsync(NM + n_nm, 0xFF, 2 * sizeof(uint64_t), s));
   launch_pack(c->d_ascii.as<uint8_t>(), L, W, NM, s);
   uint32_t *hist = c->d_hist.get<uint32_t>(NUM_BUCKETS);
-  CF1_CUDA(cudaMemsetAsync(hist, 0, NUM_BUCKETS * sizeof(uint32_t), s));
   SuperkmerArgs a{};
   a.W = W;
   a.NM = NM;
@@ -110,17 +110,35 @@ void run_impl(cf1gpu_ctx *c) {
   a.n_tiles = L >= (uint64_t)k ? ceil_div(L - k + 1, a.tile) : 0;
   a.hist = hist;
   a.n_kmers = &sm->n_kmers;
+  a.rec_count = &sm->rec_count;
   a.err = &sm->err;
   int pctas = batched ? (c->tune.persistent_ctas > 0 ? c->tune.persistent_ctas : 4 * c->num_sms) : 0;
   a.tile_counter = batched ? &sm->queues[0] : nullptr;
-  launch_superkmer_hist(a, pctas, s);
   uint16_t *lut = c->d_lut.get<uint16_t>(NUM_BUCKETS);
   uint64_t *rec_off = c->d_rec_off.get<uint64_t>(B + 1);
-  launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
+  // The record list is sized from the last run (or a quarter of the input,
+  // ~2x the density of random sequence); if it overflows, the scan reruns
+  // with the exact count.
+  // The list lives in the key buffer, which phase 3 only fills after phase 2
+  // has routed the list.
   Small hs;
-  CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
-  CF1_CUDA(cudaMemcpyAsync(&c->n_super, rec_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-  CF1_CUDA(cudaStreamSynchronize(s));
+  for (int attempt = 0;; attempt++) {
+    a.rec_cap = std::max<uint64_t>(c->rec_cap_hint, L / 4 + 1024);
+    uint8_t *rbuf = static_cast<uint8_t *>(c->d_keys.reserve(a.rec_cap * (sizeof(uint64_t) + sizeof(uint16_t))));
+    a.rec_tmp = reinterpret_cast<uint64_t *>(rbuf);
+    a.rec_bucket = reinterpret_cast<uint16_t *>(rbuf + a.rec_cap * sizeof(uint64_t));
+    CF1_CUDA(cudaMemsetAsync(hist, 0, NUM_BUCKETS * sizeof(uint32_t), s));
+    CF1_CUDA(cudaMemsetAsync(sm, 0, sizeof(Small), s));
+    launch_superkmer_scan(a, pctas, s);
+    launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
+    CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaMemcpyAsync(&c->n_super, rec_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+    if (hs.rec_count != c->n_super) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record count != histogram total");
+    if (hs.rec_count <= a.rec_cap) break;
+    if (attempt) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record list overflowed twice");
+    c->rec_cap_hint = hs.rec_count;
+  }
   c->n_occ = hs.n_kmers;
   c->n_bins_eff = hs.n_bins_eff;
   CF1_CUDA(cudaEventRecord(c->ev[1], s));
@@ -131,13 +149,7 @@ void run_impl(cf1gpu_ctx *c) {
   CF1_CUDA(cudaMemsetAsync(records, 0, (NS + 1) * sizeof(uint64_t), s));
   uint32_t *cursor = c->d_cursor.get<uint32_t>(B);
   CF1_CUDA(cudaMemsetAsync(cursor, 0, B * sizeof(uint32_t), s));
-  a.lut = lut;
-  a.num_bins = B;
-  a.rec_off = rec_off;
-  a.bin_cursor = cursor;
-  a.records = records;
-  a.tile_counter = batched ? &sm->queues[1] : nullptr;
-  launch_superkmer_emit(a, pctas, s);
+  launch_bin_scatter(a.rec_tmp, a.rec_bucket, NS, lut, B, rec_off, cursor, records, &sm->err, s);
   uint64_t *kpre = c->d_kpre.get<uint64_t>(NS + 1);
   record_kmer_prefix(records, NS, kpre, c->d_lens, c->d_scan, s);
   CF1_CUDA(cudaEventRecord(c->ev[2], s));
