@@ -283,7 +283,9 @@ class Cf1Gpu:
     def export_mphf(self) -> np.ndarray:
         need = C.c_size_t(0)
         self._check(lib().cf1gpu_export_mphf(self.h, None, C.byref(need)))
-        img = np.empty((need.value + 7) // 8, np.uint64)
+        raw = np.empty((need.value + 31) // 8, np.uint64)
+        skip = (-raw.ctypes.data % 16) // 8  # the image is 16-byte aligned
+        img = raw[skip:skip + (need.value + 7) // 8]
         size = C.c_size_t(img.nbytes)
         self._check(lib().cf1gpu_export_mphf(self.h, img.ctypes.data, C.byref(size)))
         return img

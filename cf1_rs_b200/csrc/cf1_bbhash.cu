@@ -55,7 +55,7 @@ __global__ void bb_sizes_kernel(const uint64_t *rem_off, uint32_t nbins, uint64_
 template <class KeyT>
 __global__ void __launch_bounds__(BB_BLOCK) bb_mark_kernel(const KeyT *rem, const uint64_t *rem_off,
                                                            const uint32_t *tile_off, uint32_t nbins,
-                                                           const uint64_t *woff, uint32_t level, uint64_t *A,
+                                                           const uint64_t *woff, uint32_t level, ulonglong2 *AR,
                                                            uint64_t *C) {
   const uint32_t t = blockIdx.x;
   if (t >= tile_off[nbins]) return;
@@ -66,18 +66,23 @@ __global__ void __launch_bounds__(BB_BLOCK) bb_mark_kernel(const KeyT *rem, cons
     uint64_t pos = mulhi64(KOps<KeyT>::hash(rem[i], seed), m_bits);
     uint64_t wi = w0 + (pos >> 6);
     uint64_t bit = 1ull << (pos & 63);
-    unsigned long long old = atomicOr(reinterpret_cast<unsigned long long *>(A + wi), (unsigned long long)bit);
+    unsigned long long old = atomicOr(&AR[wi].x, (unsigned long long)bit);
     if (old & bit) atomicOr(reinterpret_cast<unsigned long long *>(C + wi), (unsigned long long)bit);
   }
 }
 
-__global__ void bb_clean_kernel(uint64_t *A, const uint64_t *C, uint32_t *pc, uint64_t nw) {
+__global__ void bb_clean_kernel(ulonglong2 *AR, const uint64_t *C, uint32_t *pc, uint64_t nw) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nw) {
-    uint64_t a = A[i] & ~C[i];
-    A[i] = a;
+    uint64_t a = AR[i].x & ~C[i];
+    AR[i].x = a;
     pc[i] = (uint32_t)__popcll(a);
   }
+}
+
+__global__ void bb_rank_kernel(ulonglong2 *AR, const uint64_t *R, uint64_t nw) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nw) AR[i].y = R[i];
 }
 
 __global__ void bb_meta_kernel(const uint64_t *woff, const uint64_t *R, uint64_t *base, BBMeta *meta, uint32_t nbins) {
@@ -93,16 +98,16 @@ __global__ void bb_meta_kernel(const uint64_t *woff, const uint64_t *R, uint64_t
 }
 
 template <class KeyT>
-CF1_D bool bb_placed(const KeyT &key, uint64_t seed, uint64_t w0, uint64_t m_bits, const uint64_t *A) {
+CF1_D bool bb_placed(const KeyT &key, uint64_t seed, uint64_t w0, uint64_t m_bits, const ulonglong2 *AR) {
   uint64_t pos = mulhi64(KOps<KeyT>::hash(key, seed), m_bits);
-  return (A[w0 + (pos >> 6)] >> (pos & 63)) & 1;
+  return (AR[w0 + (pos >> 6)].x >> (pos & 63)) & 1;
 }
 
 template <class KeyT>
 __global__ void __launch_bounds__(BB_BLOCK) bb_filter_count_kernel(const KeyT *rem, const uint64_t *rem_off,
                                                                    const uint32_t *tile_off, uint32_t nbins,
                                                                    const uint64_t *woff, uint32_t level,
-                                                                   const uint64_t *A, uint32_t *tile_cnt) {
+                                                                   const ulonglong2 *A, uint32_t *tile_cnt) {
   __shared__ uint32_t sm[BB_BLOCK / 32];
   const uint32_t t = blockIdx.x;
   if (t >= tile_off[nbins]) {
@@ -122,7 +127,7 @@ template <class KeyT>
 __global__ void __launch_bounds__(BB_BLOCK) bb_filter_write_kernel(const KeyT *rem, const uint64_t *rem_off,
                                                                    const uint32_t *tile_off, uint32_t nbins,
                                                                    const uint64_t *woff, uint32_t level,
-                                                                   const uint64_t *A, const uint64_t *tile_out,
+                                                                   const ulonglong2 *A, const uint64_t *tile_out,
                                                                    KeyT *out) {
   constexpr int ITEMS = BB_TILE / BB_BLOCK;
   __shared__ uint32_t sm[BB_BLOCK / 32];
@@ -165,8 +170,7 @@ uint64_t d2h_u64(const uint64_t *p, cudaStream_t s) {
 
 template <class KeyT>
 BBHashBuild<KeyT>::~BBHashBuild() {
-  for (DevBuf *b : A) delete b;
-  for (DevBuf *b : R) delete b;
+  for (DevBuf *b : AR) delete b;
 }
 
 template <class KeyT>
@@ -213,7 +217,7 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     rem = r[0];
     roff = off0;
   }
-  std::vector<const uint64_t *> hA, hR;
+  std::vector<const ulonglong2 *> hA;
   int cur = 1;  // level l reads rem (keys, then r[cur^1]) and writes r[cur]
   uint64_t remaining = n;
   uint32_t l = 0;
@@ -226,17 +230,14 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     CF1_LAUNCH_CHECK();
     exclusive_scan_u64(cnt, woff, nbins, scan_tmp_, s);
     uint64_t nw = d2h_u64(woff + nbins, s);
-    if (A.size() <= l) {
-      A.push_back(new DevBuf());
-      R.push_back(new DevBuf());
-    }
+    if (AR.size() <= l) AR.push_back(new DevBuf());
     nwords.push_back(nw);
-    uint64_t *Al = A[l]->get<uint64_t>(nw);
-    uint64_t *Rl = R[l]->get<uint64_t>(nw + 1);
+    ulonglong2 *Al = AR[l]->get<ulonglong2>(nw);
+    uint64_t *Rl = rtmp_.get<uint64_t>(nw + 1);
     uint64_t *C = C_.get<uint64_t>(nw);
     uint32_t *pc = pc_.get<uint32_t>(nw);
-    bytes += nw * 16 + 8;
-    CF1_CUDA(cudaMemsetAsync(Al, 0, nw * 8, s));
+    bytes += nw * 16;
+    CF1_CUDA(cudaMemsetAsync(Al, 0, nw * sizeof(ulonglong2), s));
     CF1_CUDA(cudaMemsetAsync(C, 0, nw * 8, s));
     uint32_t ub = (uint32_t)(ceil_div(remaining, BB_TILE) + nbins);
     segment_tiles(roff, nbins, BB_TILE, tile_off, s);
@@ -245,6 +246,8 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     bb_clean_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, C, pc, nw);
     CF1_LAUNCH_CHECK();
     exclusive_scan_u32(pc, Rl, nw, scan_tmp_, s);
+    bb_rank_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, Rl, nw);
+    CF1_LAUNCH_CHECK();
     bb_meta_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(woff, Rl, base, meta + (size_t)l * nbins, nbins);
     CF1_LAUNCH_CHECK();
     uint32_t *tc = tile_cnt_.get<uint32_t>(ub + 1);
@@ -257,7 +260,6 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     offsets_from_tiles_kernel<<<(unsigned)ceil_div(nbins + 1, 256), 256, 0, s>>>(tile_off, nbins, to, noff);
     CF1_LAUNCH_CHECK();
     hA.push_back(Al);
-    hR.push_back(Rl);
     remaining = d2h_u64(noff + nbins, s);
     rem = nxt;
     roff = noff;
@@ -265,12 +267,8 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     l++;
   }
   levels = l;
-  const uint64_t **dA = aptr_.get<const uint64_t *>(levels + 1);
-  const uint64_t **dR = rptr_.get<const uint64_t *>(levels + 1);
-  if (levels) {
-    CF1_CUDA(cudaMemcpyAsync(dA, hA.data(), levels * sizeof(void *), cudaMemcpyHostToDevice, s));
-    CF1_CUDA(cudaMemcpyAsync(dR, hR.data(), levels * sizeof(void *), cudaMemcpyHostToDevice, s));
-  }
+  const ulonglong2 **dA = aptr_.get<const ulonglong2 *>(levels + 1);
+  if (levels) CF1_CUDA(cudaMemcpyAsync(dA, hA.data(), levels * sizeof(void *), cudaMemcpyHostToDevice, s));
   bytes += (size_t)levels * nbins * sizeof(BBMeta);
   CF1_CUDA(cudaStreamSynchronize(s));
 }
@@ -278,8 +276,7 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
 template <class KeyT>
 BBView BBHashBuild<KeyT>::view() const {
   BBView v;
-  v.A = aptr_.as<const uint64_t *const>();
-  v.R = rptr_.as<const uint64_t *const>();
+  v.AR = aptr_.as<const ulonglong2 *const>();
   v.meta = meta_.as<const BBMeta>();
   v.levels = levels;
   v.nbins = nbins;

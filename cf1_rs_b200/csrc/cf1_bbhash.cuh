@@ -6,9 +6,9 @@ namespace cf1 {
 
 template <class KeyT>
 struct BBHashBuild {
-  // per level: bit array, rank prefix (words + 1); kept across builds and
-  // grown on demand, so a rebuild allocates nothing once sizes settle
-  std::vector<DevBuf *> A, R;
+  // per level: {bit word, rank} entries; kept across builds and grown on
+  // demand, so a rebuild allocates nothing once sizes settle
+  std::vector<DevBuf *> AR;
   std::vector<uint64_t> nwords;  // words of each level in use
   uint32_t levels = 0, nbins = 0;
   uint64_t bytes = 0;
@@ -30,7 +30,7 @@ struct BBHashBuild {
   const BBMeta *meta_device() const { return meta_.as<const BBMeta>(); }
 
  private:
-  DevBuf meta_, aptr_, rptr_, base_, rem_[2], rem_off_[2], tile_off_, tile_cnt_, tile_out_, C_, wcnt_, woff_, pc_,
+  DevBuf meta_, aptr_, base_, rem_[2], rem_off_[2], tile_off_, tile_cnt_, tile_out_, C_, wcnt_, woff_, pc_, rtmp_,
       scan_tmp_;
 };
 

@@ -5,7 +5,9 @@
 // The image holds everything a query needs: the bucket -> bin table, the
 // per-bin slot offsets, the BBHash levels and, in learned mode, the roots,
 // leaves and the sorted distinct keys.  The query code is the device code
-// (cf1_mphf.cuh), compiled for the host.
+// (cf1_mphf.cuh), compiled for the host.  Image layout version 2: each BBHash
+// level is one array of 16-byte {bit word, rank} entries, so the image and
+// every section in it start on a 16-byte boundary.
 #include <cstring>
 #include <vector>
 
@@ -26,10 +28,11 @@ struct ImageHeader {
   uint64_t lut_off, dist_off_off, meta_off, levels_off, roots_off, leaves_off, keys_off, total;
 };
 struct LevelEntry {
-  uint64_t a_off, r_off, nwords;
+  uint64_t ar_off, nwords;
 };
 
-inline uint64_t align8(uint64_t x) { return (x + 7) & ~7ull; }
+constexpr uint32_t IMAGE_VERSION = 2;
+inline uint64_t align16(uint64_t x) { return (x + 15) & ~15ull; }  // sections are 16-byte aligned
 
 template <class KeyT>
 size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
@@ -40,7 +43,7 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   ImageHeader h;
   std::memset(&h, 0, sizeof(h));
   h.magic = IMAGE_MAGIC;
-  h.version = 1;
+  h.version = IMAGE_VERSION;
   h.k = c->k;
   h.m = c->m;
   h.nbins = B;
@@ -49,34 +52,33 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   h.key_words = KOps<KeyT>::WORDS;
   h.n_distinct = c->n_distinct;
   h.n_leaves = nleaves;
-  uint64_t off = align8(sizeof(ImageHeader));
+  uint64_t off = align16(sizeof(ImageHeader));
   h.lut_off = off;
-  off = align8(off + NUM_BUCKETS * sizeof(uint16_t));
+  off = align16(off + NUM_BUCKETS * sizeof(uint16_t));
   h.dist_off_off = off;
-  off = align8(off + (B + 1) * sizeof(uint64_t));
+  off = align16(off + (B + 1) * sizeof(uint64_t));
   h.meta_off = off;
-  off = align8(off + (uint64_t)NL * B * sizeof(BBMeta));
+  off = align16(off + (uint64_t)NL * B * sizeof(BBMeta));
   h.levels_off = off;
-  off = align8(off + (uint64_t)NL * sizeof(LevelEntry));
+  off = align16(off + (uint64_t)NL * sizeof(LevelEntry));
   std::vector<LevelEntry> lev(NL);
   for (uint32_t l = 0; l < NL; l++) {
     uint64_t nw = be.bb.level_words(l);
     lev[l].nwords = nw;
-    lev[l].a_off = off;
-    off = align8(off + nw * 8);
-    lev[l].r_off = off;
-    off = align8(off + (nw + 1) * 8);
+    lev[l].ar_off = off;
+    off = align16(off + nw * sizeof(ulonglong2));
   }
   h.roots_off = off;
-  off = align8(off + (learned ? B * sizeof(LIRoot) : 0));
+  off = align16(off + (learned ? B * sizeof(LIRoot) : 0));
   h.leaves_off = off;
-  off = align8(off + nleaves * sizeof(LILeaf));
+  off = align16(off + nleaves * sizeof(LILeaf));
   h.keys_off = off;
-  off = align8(off + (learned ? c->n_distinct * sizeof(KeyT) : 0));
+  off = align16(off + (learned ? c->n_distinct * sizeof(KeyT) : 0));
   h.total = off;
   if (!dst) return off;
   if (cap < off) throw Error(CF1GPU_ERR_INVALID_ARG, "export buffer too small");
-  if (reinterpret_cast<uintptr_t>(dst) % 8) throw Error(CF1GPU_ERR_INVALID_ARG, "export buffer must be 8-byte aligned");
+  if (reinterpret_cast<uintptr_t>(dst) % 16)
+    throw Error(CF1GPU_ERR_INVALID_ARG, "export buffer must be 16-byte aligned");
   char *d = static_cast<char *>(dst);
   cudaStream_t s = c->stream;
   std::memcpy(d, &h, sizeof(h));
@@ -85,10 +87,9 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   if (NL)
     CF1_CUDA(cudaMemcpyAsync(d + h.meta_off, be.bb.meta_device(), (size_t)NL * B * sizeof(BBMeta), cudaMemcpyDeviceToHost, s));
   std::memcpy(d + h.levels_off, lev.data(), NL * sizeof(LevelEntry));
-  for (uint32_t l = 0; l < NL; l++) {
-    CF1_CUDA(cudaMemcpyAsync(d + lev[l].a_off, be.bb.A[l]->p, lev[l].nwords * 8, cudaMemcpyDeviceToHost, s));
-    CF1_CUDA(cudaMemcpyAsync(d + lev[l].r_off, be.bb.R[l]->p, (lev[l].nwords + 1) * 8, cudaMemcpyDeviceToHost, s));
-  }
+  for (uint32_t l = 0; l < NL; l++)
+    CF1_CUDA(cudaMemcpyAsync(d + lev[l].ar_off, be.bb.AR[l]->p, lev[l].nwords * sizeof(ulonglong2),
+                             cudaMemcpyDeviceToHost, s));
   if (learned) {
     CF1_CUDA(cudaMemcpyAsync(d + h.roots_off, be.li.roots_device(), B * sizeof(LIRoot), cudaMemcpyDeviceToHost, s));
     CF1_CUDA(cudaMemcpyAsync(d + h.leaves_off, be.li.leaves_device(), nleaves * sizeof(LILeaf), cudaMemcpyDeviceToHost, s));
@@ -100,17 +101,13 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
 
 template <class KeyT>
 void host_query_impl(const ImageHeader &h, const char *img, const uint64_t *keys, size_t n, uint64_t *slots) {
-  std::vector<const uint64_t *> A(h.levels), R(h.levels);
+  std::vector<const ulonglong2 *> AR(h.levels);
   const LevelEntry *lev = reinterpret_cast<const LevelEntry *>(img + h.levels_off);
-  for (uint32_t l = 0; l < h.levels; l++) {
-    A[l] = reinterpret_cast<const uint64_t *>(img + lev[l].a_off);
-    R[l] = reinterpret_cast<const uint64_t *>(img + lev[l].r_off);
-  }
+  for (uint32_t l = 0; l < h.levels; l++) AR[l] = reinterpret_cast<const ulonglong2 *>(img + lev[l].ar_off);
   MphfView<KeyT> v;
   v.keys = reinterpret_cast<const KeyT *>(img + h.keys_off);
   v.dist_off = reinterpret_cast<const uint64_t *>(img + h.dist_off_off);
-  v.bb.A = A.data();
-  v.bb.R = R.data();
+  v.bb.AR = AR.data();
   v.bb.meta = reinterpret_cast<const BBMeta *>(img + h.meta_off);
   v.bb.levels = h.levels;
   v.bb.nbins = h.nbins;
@@ -136,11 +133,11 @@ size_t export_mphf(cf1gpu_ctx *c, void *dst, size_t cap) {
 }
 
 void host_query(const void *image, size_t bytes, const uint64_t *keys, size_t n, uint64_t *slots) {
-  if (bytes < sizeof(ImageHeader) || reinterpret_cast<uintptr_t>(image) % 8)
-    throw Error(CF1GPU_ERR_INVALID_ARG, "MPHF image too small or misaligned");
+  if (bytes < sizeof(ImageHeader) || reinterpret_cast<uintptr_t>(image) % 16)
+    throw Error(CF1GPU_ERR_INVALID_ARG, "MPHF image too small or not 16-byte aligned");
   ImageHeader h;
   std::memcpy(&h, image, sizeof(h));
-  if (h.magic != IMAGE_MAGIC || h.version != 1 || h.total > bytes)
+  if (h.magic != IMAGE_MAGIC || h.version != IMAGE_VERSION || h.total > bytes)
     throw Error(CF1GPU_ERR_INVALID_ARG, "not a cf1 MPHF image");
   const char *img = static_cast<const char *>(image);
   if (h.key_words == 2) host_query_impl<Key2>(h, img, keys, n, slots);

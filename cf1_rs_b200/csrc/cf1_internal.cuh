@@ -142,10 +142,11 @@ struct BBMeta {
   uint64_t rank_adj;  // bin-local slot base minus the level rank at word_off (mod 2^64)
 };
 
-// Device view of a per-bin BBHash (read by query kernels).
+// Device view of a per-bin BBHash (read by query kernels).  A level is an
+// array of {bit word, exclusive popcount before it}: one 16-byte load gives a
+// probe both the bit and the rank.
 struct BBView {
-  const uint64_t *const *A;  // per level: cleaned bit array
-  const uint64_t *const *R;  // per level: exclusive popcount per word
+  const ulonglong2 *const *AR;  // per level: {cleaned bit word, rank}
   const BBMeta *meta;        // [levels * nbins]
   uint32_t levels, nbins;
 };

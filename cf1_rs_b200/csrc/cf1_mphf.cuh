@@ -25,10 +25,9 @@ CF1_HD uint64_t bb_local_slot(const BBView &v, uint32_t bin, const KeyT &key) {
     const BBMeta mt = v.meta[(uint64_t)l * v.nbins + bin];
     if (mt.m_bits == 0) return SLOT_NONE;
     uint64_t pos = mulhi64(KOps<KeyT>::hash(key, bb_seed(l)), mt.m_bits);
-    uint64_t wi = mt.word_off + (pos >> 6);
-    uint64_t word = v.A[l][wi];
+    const ulonglong2 e = v.AR[l][mt.word_off + (pos >> 6)];
     uint32_t bit = (uint32_t)(pos & 63);
-    if ((word >> bit) & 1) return mt.rank_adj + v.R[l][wi] + (uint64_t)popc64(word & ((1ull << bit) - 1));
+    if ((e.x >> bit) & 1) return mt.rank_adj + e.y + (uint64_t)popc64(e.x & ((1ull << bit) - 1));
   }
   return SLOT_NONE;
 }

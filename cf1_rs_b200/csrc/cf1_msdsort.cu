@@ -237,7 +237,7 @@ struct CsShared {
 // memory before out is written, so they may overlap.  All threads call it.
 template <class KeyT>
 CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &dig, KeyT *S, const CsShared &sh,
-                                    KeyT *out) {
+                                    KeyT *out, bool distinct) {
   constexpr uint32_t CAP = cs_cap<KeyT>();
   const unsigned tid = threadIdx.x;
   for (uint32_t i = tid; i < CS_BUCKETS; i += CS_BLOCK) sh.hist[i] = 0;
@@ -301,8 +301,13 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
       }
     }
   }
-  // adjacent-unique
   (void)CAP;
+  if (distinct) {  // already one copy per key: plain copy out
+    for (uint32_t i = tid; i < m; i += CS_BLOCK) out[i] = S[i];
+    __syncthreads();
+    return m;
+  }
+  // adjacent-unique
   return block_select<CS_BLOCK>(
       m, [&](uint32_t i) { return i == 0 || S[i] != S[i - 1]; }, [&](uint32_t i, uint32_t r) { out[r] = S[i]; },
       sh.sm);
@@ -340,14 +345,18 @@ __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT 
   CsShared sh{hist, cur, sm, &s_big};
   CsDigit plain{shift, bits, 0, 0, 0u};
   uint32_t m = (uint32_t)n;
+  bool distinct = false;
   // 64-bit keys: one copy of each key first.  Repeats put hundreds of copies
   // of a k-mer in one bucket, where sorting copies would dominate the work.
   if (n > CS_DEDUP_MIN && KOps<KeyT>::WORDS == 1) {
     uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(T), a, n, reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
-    if (d != ~0u) m = d;
+    if (d != ~0u) {
+      m = d;
+      distinct = true;
+    }
   }
   if (m <= CAP) {
-    uint32_t tot = cs_sort_unique_range<KeyT>(T + a, m, plain, S, sh, T + a);
+    uint32_t tot = cs_sort_unique_range<KeyT>(T + a, m, plain, S, sh, T + a, distinct);
     if (tid == 0) cnt[j] = tot;
     return;
   }
@@ -414,10 +423,14 @@ __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT 
     if (b2 > shift) b2 = shift;
     CsDigit dig{shift, bits, shift - b2, b2, p0};
     uint32_t len = pstart[p1] - pstart[p0];
+    bool dd = false;
     if (len > CS_DEDUP_MIN && KOps<KeyT>::WORDS == 1) {
       uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(U), a + pstart[p0], len,
                                  reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
-      if (d != ~0u) len = d;  // (a failed pass leaves U untouched)
+      if (d != ~0u) {  // (a failed pass leaves U untouched)
+        len = d;
+        dd = true;
+      }
       if (len > CAP) {
         if (tid == 0) {
           cnt[j] = 0;
@@ -426,7 +439,7 @@ __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT 
         return;
       }
     }
-    outc += cs_sort_unique_range<KeyT>(U + a + pstart[p0], len, dig, S, sh, T + a + outc);
+    outc += cs_sort_unique_range<KeyT>(U + a + pstart[p0], len, dig, S, sh, T + a + outc, dd);
   }
   if (tid == 0) cnt[j] = outc;
 }

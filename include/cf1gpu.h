@@ -152,18 +152,20 @@ int cf1gpu_query(cf1gpu_ctx *ctx, const uint64_t *keys, size_t n, uint64_t *slot
  * storage order (bins in order, each bin sorted), n must be total_kmers. */
 int cf1gpu_dump_states(cf1gpu_ctx *ctx, uint64_t *keys, uint8_t *states, size_t n);
 
-/* Judge: queries every distinct key on the device and checks that the slots
- * form a bijection onto [0, total_kmers).  0 when they do. */
+/* Verification pass: queries every distinct key on the device and checks that
+ * the slots form a bijection onto [0, total_kmers).  0 when they do. */
 int cf1gpu_verify_bijection(cf1gpu_ctx *ctx);
 
 /* Short sequences (src/classify.rs:550-561), in input order. */
 size_t cf1gpu_short_seq_count(const cf1gpu_ctx *ctx);
 int cf1gpu_short_seq(const cf1gpu_ctx *ctx, size_t i, char *name_buf, size_t name_cap, uint64_t *len);
 
-/* Flat host image of the MPHF.  Call with dst NULL to get the size. */
+/* Flat host image of the MPHF.  Call with dst NULL to get the size; dst must
+ * be 16-byte aligned. */
 int cf1gpu_export_mphf(cf1gpu_ctx *ctx, void *dst, size_t *bytes);
 
-/* Mphf::hash on the host over an exported image (thread-safe, no device). */
+/* Mphf::hash on the host over an exported image (thread-safe, no device);
+ * image must be 16-byte aligned. */
 int cf1gpu_mphf_host_query(const void *image, size_t bytes, const uint64_t *keys, size_t n, uint64_t *slots);
 
 /* Learned-index statistics of the last run (learned mode): out5 =
