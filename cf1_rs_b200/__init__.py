@@ -41,7 +41,8 @@ class Opts(C.Structure):
         ("k", C.c_uint32), ("num_bins", C.c_uint32), ("device", C.c_int32), ("mphf_mode", C.c_uint32),
         ("batched", C.c_uint32), ("track_short_seqs", C.c_uint32), ("tuner_cache_path", C.c_char_p),
         ("learned_max_err", C.c_uint32), ("learned_train_steps", C.c_int32), ("learned_leaf_size", C.c_uint32),
-        ("sk_tile", C.c_uint32), ("sort_mode", C.c_uint32), ("reserved", C.c_uint32 * 3),
+        ("sk_tile", C.c_uint32), ("sort_mode", C.c_uint32), ("state_update", C.c_uint32),
+        ("reserved", C.c_uint32 * 2),
     ]
 
 
@@ -161,7 +162,7 @@ class Cf1Gpu:
     def __init__(self, k: int = 31, num_bins: int = 128, device: int = 0, mode: str = "bbhash",
                  batched: bool = False, track_short_seqs: bool = False, learned_max_err: int = 0,
                  learned_train_steps: int = 0, learned_leaf_size: int = 0, sk_tile: int = 0,
-                 sort_mode: str = "msd"):
+                 sort_mode: str = "msd", state_update: str = "sideset"):
         L = lib()
         o = Opts()
         L.cf1gpu_default_opts(C.byref(o))
@@ -174,6 +175,7 @@ class Cf1Gpu:
         o.learned_leaf_size = learned_leaf_size
         o.sk_tile = sk_tile
         o.sort_mode = {"msd": 0, "lsd": 1}[sort_mode]
+        o.state_update = {"sideset": 0, "cas": 1}[state_update]
         h = C.c_void_p()
         st = L.cf1gpu_create(C.byref(o), C.byref(h))
         if st != OK:

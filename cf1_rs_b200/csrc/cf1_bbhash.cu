@@ -11,8 +11,12 @@
 //   filter : keys whose bit survived are placed, the rest go to the next level.
 // A bin's local slot of a key placed at level l is the number of keys of the
 // bin placed at earlier levels plus the key's rank inside its level block.
+// All levels live in one array of {bit word, level rank} entries, addressed
+// through the per-(level, bin) BBMeta table.
+#include <algorithm>
 #include <cstring>
 
+#include "../../include/cf1gpu.h"
 #include "cf1_bbhash.cuh"
 #include "cf1_device_util.cuh"
 #include "cf1_mphf.cuh"
@@ -23,7 +27,6 @@ namespace {
 
 constexpr int BB_BLOCK = 256;
 constexpr uint32_t BB_TILE = 4096;
-constexpr uint32_t BB_MAX_LEVELS = 64;
 
 __global__ void bb_sel_counts_kernel(const uint64_t *seg_off, const uint32_t *sel, uint32_t nbins, uint64_t *cnt) {
   uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -52,6 +55,8 @@ __global__ void bb_sizes_kernel(const uint64_t *rem_off, uint32_t nbins, uint64_
   }
 }
 
+// AR points at this level's first entry; woff are the level-relative block
+// offsets of the bins.
 template <class KeyT>
 __global__ void __launch_bounds__(BB_BLOCK) bb_mark_kernel(const KeyT *rem, const uint64_t *rem_off,
                                                            const uint32_t *tile_off, uint32_t nbins,
@@ -60,10 +65,10 @@ __global__ void __launch_bounds__(BB_BLOCK) bb_mark_kernel(const KeyT *rem, cons
   const uint32_t t = blockIdx.x;
   if (t >= tile_off[nbins]) return;
   TileSpan sp = tile_span(rem_off, tile_off, nbins, t, BB_TILE);
-  const uint64_t w0 = woff[sp.seg], m_bits = (woff[sp.seg + 1] - w0) * 64;
-  const uint64_t seed = bb_seed(level);
+  const uint64_t w0 = woff[sp.seg];
+  const uint32_t nw = (uint32_t)(woff[sp.seg + 1] - w0);
   for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) {
-    uint64_t pos = mulhi64(KOps<KeyT>::hash(rem[i], seed), m_bits);
+    uint64_t pos = bb_pos(bb_key_hash(rem[i]), level, nw);
     uint64_t wi = w0 + (pos >> 6);
     uint64_t bit = 1ull << (pos & 63);
     unsigned long long old = atomicOr(&AR[wi].x, (unsigned long long)bit);
@@ -85,21 +90,22 @@ __global__ void bb_rank_kernel(ulonglong2 *AR, const uint64_t *R, uint64_t nw) {
   if (i < nw) AR[i].y = R[i];
 }
 
-__global__ void bb_meta_kernel(const uint64_t *woff, const uint64_t *R, uint64_t *base, BBMeta *meta, uint32_t nbins) {
+__global__ void bb_meta_kernel(const uint64_t *woff, const uint64_t *R, uint64_t level_base, uint64_t *base,
+                               BBMeta *meta, uint32_t nbins) {
   uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbins) return;
   uint64_t w0 = woff[b], w1 = woff[b + 1];
   BBMeta m;
-  m.word_off = w0;
-  m.m_bits = (w1 - w0) * 64;
-  m.rank_adj = base[b] - R[w0];
+  m.word_off = level_base + w0;
+  m.nwords = (uint32_t)(w1 - w0);
+  m.rank_adj = (uint32_t)(base[b] - R[w0]);
   meta[b] = m;
   base[b] += R[w1] - R[w0];
 }
 
 template <class KeyT>
-CF1_D bool bb_placed(const KeyT &key, uint64_t seed, uint64_t w0, uint64_t m_bits, const ulonglong2 *AR) {
-  uint64_t pos = mulhi64(KOps<KeyT>::hash(key, seed), m_bits);
+CF1_D bool bb_placed(const KeyT &key, uint32_t level, uint64_t w0, uint32_t nw, const ulonglong2 *AR) {
+  uint64_t pos = bb_pos(bb_key_hash(key), level, nw);
   return (AR[w0 + (pos >> 6)].x >> (pos & 63)) & 1;
 }
 
@@ -115,10 +121,10 @@ __global__ void __launch_bounds__(BB_BLOCK) bb_filter_count_kernel(const KeyT *r
     return;
   }
   TileSpan sp = tile_span(rem_off, tile_off, nbins, t, BB_TILE);
-  const uint64_t w0 = woff[sp.seg], m_bits = (woff[sp.seg + 1] - w0) * 64;
-  const uint64_t seed = bb_seed(level);
+  const uint64_t w0 = woff[sp.seg];
+  const uint32_t nw = (uint32_t)(woff[sp.seg + 1] - w0);
   uint32_t c = 0;
-  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) c += bb_placed(rem[i], seed, w0, m_bits, A) ? 0 : 1;
+  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) c += bb_placed(rem[i], level, w0, nw, A) ? 0 : 1;
   uint32_t tot = block_sum<BB_BLOCK>(c, sm);
   if (threadIdx.x == 0) tile_cnt[t] = tot;
 }
@@ -134,14 +140,14 @@ __global__ void __launch_bounds__(BB_BLOCK) bb_filter_write_kernel(const KeyT *r
   const uint32_t t = blockIdx.x;
   if (t >= tile_off[nbins]) return;
   TileSpan sp = tile_span(rem_off, tile_off, nbins, t, BB_TILE);
-  const uint64_t w0 = woff[sp.seg], m_bits = (woff[sp.seg + 1] - w0) * 64;
-  const uint64_t seed = bb_seed(level);
+  const uint64_t w0 = woff[sp.seg];
+  const uint32_t nw = (uint32_t)(woff[sp.seg + 1] - w0);
   uint64_t i0 = sp.start + (uint64_t)threadIdx.x * ITEMS;
   uint32_t flags = 0, c = 0;
 #pragma unroll
   for (int j = 0; j < ITEMS; j++) {
     uint64_t i = i0 + j;
-    bool keep = i < sp.end && !bb_placed(rem[i], seed, w0, m_bits, A);
+    bool keep = i < sp.end && !bb_placed(rem[i], level, w0, nw, A);
     flags |= (uint32_t)keep << j;
     c += keep;
   }
@@ -169,15 +175,28 @@ uint64_t d2h_u64(const uint64_t *p, cudaStream_t s) {
 }  // namespace
 
 template <class KeyT>
-BBHashBuild<KeyT>::~BBHashBuild() {
-  for (DevBuf *b : AR) delete b;
+void BBHashBuild<KeyT>::clear() {
+  nwords.clear();
+  level_off.clear();
+  total_words = 0;
+  levels = 0;
+  bytes = 0;
 }
 
 template <class KeyT>
-void BBHashBuild<KeyT>::clear() {
-  nwords.clear();
-  levels = 0;
-  bytes = 0;
+void BBHashBuild<KeyT>::reserve_entries(uint64_t words, uint64_t keep, cudaStream_t s) {
+  const size_t need = words * sizeof(ulonglong2);
+  if (ar_.p && need <= ar_.cap) return;
+  size_t cap = std::max<size_t>(need + need / 4, 4096);
+  void *np = nullptr;
+  CF1_CUDA(cudaMalloc(&np, cap));
+  if (keep && ar_.p) {
+    CF1_CUDA(cudaMemcpyAsync(np, ar_.p, keep * sizeof(ulonglong2), cudaMemcpyDeviceToDevice, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+  }
+  ar_.release();
+  ar_.p = np;
+  ar_.cap = cap;
 }
 
 template <class KeyT>
@@ -185,6 +204,14 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
                               cudaStream_t s, KeyT *ws0, KeyT *ws1, uint64_t ws_cap) {
   clear();
   nbins = nb;
+  {  // local slots are 32-bit: every bin must hold fewer than 2^32 keys
+    std::vector<uint64_t> h(nbins + 1);
+    CF1_CUDA(cudaMemcpyAsync(h.data(), seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t b = 0; b < nbins; b++)
+      if (h[b + 1] - h[b] >= (1ull << 32))
+        throw Error(CF1GPU_ERR_INVALID_ARG, "BBHash: a bin holds 2^32 or more distinct keys; use more bins");
+  }
   uint64_t *base = base_.get<uint64_t>(nbins);
   CF1_CUDA(cudaMemsetAsync(base, 0, nbins * sizeof(uint64_t), s));
   BBMeta *meta = meta_.get<BBMeta>((size_t)BB_MAX_LEVELS * nbins);
@@ -217,12 +244,14 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     rem = r[0];
     roff = off0;
   }
-  std::vector<const ulonglong2 *> hA;
+  // room for the usual level sizes (2 bits per key, then ~40% fewer keys per
+  // level) so that the entry array rarely grows in mid-build
+  reserve_entries((2 * n / 64 + nbins) * 2 + 64, 0, s);
   int cur = 1;  // level l reads rem (keys, then r[cur^1]) and writes r[cur]
   uint64_t remaining = n;
   uint32_t l = 0;
   while (remaining > 0) {
-    if (l >= BB_MAX_LEVELS) throw Error(-5, "BBHash: keys left after the last level");
+    if (l >= BB_MAX_LEVELS) throw Error(CF1GPU_ERR_BIJECTION, "BBHash: keys left after the last level");
     KeyT *nxt = r[cur];
     uint64_t *noff = roffs[cur];
     uint64_t *woff = woff_.get<uint64_t>(nbins + 1);
@@ -230,13 +259,13 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     CF1_LAUNCH_CHECK();
     exclusive_scan_u64(cnt, woff, nbins, scan_tmp_, s);
     uint64_t nw = d2h_u64(woff + nbins, s);
-    if (AR.size() <= l) AR.push_back(new DevBuf());
+    reserve_entries(total_words + nw, total_words, s);
     nwords.push_back(nw);
-    ulonglong2 *Al = AR[l]->get<ulonglong2>(nw);
+    level_off.push_back(total_words);
+    ulonglong2 *Al = ar_.as<ulonglong2>() + total_words;
     uint64_t *Rl = rtmp_.get<uint64_t>(nw + 1);
     uint64_t *C = C_.get<uint64_t>(nw);
     uint32_t *pc = pc_.get<uint32_t>(nw);
-    bytes += nw * 16;
     CF1_CUDA(cudaMemsetAsync(Al, 0, nw * sizeof(ulonglong2), s));
     CF1_CUDA(cudaMemsetAsync(C, 0, nw * 8, s));
     uint32_t ub = (uint32_t)(ceil_div(remaining, BB_TILE) + nbins);
@@ -248,7 +277,8 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     exclusive_scan_u32(pc, Rl, nw, scan_tmp_, s);
     bb_rank_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, Rl, nw);
     CF1_LAUNCH_CHECK();
-    bb_meta_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(woff, Rl, base, meta + (size_t)l * nbins, nbins);
+    bb_meta_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(woff, Rl, total_words, base, meta + (size_t)l * nbins,
+                                                                  nbins);
     CF1_LAUNCH_CHECK();
     uint32_t *tc = tile_cnt_.get<uint32_t>(ub + 1);
     uint64_t *to = tile_out_.get<uint64_t>(ub + 2);
@@ -259,7 +289,7 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     CF1_LAUNCH_CHECK();
     offsets_from_tiles_kernel<<<(unsigned)ceil_div(nbins + 1, 256), 256, 0, s>>>(tile_off, nbins, to, noff);
     CF1_LAUNCH_CHECK();
-    hA.push_back(Al);
+    total_words += nw;
     remaining = d2h_u64(noff + nbins, s);
     rem = nxt;
     roff = noff;
@@ -267,16 +297,14 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     l++;
   }
   levels = l;
-  const ulonglong2 **dA = aptr_.get<const ulonglong2 *>(levels + 1);
-  if (levels) CF1_CUDA(cudaMemcpyAsync(dA, hA.data(), levels * sizeof(void *), cudaMemcpyHostToDevice, s));
-  bytes += (size_t)levels * nbins * sizeof(BBMeta);
+  bytes = total_words * sizeof(ulonglong2) + (size_t)levels * nbins * sizeof(BBMeta);
   CF1_CUDA(cudaStreamSynchronize(s));
 }
 
 template <class KeyT>
 BBView BBHashBuild<KeyT>::view() const {
   BBView v;
-  v.AR = aptr_.as<const ulonglong2 *const>();
+  v.AR = ar_.as<const ulonglong2>();
   v.meta = meta_.as<const BBMeta>();
   v.levels = levels;
   v.nbins = nbins;

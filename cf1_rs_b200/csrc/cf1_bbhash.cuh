@@ -6,17 +6,15 @@ namespace cf1 {
 
 template <class KeyT>
 struct BBHashBuild {
-  // per level: {bit word, rank} entries; kept across builds and grown on
-  // demand, so a rebuild allocates nothing once sizes settle
-  std::vector<DevBuf *> AR;
-  std::vector<uint64_t> nwords;  // words of each level in use
+  std::vector<uint64_t> nwords;    // words of each level in use
+  std::vector<uint64_t> level_off; // first entry of each level in the entry array
+  uint64_t total_words = 0;        // entries of all levels
   uint32_t levels = 0, nbins = 0;
   uint64_t bytes = 0;
 
   BBHashBuild() = default;
   BBHashBuild(const BBHashBuild &) = delete;
   BBHashBuild &operator=(const BBHashBuild &) = delete;
-  ~BBHashBuild();
 
   // Builds over the bins with sel[b] != 0 (sel == nullptr: every bin); the
   // other bins get no levels.  Synchronises the stream between levels.
@@ -28,9 +26,16 @@ struct BBHashBuild {
   void clear();
   uint64_t level_words(uint32_t l) const;
   const BBMeta *meta_device() const { return meta_.as<const BBMeta>(); }
+  // {bit word, level rank} entries of all levels (total_words of them)
+  const ulonglong2 *entries_device() const { return ar_.as<const ulonglong2>(); }
 
  private:
-  DevBuf meta_, aptr_, base_, rem_[2], rem_off_[2], tile_off_, tile_cnt_, tile_out_, C_, wcnt_, woff_, pc_, rtmp_,
+  // Grows the entry array to hold `words` entries, keeping the first `keep`.
+  void reserve_entries(uint64_t words, uint64_t keep, cudaStream_t s);
+
+  // The entry array and the level buffers are kept across builds and grown on
+  // demand, so a rebuild allocates nothing once sizes settle.
+  DevBuf ar_, meta_, base_, rem_[2], rem_off_[2], tile_off_, tile_cnt_, tile_out_, C_, wcnt_, woff_, pc_, rtmp_,
       scan_tmp_;
 };
 

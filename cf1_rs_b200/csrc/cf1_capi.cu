@@ -67,6 +67,14 @@ int cf1gpu_create(const cf1gpu_opts *opts, cf1gpu_ctx **out) {
     g_create_error = "sk_tile must be 1024, 2048 or 4096";
     return CF1GPU_ERR_INVALID_ARG;
   }
+  if (opts->sort_mode > 1) {
+    g_create_error = "sort_mode must be 0 (MSD) or 1 (LSD)";
+    return CF1GPU_ERR_INVALID_ARG;
+  }
+  if (opts->state_update > 1) {
+    g_create_error = "state_update must be 0 (side sets) or 1 (CAS)";
+    return CF1GPU_ERR_INVALID_ARG;
+  }
   cf1gpu_ctx *c = new (std::nothrow) cf1gpu_ctx();
   if (!c) return CF1GPU_ERR_OOM;
   int st = guard(nullptr, [&] {

@@ -258,6 +258,28 @@ CF1_HD uint32_t join_state(uint32_t s, uint32_t c) {
   return encode_sides(join_side(f1, f2), join_side(b1, b2));
 }
 
+// Side sets: the per-side join embedded in bitwise OR, so that a vertex's
+// sides can be joined by fire-and-forget atomic ORs and turned into the
+// 5-bit state afterwards.  A side is one nibble: base b is the weight-2 code
+// 0x3, 0x5, 0x6 or 0x9, M is 0xF, unvisited is 0.  OR of a code with itself
+// keeps it; OR of two different weight-2 codes, or of anything with 0xF, has
+// weight >= 3, which reads back as M -- exactly join_side.  One byte per
+// vertex: front nibble low, back nibble high.
+CF1_HD uint32_t side_code(uint32_t side) { return side == SIDE_M ? 0xFu : (0x9653u >> (4 * side)) & 0xFu; }
+CF1_HD uint32_t side_of_code(uint32_t nib) {
+  if (popc64(nib) >= 3) return SIDE_M;
+  return nib == 0x3u ? 0u : nib == 0x5u ? 1u : nib == 0x6u ? 2u : 3u;
+}
+CF1_HD uint32_t sideset_of_state(uint32_t c) {
+  uint32_t f, b;
+  decode_sides(c, f, b);
+  return side_code(f) | (side_code(b) << 4);
+}
+CF1_HD uint32_t state_of_sideset(uint32_t byte) {
+  if (byte == 0) return 0;  // no occurrence reached the vertex
+  return encode_sides(side_of_code(byte & 0xFu), side_of_code(byte >> 4));
+}
+
 // The (front, back) contribution of one k-mer occurrence in canonical
 // orientation (src/classify.rs:65-518): isolated -> (M,M); rightmost ->
 // fwd (prev,M) / bwd (M,~prev); self loop (canonical == next canonical,

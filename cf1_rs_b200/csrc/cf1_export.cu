@@ -5,9 +5,10 @@
 // The image holds everything a query needs: the bucket -> bin table, the
 // per-bin slot offsets, the BBHash levels and, in learned mode, the roots,
 // leaves and the sorted distinct keys.  The query code is the device code
-// (cf1_mphf.cuh), compiled for the host.  Image layout version 2: each BBHash
-// level is one array of 16-byte {bit word, rank} entries, so the image and
-// every section in it start on a 16-byte boundary.
+// (cf1_mphf.cuh), compiled for the host.  Image layout version 3: the BBHash
+// levels are one array of 16-byte {bit word, level rank} entries addressed
+// through the 16-byte per-(level, bin) metadata, so the image and every
+// section in it start on a 16-byte boundary.
 #include <cstring>
 #include <vector>
 
@@ -25,13 +26,10 @@ struct ImageHeader {
   uint64_t magic;
   uint32_t version, k, m, nbins, levels, learned, key_words, pad;
   uint64_t n_distinct, n_leaves;
-  uint64_t lut_off, dist_off_off, meta_off, levels_off, roots_off, leaves_off, keys_off, total;
-};
-struct LevelEntry {
-  uint64_t ar_off, nwords;
+  uint64_t lut_off, dist_off_off, meta_off, ar_off, ar_words, roots_off, leaves_off, keys_off, total;
 };
 
-constexpr uint32_t IMAGE_VERSION = 2;
+constexpr uint32_t IMAGE_VERSION = 3;
 inline uint64_t align16(uint64_t x) { return (x + 15) & ~15ull; }  // sections are 16-byte aligned
 
 template <class KeyT>
@@ -59,15 +57,9 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   off = align16(off + (B + 1) * sizeof(uint64_t));
   h.meta_off = off;
   off = align16(off + (uint64_t)NL * B * sizeof(BBMeta));
-  h.levels_off = off;
-  off = align16(off + (uint64_t)NL * sizeof(LevelEntry));
-  std::vector<LevelEntry> lev(NL);
-  for (uint32_t l = 0; l < NL; l++) {
-    uint64_t nw = be.bb.level_words(l);
-    lev[l].nwords = nw;
-    lev[l].ar_off = off;
-    off = align16(off + nw * sizeof(ulonglong2));
-  }
+  h.ar_off = off;
+  h.ar_words = be.bb.total_words;
+  off = align16(off + h.ar_words * sizeof(ulonglong2));
   h.roots_off = off;
   off = align16(off + (learned ? B * sizeof(LIRoot) : 0));
   h.leaves_off = off;
@@ -86,9 +78,8 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   CF1_CUDA(cudaMemcpyAsync(d + h.dist_off_off, c->d_dist_off.p, (B + 1) * 8, cudaMemcpyDeviceToHost, s));
   if (NL)
     CF1_CUDA(cudaMemcpyAsync(d + h.meta_off, be.bb.meta_device(), (size_t)NL * B * sizeof(BBMeta), cudaMemcpyDeviceToHost, s));
-  std::memcpy(d + h.levels_off, lev.data(), NL * sizeof(LevelEntry));
-  for (uint32_t l = 0; l < NL; l++)
-    CF1_CUDA(cudaMemcpyAsync(d + lev[l].ar_off, be.bb.AR[l]->p, lev[l].nwords * sizeof(ulonglong2),
+  if (h.ar_words)
+    CF1_CUDA(cudaMemcpyAsync(d + h.ar_off, be.bb.entries_device(), h.ar_words * sizeof(ulonglong2),
                              cudaMemcpyDeviceToHost, s));
   if (learned) {
     CF1_CUDA(cudaMemcpyAsync(d + h.roots_off, be.li.roots_device(), B * sizeof(LIRoot), cudaMemcpyDeviceToHost, s));
@@ -101,13 +92,10 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
 
 template <class KeyT>
 void host_query_impl(const ImageHeader &h, const char *img, const uint64_t *keys, size_t n, uint64_t *slots) {
-  std::vector<const ulonglong2 *> AR(h.levels);
-  const LevelEntry *lev = reinterpret_cast<const LevelEntry *>(img + h.levels_off);
-  for (uint32_t l = 0; l < h.levels; l++) AR[l] = reinterpret_cast<const ulonglong2 *>(img + lev[l].ar_off);
   MphfView<KeyT> v;
   v.keys = reinterpret_cast<const KeyT *>(img + h.keys_off);
   v.dist_off = reinterpret_cast<const uint64_t *>(img + h.dist_off_off);
-  v.bb.AR = AR.data();
+  v.bb.AR = reinterpret_cast<const ulonglong2 *>(img + h.ar_off);
   v.bb.meta = reinterpret_cast<const BBMeta *>(img + h.meta_off);
   v.bb.levels = h.levels;
   v.bb.nbins = h.nbins;

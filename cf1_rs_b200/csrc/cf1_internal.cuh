@@ -66,6 +66,25 @@ struct DevBuf {
 
 inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 
+// CTAs of a persistent (work-queue) launch: `requested` when positive, else
+// one full wave -- the CTAs of `kernel` resident per SM times the SMs; never
+// more than `items` work items.
+template <class Kernel>
+unsigned persistent_grid(Kernel kernel, int block, size_t smem, int requested, uint64_t items) {
+  uint64_t g;
+  if (requested > 0) {
+    g = (uint64_t)requested;
+  } else {
+    int dev = 0, sms = 0, per_sm = 0;
+    CF1_CUDA(cudaGetDevice(&dev));
+    CF1_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CF1_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem));
+    g = (uint64_t)(per_sm > 0 ? per_sm : 1) * (uint64_t)sms;
+  }
+  if (g > items) g = items;
+  return (unsigned)(g ? g : 1);
+}
+
 // ------------------------------------------------------------ util kernels ----
 // Exclusive prefix sum of n values into out[0..n] (out[n] = total).
 // `scratch` grows as needed.
@@ -136,24 +155,29 @@ void segmented_unique(const KeyT *keys, uint64_t n, const uint64_t *seg_off, uin
                       SortScratch<KeyT> &sc, cudaStream_t s);
 
 // ------------------------------------------------------------ MPHF ----
-struct BBMeta {
-  uint64_t word_off;  // first word of this (level, bin) block in the level array
-  uint64_t m_bits;    // block size in bits (0: bin has no keys at this level)
-  uint64_t rank_adj;  // bin-local slot base minus the level rank at word_off (mod 2^64)
+// One (level, bin) block of a per-bin BBHash; 16 bytes, one load per probe.
+struct __align__(16) BBMeta {
+  uint64_t word_off;  // first entry of the block in the entry array (all levels)
+  uint32_t nwords;    // block size in 64-bit words (0: bin has no keys at this level)
+  uint32_t rank_adj;  // bin-local slot base minus the level rank at word_off (mod 2^32; bins hold < 2^32 keys)
 };
 
-// Device view of a per-bin BBHash (read by query kernels).  A level is an
-// array of {bit word, exclusive popcount before it}: one 16-byte load gives a
-// probe both the bit and the rank.
+// Device view of a per-bin BBHash (read by query kernels).  All levels share
+// one array of {bit word, exclusive popcount of the level before it}
+// entries: one 16-byte load gives a probe both the bit and the rank.
 struct BBView {
-  const ulonglong2 *const *AR;  // per level: {cleaned bit word, rank}
-  const BBMeta *meta;        // [levels * nbins]
+  const ulonglong2 *AR;  // {cleaned bit word, level rank}, levels back to back
+  const BBMeta *meta;    // [levels * nbins]
   uint32_t levels, nbins;
 };
 
 constexpr int LI_HIDDEN = 16;
+// The trained root, stored as the piecewise-linear function it computes: the
+// hidden ramps tile [0, 1] (ramp j over [knot[j], knot[j+1])), so on piece j
+// every earlier ramp is saturated and every later one is 0, and
+// root(x) = base[j] + slope[j] * (x - knot[j]).
 struct LIRoot {
-  float w1[LI_HIDDEN], b1[LI_HIDDEN], w2[LI_HIDDEN], b2;
+  float knot[LI_HIDDEN], base[LI_HIDDEN], slope[LI_HIDDEN];
   uint64_t hmin;     // high64 of the bin's smallest key
   float inv_range;   // 1 / (high64(max) - high64(min))
   uint32_t n_leaves; // leaves of this bin

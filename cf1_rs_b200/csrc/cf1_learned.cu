@@ -40,7 +40,8 @@ constexpr int H = LI_HIDDEN;
 
 // Adds one sample's MSE term (weight `scale`) and its gradient to g.
 // Parameter layout: w1[0,H) b1[H,2H) w2[2H,3H) b2[3H]; hidden units are
-// clipped ReLUs clamp(w1 x + b1, 0, 1) (li_root_eval).
+// clipped ReLUs clamp(w1 x + b1, 0, 1) (li_act).  Queries evaluate the same
+// function on its piecewise-linear form (LIRoot, li_root_eval).
 CF1_HD void mlp_accumulate(const float *P, float x, float t, float scale, float *g, float &loss) {
   float z[H];
   float y = P[3 * H];
@@ -60,16 +61,6 @@ CF1_HD void mlp_accumulate(const float *P, float x, float t, float scale, float 
     g[j] += dz * x;
     g[H + j] += dz;
   }
-}
-
-// Identity initialisation: hidden unit j ramps from 0 to 1 over
-// x in [j/H, (j+1)/H] (w1 = H, b1 = -j) and feeds the output with 1/H, so
-// root(x) = x on [0, 1] -- the index without a trained network.
-CF1_HD float init_param(int p) {
-  if (p < H) return (float)H;
-  if (p < 2 * H) return -(float)(p - H);
-  if (p < 3 * H) return 1.f / (float)H;
-  return 0.f;
 }
 
 // Trained parameters Q (2H+1): knot logits theta[H], output weights w2[H],
@@ -160,7 +151,9 @@ __global__ void __launch_bounds__(LT_BLOCK) li_train_kernel(const KeyT *keys, co
     st[i] = (float)((double)r / (double)n);
   }
   if (tid < LI_NQ) {
-    Q[tid] = tid < H ? 0.f : (tid < 2 * H ? 1.f / (float)H : 0.f);  // identity root
+    // identity root: equal knot logits (unit j ramps over [j/H, (j+1)/H]),
+    // output weights 1/H, so root(x) = x -- the index without a trained network
+    Q[tid] = tid < H ? 0.f : (tid < 2 * H ? 1.f / (float)H : 0.f);
     M1[tid] = 0.f;
     M2[tid] = 0.f;
   }
@@ -208,22 +201,30 @@ __global__ void __launch_bounds__(LT_BLOCK) li_train_kernel(const KeyT *keys, co
     if (tid == 0) derive_params(Q, P, sd, stk);
     __syncthreads();
   }
-  // Output fold: an affine map with a positive slope sends the bin's smallest
-  // key to 0 and its largest to just below 1, so the leaves cover the keys.
-  if (tid == 0 && n) {
-    LIRoot tmp;
+  // The network on its piecewise-linear form: on [t_j, t_j + d_j) ramps
+  // i < j are saturated and ramps i > j are 0, so the value is
+  // b2 + sum_{i<j} w2_i + (w2_j / d_j) (x - t_j).  Then the output fold: an
+  // affine map with a positive slope sends the bin's smallest key to 0 and
+  // its largest to just below 1, so the leaves cover the keys.
+  __shared__ LIRoot s_root;
+  if (tid == 0) {
+    float c = P[3 * H];
     for (int j = 0; j < H; j++) {
-      tmp.w1[j] = P[j];
-      tmp.b1[j] = P[H + j];
-      tmp.w2[j] = P[2 * H + j];
+      s_root.knot[j] = stk[j];
+      s_root.base[j] = c;
+      s_root.slope[j] = P[2 * H + j] / sd[j];
+      c += P[2 * H + j];
     }
-    tmp.b2 = P[3 * H];
-    tmp.hmin = hmin;
-    tmp.inv_range = inv;
-    float y0 = li_root_eval(tmp, li_x(tmp, hmin)), y1 = li_root_eval(tmp, li_x(tmp, hmax));
-    if (y1 > y0) {
+    s_root.hmin = hmin;
+    s_root.inv_range = inv;
+    float y0 = li_root_eval(s_root, li_x(s_root, hmin)), y1 = li_root_eval(s_root, li_x(s_root, hmax));
+    if (n && y1 > y0) {
       float a = 0.99999905f / (y1 - y0);
-      for (int j = 0; j < H; j++) P[2 * H + j] *= a;
+      for (int j = 0; j < H; j++) {
+        P[2 * H + j] *= a;
+        s_root.base[j] = a * (s_root.base[j] - y0);
+        s_root.slope[j] *= a;
+      }
       P[3 * H] = a * P[3 * H] - a * y0;
     }
   }
@@ -244,12 +245,11 @@ __global__ void __launch_bounds__(LT_BLOCK) li_train_kernel(const KeyT *keys, co
     }
   }
   if (tid < H) {
-    R.w1[tid] = P[tid];
-    R.b1[tid] = P[H + tid];
-    R.w2[tid] = P[2 * H + tid];
+    R.knot[tid] = s_root.knot[tid];
+    R.base[tid] = s_root.base[tid];
+    R.slope[tid] = s_root.slope[tid];
   }
   if (tid == 0) {
-    R.b2 = P[3 * H];
     R.hmin = hmin;
     R.inv_range = inv;
   }
@@ -447,12 +447,11 @@ void LearnedBuild<KeyT>::build(const KeyT *keys, const uint64_t *dist_off, uint3
     uint64_t n = hoff[b + 1] - hoff[b];
     uint64_t nl = n ? (n + leaf_size - 1) / leaf_size : 1;
     std::memset(&hroots[b], 0, sizeof(LIRoot));
-    for (int p = 0; p < H; p++) {
-      hroots[b].w1[p] = init_param(p);
-      hroots[b].b1[p] = init_param(H + p);
-      hroots[b].w2[p] = init_param(2 * H + p);
+    for (int p = 0; p < H; p++) {  // identity root until training writes its own
+      hroots[b].knot[p] = (float)p / (float)H;
+      hroots[b].base[p] = (float)p / (float)H;
+      hroots[b].slope[p] = 1.f;
     }
-    hroots[b].b2 = init_param(3 * H);
     hroots[b].n_leaves = (uint32_t)nl;
     hroots[b].leaf_off = total_leaves;
     hroots[b].use_learned = n > 0;

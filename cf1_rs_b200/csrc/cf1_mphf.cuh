@@ -8,7 +8,7 @@
 //   * the learned index: a small MLP root picks a leaf, the leaf's linear
 //     model predicts the rank, and a search in [pred - err, pred + err] of the
 //     bin's sorted keys finds the exact rank, which is the local slot.
-// Both evaluate identically on the host (cf1_host_query.cpp), so every
+// Both evaluate identically on the host (cf1_export.cu), so every
 // floating-point step is an explicitly rounded single operation.
 #pragma once
 #include "cf1_internal.cuh"
@@ -17,17 +17,56 @@ namespace cf1 {
 
 constexpr uint64_t SLOT_NONE = ~0ull;
 
-CF1_HD uint64_t bb_seed(uint32_t level) { return 0x9E3779B97F4A7C15ull * (uint64_t)(level + 1) ^ 0xD1B54A32D192ED03ull; }
+// BBHash hashing: one 64-bit hash H of the key; level l takes the top bits
+// of H * BB_MUL[l] (odd, independent per level), scaled to the block size.
+// Two keys that collide at one level differ in H, and the product's top bits
+// spread that difference afresh at every level, so their next collision is
+// as unlikely as a fresh one.
+constexpr uint64_t BB_SEED = 0xD1B54A32D192ED03ull;
+constexpr uint32_t BB_MAX_LEVELS = 64;
+#define CF1_BB_MUL_TABLE                                                                       \
+  {0x9444bd23aedfa6f5ull, 0x358e91a8e48b97dbull, 0x970f24b9078ea7c7ull, 0x8f4bacefadb4bcb1ull, \
+   0xa1802fdd5c8f452bull, 0xde85f58b25603303ull, 0x364762f470077587ull, 0x7f864ce0775a0c77ull, \
+   0x73cc8629f782b791ull, 0x5b3cac1b3a1059edull, 0xf3f2d21e76f5d423ull, 0x5311b35a85f468b1ull, \
+   0x9e88fd5a131be1adull, 0x9e9c01811d2017e5ull, 0x129062e2de60e9ffull, 0x56392910d55d4001ull, \
+   0x369f3d3960628741ull, 0x07d07f6fa9535d11ull, 0xd28c09328db0b0b1ull, 0x1ae6162a1a4d4957ull, \
+   0xb1210c3c3e2d9b4dull, 0x4f6d46e98e254fa1ull, 0x7769e3490c7cff51ull, 0xaa0e641aed9e44d9ull, \
+   0x9af1b4f518c92531ull, 0xad08829c8b86913dull, 0x74b11bbb7c9b68b5ull, 0xf88c91c7a171ab17ull, \
+   0x6f3ef252b55ad381ull, 0x4913fb1d991cf239ull, 0x08665c7e23c0234full, 0x680bd205a47aa7fbull, \
+   0xab26a44018d9d3ebull, 0xf38a638278b6472dull, 0x96db61b024ebdb5bull, 0xa8a816634336b1e3ull, \
+   0x6d4ee8af9b7d3935ull, 0x6996bb528191ecf1ull, 0xd9054779fe0087cdull, 0x225b83001770e169ull, \
+   0xc2cdad46272294abull, 0xe3e791cdd9a11fbfull, 0x37378255f5fd2a7bull, 0xd2b93a15118fee2bull, \
+   0x7db37ee48f069867ull, 0x09670f4e3d3e2fd9ull, 0xe9beb57f8493c53full, 0x47921d41eea996ebull, \
+   0xdf3db336bee3959full, 0x9ed13e46eb4adfebull, 0x137132bc0e302887ull, 0xda532fced984988bull, \
+   0x3939421e2266f117ull, 0x55db8408d8b43be9ull, 0x9b3c3b4a24da4965ull, 0x397e02be01aca861ull, \
+   0x723c864e2ada4953ull, 0x533aa12154e09b8full, 0x516fa0ddd045e98bull, 0x8da77e07eff2b063ull, \
+   0xe9b3bdcdc9c409cdull, 0x9b6df4ffc06e320full, 0x0550f8043685bb11ull, 0x42c2a6bcdd74430bull}
+static __constant__ uint64_t c_bb_mul[BB_MAX_LEVELS] = CF1_BB_MUL_TABLE;
+static const uint64_t h_bb_mul[BB_MAX_LEVELS] = CF1_BB_MUL_TABLE;
+
+template <class KeyT>
+CF1_HD uint64_t bb_key_hash(const KeyT &key) { return KOps<KeyT>::hash(key, BB_SEED); }
+
+// Bit of a key (hash H) in a block of nwords words at level l.
+CF1_HD uint64_t bb_pos(uint64_t H, uint32_t l, uint32_t nwords) {
+#ifdef __CUDA_ARCH__
+  const uint64_t mul = c_bb_mul[l];
+#else
+  const uint64_t mul = h_bb_mul[l];
+#endif
+  return mulhi64(H * mul, (uint64_t)nwords << 6);
+}
 
 template <class KeyT>
 CF1_HD uint64_t bb_local_slot(const BBView &v, uint32_t bin, const KeyT &key) {
+  const uint64_t H = bb_key_hash(key);
   for (uint32_t l = 0; l < v.levels; l++) {
     const BBMeta mt = v.meta[(uint64_t)l * v.nbins + bin];
-    if (mt.m_bits == 0) return SLOT_NONE;
-    uint64_t pos = mulhi64(KOps<KeyT>::hash(key, bb_seed(l)), mt.m_bits);
-    const ulonglong2 e = v.AR[l][mt.word_off + (pos >> 6)];
-    uint32_t bit = (uint32_t)(pos & 63);
-    if ((e.x >> bit) & 1) return mt.rank_adj + e.y + (uint64_t)popc64(e.x & ((1ull << bit) - 1));
+    if (mt.nwords == 0) return SLOT_NONE;
+    const uint64_t pos = bb_pos(H, l, mt.nwords);
+    const ulonglong2 e = v.AR[mt.word_off + (pos >> 6)];
+    const uint32_t bit = (uint32_t)(pos & 63);
+    if ((e.x >> bit) & 1) return (uint32_t)(mt.rank_adj + (uint32_t)e.y + (uint32_t)popc64(e.x & ((1ull << bit) - 1)));
   }
   return SLOT_NONE;
 }
@@ -54,6 +93,13 @@ CF1_HD float u64_to_f(uint64_t x) {
   return (float)x;
 #endif
 }
+CF1_HD float f_sub(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fsub_rn(a, b);
+#else
+  return a - b;
+#endif
+}
 CF1_HD int64_t f_round(float x) {
 #ifdef __CUDA_ARCH__
   return (int64_t)__float2ll_rn(x);
@@ -66,13 +112,15 @@ CF1_HD int64_t f_round(float x) {
 // scaled to [0, 1].
 CF1_HD float li_x(const LIRoot &r, uint64_t h) { return f_mul(u64_to_f(h - r.hmin), r.inv_range); }
 
-// Hidden activation: clipped ReLU, clamp(z, 0, 1).
+// Hidden activation of the training network: clipped ReLU, clamp(z, 0, 1).
 CF1_HD float li_act(float z) { return z > 0.f ? (z < 1.f ? z : 1.f) : 0.f; }
 
+// The root on its piecewise-linear form: find the piece, one fma.
 CF1_HD float li_root_eval(const LIRoot &r, float x) {
-  float y = r.b2;
-  for (int j = 0; j < LI_HIDDEN; j++) y = f_fma(r.w2[j], li_act(f_fma(r.w1[j], x, r.b1[j])), y);
-  return y;
+  uint32_t j = 0;
+#pragma unroll
+  for (int i = 1; i < LI_HIDDEN; i++) j += x >= r.knot[i] ? 1u : 0u;
+  return f_fma(r.slope[j], f_sub(x, r.knot[j]), r.base[j]);
 }
 
 CF1_HD uint32_t li_leaf_of(const LIRoot &r, float y) {

@@ -217,12 +217,13 @@ __global__ void __launch_bounds__(BS_BLOCK) bin_scatter_kernel(const uint64_t *r
 void launch_sk(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
   if (a.n_tiles == 0) return;
   size_t smem = 2 * (a.tile + 64) * sizeof(uint64_t);
-  unsigned grid = persistent_ctas > 0 ? (unsigned)persistent_ctas : (unsigned)a.n_tiles;
   switch (a.tile) {
 #define CF1_SK_CASE(IT)                                                                              \
   case SK_BLOCK * IT: {                                                                            \
     auto kern = superkmer_kernel<SK_BLOCK, IT>;                                                    \
     CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    unsigned grid = persistent_ctas ? persistent_grid(kern, SK_BLOCK, smem, persistent_ctas, a.n_tiles) \
+                                    : (unsigned)a.n_tiles;                                         \
     kern<<<grid, SK_BLOCK, smem, s>>>(a);                                                          \
     break;                                                                                         \
   }

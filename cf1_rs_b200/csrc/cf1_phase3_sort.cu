@@ -223,9 +223,10 @@ void launch_expand(const uint64_t *records, uint64_t n_rec, const uint64_t *kpre
                    uint64_t n_keys, uint64_t L, uint32_t *queue, uint32_t *err, int persistent_ctas, cudaStream_t s) {
   if (n_rec == 0) return;
   uint64_t warps = ceil_div(n_rec, 32);
-  unsigned grid = persistent_ctas > 0 ? (unsigned)persistent_ctas : (unsigned)ceil_div(warps, 8);
+  unsigned grid = persistent_ctas ? persistent_grid(expand_kernel<KeyT>, 256, 0, persistent_ctas, ceil_div(warps, 8))
+                                  : (unsigned)ceil_div(warps, 8);
   expand_kernel<KeyT><<<grid, 256, 0, s>>>(records, n_rec, kpre, W, k, keys, n_keys, L,
-                                           persistent_ctas > 0 ? queue : nullptr, err);
+                                           persistent_ctas ? queue : nullptr, err);
   CF1_LAUNCH_CHECK();
 }
 

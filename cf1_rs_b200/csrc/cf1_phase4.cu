@@ -6,10 +6,14 @@
 // same per-occurrence step runs over the routed super k-mers, bin after bin,
 // so one bin's MPHF blocks and state words are what the SMs touch at a time.
 // Each occurrence reads its true neighbours from the resident sequence, so the
-// k-mer's (front, back) contribution is exactly the reference's; the state
-// word is updated by a 64-bit atomicCAS loop on the reference layout (12 five-
-// bit states per word, LSB first).  The DFA is a per-side join, so the final
-// words do not depend on the order of the updates.
+// k-mer's (front, back) contribution is exactly the reference's.  The DFA is
+// a per-side join, so the final words do not depend on the order of the
+// updates, and two update modes give the same words:
+//   * side sets (default): each occurrence ORs its side-set byte into the
+//     vertex's byte with a fire-and-forget atomic (no read, no retry); a
+//     streaming pass then packs the bytes into the reference layout;
+//   * CAS: a 64-bit atomicCAS loop directly on the reference layout (12 five-
+//     bit states per word, LSB first), as src/state_vector.rs:47-70 does.
 #include "cf1_device_util.cuh"
 #include "cf1_internal.cuh"
 #include "cf1_mphf.cuh"
@@ -42,7 +46,7 @@ CF1_D void state_join_cas(unsigned long long *states, uint64_t slot, uint32_t c,
   atomicOr(err, (uint32_t)DEV_CAS_LIMIT);
 }
 
-template <class KeyT>
+template <class KeyT, bool SIDESET>
 __global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a) {
   const unsigned lane = lane_id();
   const uint64_t n_chunks = (a.n_rec + 31) / 32;
@@ -73,20 +77,24 @@ __global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a
       }
       uint64_t orec = __shfl_sync(FULL, rec, lo);
       uint32_t oex = __shfl_sync(FULL, excl, lo);
-      uint64_t p = rec_pos(orec) + (j - oex);
+      const uint32_t q = j - oex;  // k-mer q of the super k-mer
+      uint64_t p = rec_pos(orec) + q;
       if (j < total && p + k > a.L) {
         atomicOr(a.err, (uint32_t)DEV_OVERFLOW);
       } else if (j < total) {
         uint32_t bin = rec_bin(orec);
         KeyT fw = KOps<KeyT>::extract(a.W, p, k);
         KeyT rc = KOps<KeyT>::rc(fw, k);
-        bool hp = p > 0 && !is_n(a.NM, p - 1);
-        bool hn = p + k < a.L && !is_n(a.NM, p + k);
+        // Inside a super k-mer the k-mers before and after are valid windows,
+        // so only its first and last k-mers can lack a neighbour.
+        bool hp = q > 0 || (p > 0 && !is_n(a.NM, p - 1));
+        bool hn = q + 1 < rec_n(orec) || (p + k < a.L && !is_n(a.NM, p + k));
         uint32_t pb = hp ? base_at(a.W, p - 1) : 0;
         uint32_t nb = hn ? base_at(a.W, p + k) : 0;
         uint32_t c = contribution(fw, rc, hp, pb, hn, nb, k);
         uint64_t slot = mphf_slot(a.mphf, bin, kmin(fw, rc));
         if (slot == SLOT_NONE) atomicOr(a.err, (uint32_t)DEV_MPHF_MISS);
+        else if (SIDESET) atomicOr(a.sides + (slot >> 2), sideset_of_state(c) << (8 * (uint32_t)(slot & 3)));
         else state_join_cas(a.states, slot, c, a.err, retries);
       }
     }
@@ -94,6 +102,23 @@ __global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a
   }
   retries = warp_sum(retries);
   if (lane == 0 && retries) atomicAdd(a.cas_retries, (unsigned long long)retries);
+}
+
+// Word w of the state vector from side-set bytes 12w .. 12w+11 (three u32).
+constexpr int PK_BLOCK = 256;
+__global__ void __launch_bounds__(PK_BLOCK) sideset_pack_kernel(const uint32_t *sides, uint64_t nwords,
+                                                                unsigned long long *states) {
+  __shared__ uint8_t lut[256];  // side-set byte -> 5-bit state
+  lut[threadIdx.x] = (uint8_t)state_of_sideset(threadIdx.x);
+  __syncthreads();
+  uint64_t w = (uint64_t)blockIdx.x * PK_BLOCK + threadIdx.x;
+  if (w >= nwords) return;
+  const uint32_t *q = sides + 3 * w;
+  uint32_t b[3] = {q[0], q[1], q[2]};
+  unsigned long long out = 0;
+#pragma unroll
+  for (int j = 0; j < 12; j++) out |= (unsigned long long)lut[(b[j >> 2] >> (8 * (j & 3))) & 0xFFu] << (5 * j);
+  states[w] = out;
 }
 
 template <class KeyT>
@@ -160,8 +185,20 @@ template <class KeyT>
 void launch_classify(const ClassifyArgs<KeyT> &a, int persistent_ctas, cudaStream_t s) {
   if (a.n_rec == 0) return;
   uint64_t warps = (a.n_rec + 31) / 32;
-  unsigned grid = persistent_ctas > 0 ? (unsigned)persistent_ctas : (unsigned)ceil_div(warps, CL_BLOCK / 32);
-  classify_kernel<KeyT><<<grid, CL_BLOCK, 0, s>>>(a);
+  const uint64_t ctas = ceil_div(warps, CL_BLOCK / 32);
+  if (a.sides) {
+    auto kern = classify_kernel<KeyT, true>;
+    kern<<<persistent_ctas ? persistent_grid(kern, CL_BLOCK, 0, persistent_ctas, ctas) : (unsigned)ctas, CL_BLOCK, 0, s>>>(a);
+  } else {
+    auto kern = classify_kernel<KeyT, false>;
+    kern<<<persistent_ctas ? persistent_grid(kern, CL_BLOCK, 0, persistent_ctas, ctas) : (unsigned)ctas, CL_BLOCK, 0, s>>>(a);
+  }
+  CF1_LAUNCH_CHECK();
+}
+
+void launch_sideset_pack(const uint32_t *sides, uint64_t nwords, unsigned long long *states, cudaStream_t s) {
+  if (!nwords) return;
+  sideset_pack_kernel<<<(unsigned)ceil_div(nwords, PK_BLOCK), PK_BLOCK, 0, s>>>(sides, nwords, states);
   CF1_LAUNCH_CHECK();
 }
 

@@ -13,7 +13,8 @@ struct ClassifyArgs {
   uint64_t L;
   int k;
   MphfView<KeyT> mphf;
-  unsigned long long *states;   // ceil(n_distinct/12) words, zeroed
+  unsigned long long *states;   // CAS mode: ceil(n_distinct/12) words, zeroed
+  uint32_t *sides;              // side-set mode: 12 * ceil(n_distinct/12) bytes, zeroed; nullptr = CAS mode
   uint32_t *queue;              // persistent mode work counter (zeroed), else nullptr
   uint32_t *err;
   unsigned long long *cas_retries;
@@ -21,6 +22,9 @@ struct ClassifyArgs {
 
 template <class KeyT>
 void launch_classify(const ClassifyArgs<KeyT> &a, int persistent_ctas, cudaStream_t s);
+
+// Packs side-set bytes (3 u32 per state word) into nwords state words.
+void launch_sideset_pack(const uint32_t *sides, uint64_t nwords, unsigned long long *states, cudaStream_t s);
 
 template <class KeyT>
 void launch_dump(const MphfView<KeyT> &m, uint32_t nbins, uint64_t n, const unsigned long long *states, uint64_t *keys_out,

@@ -112,7 +112,8 @@ void run_impl(cf1gpu_ctx *c) {
   a.n_kmers = &sm->n_kmers;
   a.rec_count = &sm->rec_count;
   a.err = &sm->err;
-  int pctas = batched ? (c->tune.persistent_ctas > 0 ? c->tune.persistent_ctas : 4 * c->num_sms) : 0;
+  // persistent launches: the tuned CTA count, else one full wave (-1)
+  int pctas = batched ? (c->tune.persistent_ctas > 0 ? c->tune.persistent_ctas : -1) : 0;
   a.tile_counter = batched ? &sm->queues[0] : nullptr;
   uint16_t *lut = c->d_lut.get<uint16_t>(NUM_BUCKETS);
   uint64_t *rec_off = c->d_rec_off.get<uint64_t>(B + 1);
@@ -194,9 +195,18 @@ void run_impl(cf1gpu_ctx *c) {
   CF1_CUDA(cudaEventRecord(c->ev[4], s));
 
   // ---- phase 4: classification
+  // Side-set mode keeps one byte per vertex in the key buffer, which is free
+  // once the MPHF is built (12 * nwords <= n_distinct + 11 <= 8 * (NO + 1)).
   const uint64_t nwords = ceil_div(c->n_distinct, 12);
+  const bool sideset = c->opts.state_update == 0;
   unsigned long long *states = c->d_states.get<unsigned long long>(nwords + 1);
-  CF1_CUDA(cudaMemsetAsync(states, 0, (nwords + 1) * sizeof(unsigned long long), s));
+  uint32_t *sides = sideset ? reinterpret_cast<uint32_t *>(keys) : nullptr;
+  if (sideset) {
+    CF1_CUDA(cudaMemsetAsync(sides, 0, nwords * 12, s));
+    CF1_CUDA(cudaMemsetAsync(states + nwords, 0, sizeof(unsigned long long), s));
+  } else {
+    CF1_CUDA(cudaMemsetAsync(states, 0, (nwords + 1) * sizeof(unsigned long long), s));
+  }
   ClassifyArgs<KeyT> ca;
   ca.records = records;
   ca.n_rec = NS;
@@ -206,12 +216,15 @@ void run_impl(cf1gpu_ctx *c) {
   ca.k = k;
   ca.mphf = make_view<KeyT>(c);
   ca.states = states;
+  ca.sides = sides;
   ca.queue = batched ? &sm->queues[3] : nullptr;
   ca.err = &sm->err;
   ca.cas_retries = &sm->cas_retries;
   CF1_CUDA(cudaEventRecord(c->ev[5], s));
-  launch_classify<KeyT>(ca, batched ? 8 * c->num_sms : 0, s);
+  launch_classify<KeyT>(ca, pctas, s);
   CF1_CUDA(cudaEventRecord(c->ev[6], s));
+  if (sideset) launch_sideset_pack(sides, nwords, states, s);
+  CF1_CUDA(cudaEventRecord(c->ev[7], s));
   CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaStreamSynchronize(s));
   check_device_errors(hs.err);
@@ -241,9 +254,9 @@ void run_impl(cf1gpu_ctx *c) {
   st.ms_phase2 = elapsed(c->ev[1], c->ev[2]);
   st.ms_phase3_sort = elapsed(c->ev[2], c->ev[3]);
   st.ms_phase3_mphf = elapsed(c->ev[3], c->ev[4]);
-  st.ms_phase4 = elapsed(c->ev[4], c->ev[6]);
+  st.ms_phase4 = elapsed(c->ev[4], c->ev[7]);
   st.ms_classify_kernel = elapsed(c->ev[5], c->ev[6]);
-  st.ms_total = elapsed(c->ev[0], c->ev[6]);
+  st.ms_total = elapsed(c->ev[0], c->ev[7]);
 }
 
 template <class KeyT>

@@ -65,7 +65,8 @@ typedef struct cf1gpu_opts {
   uint32_t num_bins;          /* --num-bins (src/params.rs:58-59), 1..4096 */
   int32_t device;             /* CUDA device ordinal */
   uint32_t mphf_mode;         /* CF1GPU_MPHF_* */
-  uint32_t batched;           /* 1: persistent queue kernels + CUDA graph replay */
+  uint32_t batched;           /* 1: persistent work-queue kernels (one full-occupancy wave per phase kernel
+                                 pulling fixed-size chunks from an atomic queue) */
   uint32_t track_short_seqs;  /* --track-short-seqs (src/params.rs:45-47) */
   const char *tuner_cache_path; /* autotuner cache file, NULL = built-in defaults */
   uint32_t learned_max_err;   /* learned index: per-bin error bound above which the bin falls back to BBHash (0 = default 1024) */
@@ -74,7 +75,10 @@ typedef struct cf1gpu_opts {
   uint32_t sk_tile;           /* k-mer positions per minimizer tile: 1024, 2048 or 4096 (0 = tuner / default) */
   uint32_t sort_mode;         /* phase-3 sort: 0 = per-bin MSD + shared-memory sort (LSD when a sub-bucket
                                  overflows), 1 = segmented LSD radix sort only */
-  uint32_t reserved[3];
+  uint32_t state_update;      /* phase-4 state update: 0 = side-set bytes joined by atomic OR, then packed;
+                                 1 = atomicCAS loop on the packed words (src/state_vector.rs:47-70).
+                                 Both give the same words. */
+  uint32_t reserved[2];
 } cf1gpu_opts;
 
 typedef struct cf1gpu_stats {

@@ -53,6 +53,22 @@ def test_sort_modes(k, sort_mode):
     g.close()
 
 
+@pytest.mark.parametrize("mode", ["bbhash", "learned"])
+@pytest.mark.parametrize("k", [5, 31, 33, 63])
+def test_state_update_modes(k, mode):
+    # side-set OR + pack and the CAS loop on packed words give the same words
+    recs = random_records(900 + k, k, n_records=120, max_len=5000)
+    seq, off = o.concat_records(recs)
+    words = {}
+    for upd in ("sideset", "cas"):
+        g, _ = assert_parity(seq, off, k, mode=mode, num_bins=16, state_update=upd)
+        words[upd] = g.states()
+        if upd == "sideset":
+            assert g.stats()["classify_cas_retries"] == 0
+        g.close()
+    assert np.array_equal(words["sideset"], words["cas"])
+
+
 @pytest.mark.parametrize("k", [31, 63])
 def test_oversized_subbucket(k):
     # a long homopolymer and a tandem repeat put tens of thousands of copies of
