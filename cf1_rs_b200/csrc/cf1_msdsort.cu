@@ -34,11 +34,28 @@ constexpr uint32_t CS_DEDUP_MIN = 64;  // 64-bit sub-buckets above this size are
 template <class KeyT>
 constexpr uint32_t cs_cap() { return KOps<KeyT>::WORDS == 1 ? 8192u : 4096u; }
 
+// Digit of a key in a multisplit pass: bits [shift, shift + width) of the key
+// or, when only the distinct keys and not their order are needed (hashed),
+// of key * MS_HASH_MUL.  The product's top bits spread any key set evenly,
+// where the key's own top bits -- the first bases of a canonical k-mer --
+// are skewed several-fold.  (64-bit keys; wider keys always sort.)
+constexpr uint64_t MS_HASH_MUL = 0xD6E8FEB86659FD93ull;
+template <class KeyT>
+CF1_D uint32_t ms_digit(const KeyT &k, int shift, uint32_t mask, bool hashed);
+template <>
+CF1_D uint32_t ms_digit<uint64_t>(const uint64_t &k, int shift, uint32_t mask, bool hashed) {
+  return (uint32_t)((hashed ? k * MS_HASH_MUL : k) >> shift) & mask;
+}
+template <>
+CF1_D uint32_t ms_digit<Key2>(const Key2 &k, int shift, uint32_t mask, bool) {
+  return KOps<Key2>::digit(k, shift, mask);
+}
+
 // ---------------------------------------------------------------- multisplit pass
 template <class KeyT, int BITS>
 __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, const uint64_t *seg_off,
                                                            const uint32_t *tile_off, uint32_t nseg, int shift,
-                                                           uint32_t *H) {
+                                                           bool hashed, uint32_t *H) {
   constexpr uint32_t DIG = 1u << BITS;
   __shared__ uint32_t h[DIG];
   const uint32_t t = blockIdx.x;
@@ -50,7 +67,7 @@ __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, con
   __syncthreads();
   TileSpan sp = tile_span(seg_off, tile_off, nseg, t, MS_TILE);
   for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += MS_BLOCK)
-    atomicAdd(&h[KOps<KeyT>::digit(keys[i], shift, DIG - 1)], 1u);
+    atomicAdd(&h[ms_digit(keys[i], shift, DIG - 1, hashed)], 1u);
   __syncthreads();
   for (uint32_t d = threadIdx.x; d < DIG; d += MS_BLOCK)
     H[(uint64_t)sp.first_tile * DIG + (uint64_t)d * sp.ntiles + (t - sp.first_tile)] = h[d];
@@ -65,7 +82,7 @@ __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, con
 template <class KeyT, int BITS>
 __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
                                                                  const uint32_t *tile_off, uint32_t nseg, int shift,
-                                                                 const uint64_t *Hs) {
+                                                                 bool hashed, const uint64_t *Hs) {
   constexpr uint32_t DIG = 1u << BITS;
   extern __shared__ __align__(16) unsigned char ms_smem[];
   KeyT *stage = reinterpret_cast<KeyT *>(ms_smem);                            // [MS_TILE]
@@ -92,7 +109,7 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
   for (int r = 0; r < MS_ITEMS; r++) {
     uint32_t li = warp * (MS_ITEMS * 32) + r * 32 + lane;
     bool act = li < n;
-    uint32_t d = act ? KOps<KeyT>::digit(in[sp.start + li], shift, DIG - 1) : 0xFFFFFFFFu;
+    uint32_t d = act ? ms_digit(in[sp.start + li], shift, DIG - 1, hashed) : 0xFFFFFFFFu;
     unsigned peers = __match_any_sync(FULL, d);
     unsigned leader = __ffs(peers) - 1;
     uint32_t old = 0;
@@ -141,7 +158,7 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
   __syncthreads();
   for (uint32_t i = tid; i < n; i += MS_BLOCK) {
     KeyT kk = stage[i];
-    uint32_t d = KOps<KeyT>::digit(kk, shift, DIG - 1);
+    uint32_t d = ms_digit(kk, shift, DIG - 1, hashed);
     out[base[d] + (i - lstart[d])] = kk;
   }
 }
@@ -177,37 +194,61 @@ CF1_D void cs_swap_if(KeyT &a, KeyT &b, bool up) {
 // Replaces T[a, a+n) by its distinct keys (any order) through an
 // open-addressing set in shared memory; returns their count, or ~0u when
 // they do not fit in three quarters of the set.  Every probe sequence is
-// bounded by the set size.
+// bounded by the set size.  Warps step through the keys together, so the
+// insert count and the give-up test are per warp; the set is emptied into T
+// a warp-sized group of slots at a time.
 CF1_D uint32_t cs_hash_dedup(uint64_t *T, uint64_t a, uint64_t n, uint64_t *S, uint32_t cap, uint32_t *s_cnt,
                              uint32_t *sm) {
-  const unsigned tid = threadIdx.x;
+  (void)sm;
+  const unsigned tid = threadIdx.x, lane = lane_id();
   const uint64_t EMPTY = ~0ull;  // above every key (keys use at most 62 bits)
-  uint32_t tsize = 64;           // a power of two >= 2n, at most cap
-  while (tsize < cap && (uint64_t)tsize < 2 * n) tsize <<= 1;
+  uint32_t tsize = 64, tbits = 6;  // a power of two >= 2n, at most cap
+  while (tsize < cap && (uint64_t)tsize < 2 * n) {
+    tsize <<= 1;
+    tbits++;
+  }
   for (uint32_t i = tid; i < tsize; i += CS_BLOCK) S[i] = EMPTY;
   if (tid == 0) *s_cnt = 0;
   __syncthreads();
   const uint32_t limit = tsize / 4 * 3;
-  for (uint64_t i = tid; i < n; i += CS_BLOCK) {
-    if (*reinterpret_cast<volatile uint32_t *>(s_cnt) > limit) break;
-    uint64_t key = T[a + i];
-    uint32_t h = (uint32_t)KOps<uint64_t>::hash(key, 0x5851F42D4C957F2Dull) & (tsize - 1);
-    for (uint32_t probe = 0; probe < tsize; probe++) {
-      unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long *>(S + h), EMPTY, key);
-      if (old == EMPTY) {
-        atomicAdd(s_cnt, 1u);
-        break;
+  for (uint64_t base = tid - lane; base < n; base += CS_BLOCK) {
+    uint32_t seen = 0;
+    if (lane == 0) seen = *reinterpret_cast<volatile uint32_t *>(s_cnt);
+    if (__shfl_sync(FULL, seen, 0) > limit) break;
+    const uint64_t i = base + lane;
+    bool added = false;
+    if (i < n) {
+      const uint64_t key = T[a + i];
+      uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - tbits));  // multiplicative hashing
+      for (uint32_t probe = 0; probe < tsize; probe++) {
+        unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long *>(S + h), EMPTY, key);
+        if (old == EMPTY) {
+          added = true;
+          break;
+        }
+        if (old == key) break;
+        h = (h + 1) & (tsize - 1);
       }
-      if (old == key) break;
-      h = (h + 1) & (tsize - 1);
     }
+    const unsigned b = __ballot_sync(FULL, added);
+    if (lane == 0 && b) atomicAdd(s_cnt, (uint32_t)__popc(b));
   }
   __syncthreads();
-  uint32_t d = *s_cnt;
+  const uint32_t d = *s_cnt;
+  __syncthreads();
   if (d > limit) return ~0u;
-  // compact the occupied slots to T[a, a+d)
-  block_select<CS_BLOCK>(
-      tsize, [&](uint32_t i) { return S[i] != EMPTY; }, [&](uint32_t i, uint32_t r) { T[a + r] = S[i]; }, sm);
+  if (tid == 0) *s_cnt = 0;
+  __syncthreads();
+  for (uint32_t base = tid - lane; base < tsize; base += CS_BLOCK) {
+    const uint64_t v = S[base + lane];
+    const bool f = v != EMPTY;
+    const unsigned b = __ballot_sync(FULL, f);
+    uint32_t o = 0;
+    if (lane == 0 && b) o = atomicAdd(s_cnt, (uint32_t)__popc(b));
+    o = __shfl_sync(FULL, o, 0);
+    if (f) T[a + o + __popc(b & lanemask_lt())] = v;
+  }
+  __syncthreads();
   return d;
 }
 
@@ -313,14 +354,16 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
       sh.sm);
 }
 
-// Sorted distinct keys of one sub-bucket T[a, a+n), written back at a.
+// Sorted distinct keys of one sub-bucket T[a, a+n), written back at a
+// (SORTED = false: distinct keys in any order -- 64-bit keys then skip the
+// sort whenever the shared-memory set holds the sub-bucket).
 // Sub-buckets above CAP keys: 64-bit keys are first reduced to one copy each
 // through a shared-memory set; if still above CAP, the sub-bucket is split on
 // its next `bits` bits into U[a, a+n) (the free ping-pong buffer), runs of
 // consecutive pieces up to CAP keys are sorted one after another, and their
 // distinct keys are appended at T[a].  Only a single piece above CAP keys
 // makes the kernel report the sub-bucket as oversized.
-template <class KeyT>
+template <class KeyT, bool SORTED>
 __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT *U, const uint64_t *sb_off,
                                                                   uint64_t nsub, int shift, int bits, uint32_t *cnt,
                                                                   uint32_t *oversize) {
@@ -348,11 +391,15 @@ __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT 
   bool distinct = false;
   // 64-bit keys: one copy of each key first.  Repeats put hundreds of copies
   // of a k-mer in one bucket, where sorting copies would dominate the work.
-  if (n > CS_DEDUP_MIN && KOps<KeyT>::WORDS == 1) {
+  if ((!SORTED || n > CS_DEDUP_MIN) && KOps<KeyT>::WORDS == 1) {
     uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(T), a, n, reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
     if (d != ~0u) {
       m = d;
       distinct = true;
+      if (!SORTED) {  // distinct keys are all that is needed
+        if (tid == 0) cnt[j] = d;
+        return;
+      }
     }
   }
   if (m <= CAP) {
@@ -461,7 +508,7 @@ __global__ void cs_bin_off_kernel(const uint64_t *out_off, uint32_t nbins, uint6
 }
 
 template <class KeyT, int BITS>
-void ms_pass(const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift,
+void ms_pass(const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift, bool hashed,
              MsdScratch &sc, cudaStream_t s) {
   constexpr uint32_t DIG = 1u << BITS;
   uint32_t ub = (uint32_t)(ceil_div(n, MS_TILE) + nseg);
@@ -469,27 +516,27 @@ void ms_pass(const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uin
   segment_tiles(seg_off, nseg, MS_TILE, tile_off, s);
   uint32_t *H = sc.hist.get<uint32_t>((uint64_t)ub * DIG);
   uint64_t *Hs = sc.hscan.get<uint64_t>((uint64_t)ub * DIG + 1);
-  ms_hist_kernel<KeyT, BITS><<<ub, MS_BLOCK, 0, s>>>(in, seg_off, tile_off, nseg, shift, H);
+  ms_hist_kernel<KeyT, BITS><<<ub, MS_BLOCK, 0, s>>>(in, seg_off, tile_off, nseg, shift, hashed, H);
   CF1_LAUNCH_CHECK();
   exclusive_scan_u32(H, Hs, (uint64_t)ub * DIG, sc.scan_tmp, s);
   size_t smem = MS_TILE * sizeof(KeyT) + (MS_NW + 1) * DIG * sizeof(uint32_t) + DIG * sizeof(uint64_t);
   CF1_CUDA(cudaFuncSetAttribute(ms_scatter_kernel<KeyT, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  ms_scatter_kernel<KeyT, BITS><<<ub, MS_BLOCK, smem, s>>>(in, out, seg_off, tile_off, nseg, shift, Hs);
+  ms_scatter_kernel<KeyT, BITS><<<ub, MS_BLOCK, smem, s>>>(in, out, seg_off, tile_off, nseg, shift, hashed, Hs);
   CF1_LAUNCH_CHECK();
 }
 
 template <class KeyT>
 void ms_pass_bits(int bits, const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift,
-                  MsdScratch &sc, cudaStream_t s) {
+                  bool hashed, MsdScratch &sc, cudaStream_t s) {
   switch (bits) {
-    case 1: ms_pass<KeyT, 1>(in, out, n, seg_off, nseg, shift, sc, s); break;
-    case 2: ms_pass<KeyT, 2>(in, out, n, seg_off, nseg, shift, sc, s); break;
-    case 3: ms_pass<KeyT, 3>(in, out, n, seg_off, nseg, shift, sc, s); break;
-    case 4: ms_pass<KeyT, 4>(in, out, n, seg_off, nseg, shift, sc, s); break;
-    case 5: ms_pass<KeyT, 5>(in, out, n, seg_off, nseg, shift, sc, s); break;
-    case 6: ms_pass<KeyT, 6>(in, out, n, seg_off, nseg, shift, sc, s); break;
-    case 7: ms_pass<KeyT, 7>(in, out, n, seg_off, nseg, shift, sc, s); break;
-    case 8: ms_pass<KeyT, 8>(in, out, n, seg_off, nseg, shift, sc, s); break;
+    case 1: ms_pass<KeyT, 1>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
+    case 2: ms_pass<KeyT, 2>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
+    case 3: ms_pass<KeyT, 3>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
+    case 4: ms_pass<KeyT, 4>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
+    case 5: ms_pass<KeyT, 5>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
+    case 6: ms_pass<KeyT, 6>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
+    case 7: ms_pass<KeyT, 7>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
+    case 8: ms_pass<KeyT, 8>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
     default: throw Error(-1, "MSD pass width must be 1..8 bits");
   }
 }
@@ -529,8 +576,11 @@ int msd_prefix_bits(uint64_t max_bin_keys) {
 
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
-                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s) {
-  // passes on the top P bits: P1 then P2 (P2 may be 0)
+                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted) {
+  // passes on the top P bits: P1 then P2 (P2 may be 0) -- of the key, or of
+  // its hash when only distinct keys are wanted (64-bit keys)
+  const bool hashed = !sorted && KOps<KeyT>::WORDS == 1;
+  if (hashed) key_bits = 64;
   const int P1 = P > 8 ? (P + 1) / 2 : P, P2 = P - P1;
   KeyT *T = keys;
   uint64_t nsub = (uint64_t)nbins << P;
@@ -538,7 +588,7 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
   if (P == 0) {
     CF1_CUDA(cudaMemcpyAsync(sb_off, seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
   } else if (n) {
-    ms_pass_bits<KeyT>(P1, keys, alt, n, seg_off, nbins, key_bits - P1, sc, s);
+    ms_pass_bits<KeyT>(P1, keys, alt, n, seg_off, nbins, key_bits - P1, hashed, sc, s);
     const uint64_t *seg2 = seg_off;
     uint32_t nseg2 = nbins;
     if (P2) {
@@ -547,7 +597,7 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
       subbuckets_bits(P1, seg_off, sc.tile_off.as<uint32_t>(), nbins, sc.hscan.as<uint64_t>(), sb1, s);
       nseg2 = (uint32_t)((uint64_t)nbins << P1);
       seg2 = sb1;
-      ms_pass_bits<KeyT>(P2, alt, keys, n, seg2, nseg2, key_bits - P1 - P2, sc, s);
+      ms_pass_bits<KeyT>(P2, alt, keys, n, seg2, nseg2, key_bits - P1 - P2, hashed, sc, s);
       T = keys;
     } else {
       T = alt;
@@ -566,14 +616,18 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
     bits = 1;  // every key of a sub-bucket is equal: one bucket
     shift = 0;
   }
+  if (hashed) {  // the key's own bits: any bits split a sub-bucket into pieces
+    bits = CS_BITS;
+    shift = 0;
+  }
   // S, hist, cur, pstart (u32) and the chunk bounds (u16)
   size_t smem = cs_cap<KeyT>() * sizeof(KeyT) + (3 * CS_BUCKETS + 1) * sizeof(uint32_t) +
                 (CS_BUCKETS + 1) * sizeof(uint16_t);
-  CF1_CUDA(cudaFuncSetAttribute(cs_sort_unique_kernel<KeyT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  auto kern = sorted ? cs_sort_unique_kernel<KeyT, true> : cs_sort_unique_kernel<KeyT, false>;
+  CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   KeyT *U = T == keys ? alt : keys;
   if (nsub) {
-    cs_sort_unique_kernel<KeyT><<<(unsigned)nsub, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift,
-                                                                      rest > 0 ? bits : 0, cnt, over);
+    kern<<<(unsigned)nsub, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over);
     CF1_LAUNCH_CHECK();
   }
   uint32_t h_over = 0;
@@ -594,7 +648,7 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
 #define CF1_INST(KT)                                                                                              \
   template int msd_prefix_bits<KT>(uint64_t);                                                                     \
   template bool msd_sort_unique<KT>(KT *, KT *, uint64_t, const uint64_t *, uint32_t, int, int, KT *, uint64_t *, \
-                                    MsdScratch &, cudaStream_t);
+                                    MsdScratch &, cudaStream_t, bool);
 CF1_INST(uint64_t)
 CF1_INST(Key2)
 #undef CF1_INST

@@ -15,12 +15,14 @@ template <class KeyT>
 int msd_prefix_bits(uint64_t max_bin_keys);
 
 // keys: n keys segmented by bin (seg_off[0..nbins]); alt: n scratch keys.
-// Writes the sorted distinct keys of every bin to dist and their offsets to
-// dist_off[0..nbins].  Returns false (nothing written) when a sub-bucket is
-// larger than the shared-memory capacity; keys are then clobbered and the
-// caller re-expands and takes the LSD path.
+// Writes the distinct keys of every bin to dist and their offsets to
+// dist_off[0..nbins]: sorted within each bin, or (sorted = false) in
+// sub-bucket order with any order inside a sub-bucket.  Returns false
+// (nothing written) when a sub-bucket is larger than the shared-memory
+// capacity; keys are then clobbered and the caller re-expands and takes the
+// LSD path.
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
-                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s);
+                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted = true);
 
 }  // namespace cf1

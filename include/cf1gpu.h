@@ -153,7 +153,8 @@ int cf1gpu_copy_states(cf1gpu_ctx *ctx, uint64_t *dst, size_t n_words);
 int cf1gpu_query(cf1gpu_ctx *ctx, const uint64_t *keys, size_t n, uint64_t *slots);
 
 /* Every distinct canonical k-mer with its state (for parity checks): keys in
- * storage order (bins in order, each bin sorted), n must be total_kmers. */
+ * storage order (bins in order; each bin sorted in learned mode and with
+ * sort_mode 1, otherwise in no particular order), n must be total_kmers. */
 int cf1gpu_dump_states(cf1gpu_ctx *ctx, uint64_t *keys, uint8_t *states, size_t n);
 
 /* Verification pass: queries every distinct key on the device and checks that
