@@ -28,58 +28,65 @@ namespace {
 constexpr int BB_BLOCK = 256;
 constexpr uint32_t BB_TILE = 4096;
 
-__global__ void bb_sel_counts_kernel(const uint64_t *seg_off, const uint32_t *sel, uint32_t nbins, uint64_t *cnt) {
+// Keys of bin b at level 0: all its distinct keys when selected.
+__global__ void bb_init_counts_kernel(const uint64_t *seg_off, const uint32_t *sel, uint32_t nbins, uint64_t *cnt) {
   uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < nbins) cnt[b] = (sel == nullptr || sel[b]) ? seg_off[b + 1] - seg_off[b] : 0;
 }
 
-template <class KeyT>
-__global__ void __launch_bounds__(BB_BLOCK) bb_copy_sel_kernel(const KeyT *keys, const uint64_t *seg_off,
-                                                               const uint32_t *tile_off, uint32_t nbins,
-                                                               const uint32_t *sel, const uint64_t *new_off,
-                                                               KeyT *out) {
-  const uint32_t t = blockIdx.x;
-  if (t >= tile_off[nbins]) return;
-  TileSpan sp = tile_span(seg_off, tile_off, nbins, t, BB_TILE);
-  if (sel && !sel[sp.seg]) return;
-  uint64_t delta = new_off[sp.seg] - seg_off[sp.seg];
-  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) out[i + delta] = keys[i];
-}
+// Bits per key of a level: 4 at level 0, 2 after (gamma 2 as in ph::fmph,
+// src/mphf.rs:155-160).  The wider first level places ~78% of the keys
+// instead of ~61%, so a query -- and a warp of queries, which waits for its
+// deepest lane -- walks fewer levels, and the build marks fewer keys.
+constexpr uint32_t BB_GAMMA0 = 4, BB_GAMMA = 2;
 
-__global__ void bb_sizes_kernel(const uint64_t *rem_off, uint32_t nbins, uint64_t *wcnt) {
+// Words of each bin's block at this level (gamma bits per key, at least one
+// word for a non-empty bin) and the level's totals {keys, words}.
+__global__ void bb_sizes_kernel(const uint64_t *cnt, uint32_t nbins, uint32_t gamma, uint64_t *wcnt,
+                                unsigned long long *tot) {
   uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t n = 0, words = 0;
   if (b < nbins) {
-    uint64_t n = rem_off[b + 1] - rem_off[b];
-    uint64_t words = (2 * n + 63) / 64;
-    wcnt[b] = n ? (words ? words : 1) : 0;
+    n = cnt[b];
+    words = n ? (gamma * n + 63) / 64 : 0;
+    wcnt[b] = words;
+  }
+  n = warp_sum(n);
+  words = warp_sum(words);
+  if (lane_id() == 0 && (n | words)) {
+    atomicAdd(&tot[0], (unsigned long long)n);
+    atomicAdd(&tot[1], (unsigned long long)words);
   }
 }
 
-// AR points at this level's first entry; woff are the level-relative block
-// offsets of the bins.
+// Marks every key's bit in this level's block of its bin.  The entry's rank
+// half (y) collects the bits that more than one key set; AR points at this
+// level's first entry and woff are the level-relative block offsets.  Keys
+// of bin b are rem[start[b], start[b] + cnt[b]).
 template <class KeyT>
-__global__ void __launch_bounds__(BB_BLOCK) bb_mark_kernel(const KeyT *rem, const uint64_t *rem_off,
+__global__ void __launch_bounds__(BB_BLOCK) bb_mark_kernel(const KeyT *rem, const uint64_t *start, const uint64_t *cnt,
                                                            const uint32_t *tile_off, uint32_t nbins,
-                                                           const uint64_t *woff, uint32_t level, ulonglong2 *AR,
-                                                           uint64_t *C) {
+                                                           const uint64_t *woff, uint32_t level, ulonglong2 *AR) {
   const uint32_t t = blockIdx.x;
   if (t >= tile_off[nbins]) return;
-  TileSpan sp = tile_span(rem_off, tile_off, nbins, t, BB_TILE);
+  TileSpan sp = tile_span_gapped(start, cnt, tile_off, nbins, t, BB_TILE);
   const uint64_t w0 = woff[sp.seg];
   const uint32_t nw = (uint32_t)(woff[sp.seg + 1] - w0);
   for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) {
     uint64_t pos = bb_pos(bb_key_hash(rem[i]), level, nw);
-    uint64_t wi = w0 + (pos >> 6);
-    uint64_t bit = 1ull << (pos & 63);
-    unsigned long long old = atomicOr(&AR[wi].x, (unsigned long long)bit);
-    if (old & bit) atomicOr(reinterpret_cast<unsigned long long *>(C + wi), (unsigned long long)bit);
+    ulonglong2 *e = AR + w0 + (pos >> 6);
+    unsigned long long bit = 1ull << (pos & 63);
+    unsigned long long old = atomicOr(&e->x, bit);
+    if (old & bit) atomicOr(&e->y, bit);
   }
 }
 
-__global__ void bb_clean_kernel(ulonglong2 *AR, const uint64_t *C, uint32_t *pc, uint64_t nw) {
+// Clears the bits set by more than one key; popcount per word for the ranks.
+__global__ void bb_clean_kernel(ulonglong2 *AR, uint32_t *pc, uint64_t nw) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nw) {
-    uint64_t a = AR[i].x & ~C[i];
+    ulonglong2 e = AR[i];
+    uint64_t a = e.x & ~e.y;
     AR[i].x = a;
     pc[i] = (uint32_t)__popcll(a);
   }
@@ -103,43 +110,20 @@ __global__ void bb_meta_kernel(const uint64_t *woff, const uint64_t *R, uint64_t
   base[b] += R[w1] - R[w0];
 }
 
+// Keys whose bit did not survive go to the next level: each tile appends its
+// survivors to out[start[b] + ...] behind one atomic on the bin's next count
+// (the order of the keys inside a bin does not matter to BBHash).
 template <class KeyT>
-CF1_D bool bb_placed(const KeyT &key, uint32_t level, uint64_t w0, uint32_t nw, const ulonglong2 *AR) {
-  uint64_t pos = bb_pos(bb_key_hash(key), level, nw);
-  return (AR[w0 + (pos >> 6)].x >> (pos & 63)) & 1;
-}
-
-template <class KeyT>
-__global__ void __launch_bounds__(BB_BLOCK) bb_filter_count_kernel(const KeyT *rem, const uint64_t *rem_off,
-                                                                   const uint32_t *tile_off, uint32_t nbins,
-                                                                   const uint64_t *woff, uint32_t level,
-                                                                   const ulonglong2 *A, uint32_t *tile_cnt) {
-  __shared__ uint32_t sm[BB_BLOCK / 32];
-  const uint32_t t = blockIdx.x;
-  if (t >= tile_off[nbins]) {
-    if (threadIdx.x == 0) tile_cnt[t] = 0;
-    return;
-  }
-  TileSpan sp = tile_span(rem_off, tile_off, nbins, t, BB_TILE);
-  const uint64_t w0 = woff[sp.seg];
-  const uint32_t nw = (uint32_t)(woff[sp.seg + 1] - w0);
-  uint32_t c = 0;
-  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) c += bb_placed(rem[i], level, w0, nw, A) ? 0 : 1;
-  uint32_t tot = block_sum<BB_BLOCK>(c, sm);
-  if (threadIdx.x == 0) tile_cnt[t] = tot;
-}
-
-template <class KeyT>
-__global__ void __launch_bounds__(BB_BLOCK) bb_filter_write_kernel(const KeyT *rem, const uint64_t *rem_off,
-                                                                   const uint32_t *tile_off, uint32_t nbins,
-                                                                   const uint64_t *woff, uint32_t level,
-                                                                   const ulonglong2 *A, const uint64_t *tile_out,
-                                                                   KeyT *out) {
+__global__ void __launch_bounds__(BB_BLOCK) bb_filter_kernel(const KeyT *rem, const uint64_t *start, const uint64_t *cnt,
+                                                             const uint32_t *tile_off, uint32_t nbins,
+                                                             const uint64_t *woff, uint32_t level, const ulonglong2 *AR,
+                                                             unsigned long long *cnt_next, KeyT *out) {
   constexpr int ITEMS = BB_TILE / BB_BLOCK;
   __shared__ uint32_t sm[BB_BLOCK / 32];
+  __shared__ unsigned long long s_base;
   const uint32_t t = blockIdx.x;
   if (t >= tile_off[nbins]) return;
-  TileSpan sp = tile_span(rem_off, tile_off, nbins, t, BB_TILE);
+  TileSpan sp = tile_span_gapped(start, cnt, tile_off, nbins, t, BB_TILE);
   const uint64_t w0 = woff[sp.seg];
   const uint32_t nw = (uint32_t)(woff[sp.seg + 1] - w0);
   uint64_t i0 = sp.start + (uint64_t)threadIdx.x * ITEMS;
@@ -147,29 +131,22 @@ __global__ void __launch_bounds__(BB_BLOCK) bb_filter_write_kernel(const KeyT *r
 #pragma unroll
   for (int j = 0; j < ITEMS; j++) {
     uint64_t i = i0 + j;
-    bool keep = i < sp.end && !bb_placed(rem[i], level, w0, nw, A);
+    bool keep = false;
+    if (i < sp.end) {
+      uint64_t pos = bb_pos(bb_key_hash(rem[i]), level, nw);
+      keep = ((AR[w0 + (pos >> 6)].x >> (pos & 63)) & 1) == 0;
+    }
     flags |= (uint32_t)keep << j;
     c += keep;
   }
   uint32_t tot;
   uint32_t pre = block_exclusive_scan<BB_BLOCK>(c, sm, tot);
-  uint64_t o = tile_out[t] + pre;
+  if (threadIdx.x == 0) s_base = tot ? atomicAdd(&cnt_next[sp.seg], (unsigned long long)tot) : 0;
+  __syncthreads();
+  uint64_t o = start[sp.seg] + s_base + pre;
 #pragma unroll
   for (int j = 0; j < ITEMS; j++)
     if ((flags >> j) & 1) out[o++] = rem[i0 + j];
-}
-
-__global__ void offsets_from_tiles_kernel(const uint32_t *tile_off, uint32_t nseg, const uint64_t *tile_out,
-                                          uint64_t *out_off) {
-  uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b <= nseg) out_off[b] = tile_out[tile_off[b]];
-}
-
-uint64_t d2h_u64(const uint64_t *p, cudaStream_t s) {
-  uint64_t v = 0;
-  CF1_CUDA(cudaMemcpyAsync(&v, p, sizeof(v), cudaMemcpyDeviceToHost, s));
-  CF1_CUDA(cudaStreamSynchronize(s));
-  return v;
 }
 
 }  // namespace
@@ -204,75 +181,59 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
                               cudaStream_t s, KeyT *ws0, KeyT *ws1, uint64_t ws_cap) {
   clear();
   nbins = nb;
-  {  // local slots are 32-bit: every bin must hold fewer than 2^32 keys
-    std::vector<uint64_t> h(nbins + 1);
-    CF1_CUDA(cudaMemcpyAsync(h.data(), seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    CF1_CUDA(cudaStreamSynchronize(s));
-    for (uint32_t b = 0; b < nbins; b++)
-      if (h[b + 1] - h[b] >= (1ull << 32))
-        throw Error(CF1GPU_ERR_INVALID_ARG, "BBHash: a bin holds 2^32 or more distinct keys; use more bins");
-  }
+  std::vector<uint64_t> hoff(nbins + 1);
+  CF1_CUDA(cudaMemcpyAsync(hoff.data(), seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  for (uint32_t b = 0; b < nbins; b++)  // local slots are 32-bit
+    if (hoff[b + 1] - hoff[b] >= (1ull << 32))
+      throw Error(CF1GPU_ERR_INVALID_ARG, "BBHash: a bin holds 2^32 or more distinct keys; use more bins");
+  const uint64_t n_all = hoff[nbins];
   uint64_t *base = base_.get<uint64_t>(nbins);
   CF1_CUDA(cudaMemsetAsync(base, 0, nbins * sizeof(uint64_t), s));
   BBMeta *meta = meta_.get<BBMeta>((size_t)BB_MAX_LEVELS * nbins);
   CF1_CUDA(cudaMemsetAsync(meta, 0, (size_t)BB_MAX_LEVELS * nbins * sizeof(BBMeta), s));
-
-  uint64_t *cnt = wcnt_.get<uint64_t>(nbins + 1);
-  uint64_t *off0 = rem_off_[0].get<uint64_t>(nbins + 1);
-  uint64_t *off1 = rem_off_[1].get<uint64_t>(nbins + 1);
+  // Keys of bin b at every level sit at [seg_off[b], seg_off[b] + cnt[b]) of
+  // the level's key array: the distinct keys at level 0, then the two
+  // workspaces in turn (the caller's, when big enough).
+  uint64_t *cnt[2] = {cnt_[0].get<uint64_t>(nbins), cnt_[1].get<uint64_t>(nbins)};
+  uint64_t *wcnt = wcnt_.get<uint64_t>(nbins + 1);
+  uint64_t *woff = woff_.get<uint64_t>(nbins + 1);
   uint32_t *tile_off = tile_off_.get<uint32_t>(nbins + 1);
-  uint64_t n_all = d2h_u64(seg_off + nbins, s);
-  uint64_t n = n_all;
-  // level workspace: two key arrays of n keys (the caller's, when big enough)
+  unsigned long long *tot = reinterpret_cast<unsigned long long *>(tot_.get<uint64_t>(2));
   KeyT *r[2];
-  r[0] = (ws0 && ws_cap >= n + 1) ? ws0 : rem_[0].get<KeyT>(n + 1);
-  r[1] = (ws1 && ws_cap >= n + 1) ? ws1 : rem_[1].get<KeyT>(n + 1);
-  uint64_t *roffs[2] = {off0, off1};
+  r[0] = (ws0 && ws_cap >= n_all + 1) ? ws0 : rem_[0].get<KeyT>(n_all + 1);
+  r[1] = (ws1 && ws_cap >= n_all + 1) ? ws1 : rem_[1].get<KeyT>(n_all + 1);
+  bb_init_counts_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(seg_off, sel, nbins, cnt[0]);
+  CF1_LAUNCH_CHECK();
+  // room for the usual level sizes (gamma0 bits per key, then ~22% and
+  // fewer keys per level) so that the entry array rarely grows in mid-build
+  reserve_entries((BB_GAMMA0 * n_all / 64 + nbins) * 3 / 2 + 64 * nbins + 64, 0, s);
   const KeyT *rem = keys;
-  const uint64_t *roff = seg_off;
-  if (sel) {  // keys of the selected bins -> r[0]
-    bb_sel_counts_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(seg_off, sel, nbins, cnt);
-    CF1_LAUNCH_CHECK();
-    exclusive_scan_u64(cnt, off0, nbins, scan_tmp_, s);
-    n = d2h_u64(off0 + nbins, s);
-    if (n) {
-      uint32_t ub = (uint32_t)(ceil_div(n_all, BB_TILE) + nbins);
-      segment_tiles(seg_off, nbins, BB_TILE, tile_off, s);
-      bb_copy_sel_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(keys, seg_off, tile_off, nbins, sel, off0, r[0]);
-      CF1_LAUNCH_CHECK();
-    }
-    rem = r[0];
-    roff = off0;
-  }
-  // room for the usual level sizes (2 bits per key, then ~40% fewer keys per
-  // level) so that the entry array rarely grows in mid-build
-  reserve_entries((2 * n / 64 + nbins) * 2 + 64, 0, s);
-  int cur = 1;  // level l reads rem (keys, then r[cur^1]) and writes r[cur]
-  uint64_t remaining = n;
   uint32_t l = 0;
-  while (remaining > 0) {
-    if (l >= BB_MAX_LEVELS) throw Error(CF1GPU_ERR_BIJECTION, "BBHash: keys left after the last level");
-    KeyT *nxt = r[cur];
-    uint64_t *noff = roffs[cur];
-    uint64_t *woff = woff_.get<uint64_t>(nbins + 1);
-    bb_sizes_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(roff, nbins, cnt);
+  for (;; l++) {
+    uint64_t *cur = cnt[l & 1], *nxt_cnt = cnt[(l + 1) & 1];
+    CF1_CUDA(cudaMemsetAsync(tot, 0, 2 * sizeof(unsigned long long), s));
+    bb_sizes_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(cur, nbins, l ? BB_GAMMA : BB_GAMMA0, wcnt, tot);
     CF1_LAUNCH_CHECK();
-    exclusive_scan_u64(cnt, woff, nbins, scan_tmp_, s);
-    uint64_t nw = d2h_u64(woff + nbins, s);
+    uint64_t ht[2] = {0, 0};
+    CF1_CUDA(cudaMemcpyAsync(ht, tot, sizeof(ht), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+    const uint64_t remaining = ht[0], nw = ht[1];
+    if (remaining == 0) break;
+    if (l >= BB_MAX_LEVELS) throw Error(CF1GPU_ERR_BIJECTION, "BBHash: keys left after the last level");
+    exclusive_scan_u64(wcnt, woff, nbins, scan_tmp_, s);
     reserve_entries(total_words + nw, total_words, s);
     nwords.push_back(nw);
     level_off.push_back(total_words);
     ulonglong2 *Al = ar_.as<ulonglong2>() + total_words;
     uint64_t *Rl = rtmp_.get<uint64_t>(nw + 1);
-    uint64_t *C = C_.get<uint64_t>(nw);
     uint32_t *pc = pc_.get<uint32_t>(nw);
     CF1_CUDA(cudaMemsetAsync(Al, 0, nw * sizeof(ulonglong2), s));
-    CF1_CUDA(cudaMemsetAsync(C, 0, nw * 8, s));
     uint32_t ub = (uint32_t)(ceil_div(remaining, BB_TILE) + nbins);
-    segment_tiles(roff, nbins, BB_TILE, tile_off, s);
-    bb_mark_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, roff, tile_off, nbins, woff, l, Al, C);
+    segment_tiles_counts(cur, nbins, BB_TILE, tile_off, s);
+    bb_mark_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, seg_off, cur, tile_off, nbins, woff, l, Al);
     CF1_LAUNCH_CHECK();
-    bb_clean_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, C, pc, nw);
+    bb_clean_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, pc, nw);
     CF1_LAUNCH_CHECK();
     exclusive_scan_u32(pc, Rl, nw, scan_tmp_, s);
     bb_rank_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, Rl, nw);
@@ -280,21 +241,13 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     bb_meta_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(woff, Rl, total_words, base, meta + (size_t)l * nbins,
                                                                   nbins);
     CF1_LAUNCH_CHECK();
-    uint32_t *tc = tile_cnt_.get<uint32_t>(ub + 1);
-    uint64_t *to = tile_out_.get<uint64_t>(ub + 2);
-    bb_filter_count_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, roff, tile_off, nbins, woff, l, Al, tc);
-    CF1_LAUNCH_CHECK();
-    exclusive_scan_u32(tc, to, ub, scan_tmp_, s);
-    bb_filter_write_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, roff, tile_off, nbins, woff, l, Al, to, nxt);
-    CF1_LAUNCH_CHECK();
-    offsets_from_tiles_kernel<<<(unsigned)ceil_div(nbins + 1, 256), 256, 0, s>>>(tile_off, nbins, to, noff);
+    KeyT *out = r[l & 1];
+    CF1_CUDA(cudaMemsetAsync(nxt_cnt, 0, nbins * sizeof(uint64_t), s));
+    bb_filter_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, seg_off, cur, tile_off, nbins, woff, l, Al,
+                                                   reinterpret_cast<unsigned long long *>(nxt_cnt), out);
     CF1_LAUNCH_CHECK();
     total_words += nw;
-    remaining = d2h_u64(noff + nbins, s);
-    rem = nxt;
-    roff = noff;
-    cur ^= 1;
-    l++;
+    rem = out;
   }
   levels = l;
   bytes = total_words * sizeof(ulonglong2) + (size_t)levels * nbins * sizeof(BBMeta);

@@ -35,8 +35,7 @@ struct BBHashBuild {
 
   // The entry array and the level buffers are kept across builds and grown on
   // demand, so a rebuild allocates nothing once sizes settle.
-  DevBuf ar_, meta_, base_, rem_[2], rem_off_[2], tile_off_, tile_cnt_, tile_out_, C_, wcnt_, woff_, pc_, rtmp_,
-      scan_tmp_;
+  DevBuf ar_, meta_, base_, rem_[2], cnt_[2], tot_, tile_off_, wcnt_, woff_, pc_, rtmp_, scan_tmp_;
 };
 
 }  // namespace cf1

@@ -125,5 +125,17 @@ CF1_D TileSpan tile_span(const uint64_t *seg_off, const uint32_t *tile_off, uint
   s.end = e < seg_off[s.seg + 1] ? e : seg_off[s.seg + 1];
   return s;
 }
+// Tile t over gapped segments: segment b holds cnt[b] items from start[b].
+CF1_D TileSpan tile_span_gapped(const uint64_t *start, const uint64_t *cnt, const uint32_t *tile_off, uint32_t nseg,
+                                uint32_t t, uint32_t tile) {
+  TileSpan s;
+  s.seg = upper_segment(tile_off, nseg, t);
+  s.first_tile = tile_off[s.seg];
+  s.ntiles = tile_off[s.seg + 1] - s.first_tile;
+  s.start = start[s.seg] + (uint64_t)(t - s.first_tile) * tile;
+  uint64_t e = s.start + tile, stop = start[s.seg] + cnt[s.seg];
+  s.end = e < stop ? e : stop;
+  return s;
+}
 
 }  // namespace cf1

@@ -95,6 +95,8 @@ void exclusive_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, DevBuf &s
 // crosses a segment edge.  tile_off[0..nseg] (u32) gets the first tile of each
 // segment; tile_off[nseg] is the tile count.
 void segment_tiles(const uint64_t *seg_off, uint32_t nseg, uint32_t tile, uint32_t *tile_off, cudaStream_t s);
+// The same over gapped segments given by item counts cnt[0..nseg).
+void segment_tiles_counts(const uint64_t *cnt, uint32_t nseg, uint32_t tile, uint32_t *tile_off, cudaStream_t s);
 
 // ------------------------------------------------------------ phase kernels ----
 void launch_pack(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, cudaStream_t s);

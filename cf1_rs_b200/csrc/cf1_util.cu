@@ -82,14 +82,17 @@ size_t scan_scratch_bytes(uint64_t n) {
   return bytes;
 }
 
-__global__ void segment_tiles_kernel(const uint64_t *seg_off, uint32_t nseg, uint32_t tile, uint32_t *tile_off) {
+// seg_off: offsets (segment b has seg_off[b+1] - seg_off[b] items) or, when
+// counts is set, the item counts themselves.
+__global__ void segment_tiles_kernel(const uint64_t *seg_off, uint32_t nseg, uint32_t tile, bool counts,
+                                     uint32_t *tile_off) {
   constexpr int B = 1024;
   __shared__ uint32_t sm[B / 32];
   uint32_t carry = 0;
   for (uint32_t base = 0; base < nseg; base += B) {
     uint32_t b = base + threadIdx.x;
     uint32_t c = 0;
-    if (b < nseg) c = (uint32_t)((seg_off[b + 1] - seg_off[b] + tile - 1) / tile);
+    if (b < nseg) c = (uint32_t)(((counts ? seg_off[b] : seg_off[b + 1] - seg_off[b]) + tile - 1) / tile);
     uint32_t tot;
     uint32_t pre = block_exclusive_scan<B>(c, sm, tot);
     if (b < nseg) tile_off[b] = carry + pre;
@@ -110,7 +113,12 @@ void exclusive_scan_u64(const uint64_t *in, uint64_t *out, uint64_t n, DevBuf &s
 }
 
 void segment_tiles(const uint64_t *seg_off, uint32_t nseg, uint32_t tile, uint32_t *tile_off, cudaStream_t s) {
-  segment_tiles_kernel<<<1, 1024, 0, s>>>(seg_off, nseg, tile, tile_off);
+  segment_tiles_kernel<<<1, 1024, 0, s>>>(seg_off, nseg, tile, false, tile_off);
+  CF1_LAUNCH_CHECK();
+}
+
+void segment_tiles_counts(const uint64_t *cnt, uint32_t nseg, uint32_t tile, uint32_t *tile_off, cudaStream_t s) {
+  segment_tiles_kernel<<<1, 1024, 0, s>>>(cnt, nseg, tile, true, tile_off);
   CF1_LAUNCH_CHECK();
 }
 
