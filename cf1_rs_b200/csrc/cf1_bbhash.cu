@@ -34,11 +34,13 @@ __global__ void bb_init_counts_kernel(const uint64_t *seg_off, const uint32_t *s
   if (b < nbins) cnt[b] = (sel == nullptr || sel[b]) ? seg_off[b + 1] - seg_off[b] : 0;
 }
 
-// Bits per key of a level: 4 at level 0, 2 after (gamma 2 as in ph::fmph,
-// src/mphf.rs:155-160).  The wider first level places ~78% of the keys
+// Bits per key of a level: 8 at level 0, 2 after (gamma 2 as in ph::fmph,
+// src/mphf.rs:155-160).  The wide first level places ~88% of the keys
 // instead of ~61%, so a query -- and a warp of queries, which waits for its
-// deepest lane -- walks fewer levels, and the build marks fewer keys.
-constexpr uint32_t BB_GAMMA0 = 4, BB_GAMMA = 2;
+// deepest lane -- walks fewer levels, and the build marks fewer keys.  At
+// 2.5e9 keys it costs ~5.7 GB of HBM; 4 bits ran phases 1-4 3% slower, 16
+// bits 1% slower (its first level's passes outweigh the shorter probes).
+constexpr uint32_t BB_GAMMA0 = 8, BB_GAMMA = 2;
 
 // Words of each bin's block at this level (gamma bits per key, at least one
 // word for a non-empty bin) and the level's totals {keys, words}.
@@ -205,7 +207,7 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
   r[1] = (ws1 && ws_cap >= n_all + 1) ? ws1 : rem_[1].get<KeyT>(n_all + 1);
   bb_init_counts_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(seg_off, sel, nbins, cnt[0]);
   CF1_LAUNCH_CHECK();
-  // room for the usual level sizes (gamma0 bits per key, then ~22% and
+  // room for the usual level sizes (gamma0 bits per key, then ~12% and
   // fewer keys per level) so that the entry array rarely grows in mid-build
   reserve_entries((BB_GAMMA0 * n_all / 64 + nbins) * 3 / 2 + 64 * nbins + 64, 0, s);
   const KeyT *rem = keys;

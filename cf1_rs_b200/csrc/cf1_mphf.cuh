@@ -2,7 +2,7 @@
 //
 // The key set is split into bins (phase 2); bin b owns slots
 // [dist_off[b], dist_off[b+1]).  Inside a bin a key's local slot comes from
-//   * BBHash (per bin): levels of bit arrays 4x (first level) then 2x the
+//   * BBHash (per bin): levels of bit arrays 8x (first level) then 2x the
 //     keys still unplaced (gamma 2 is ph::fmph's relative_level_size 200,
 //     src/mphf.rs:155-160); the first level where the key's bit is set gives
 //     the level rank; or
