@@ -90,7 +90,7 @@ struct KOps<uint64_t> {
     rcv = (rcv >> 2) | ((uint64_t)(3 - base) << (2 * k - 2));
   }
   static CF1_HD uint32_t digit(uint64_t x, int shift, uint32_t dmask) { return (uint32_t)(x >> shift) & dmask; }
-  // Bits [shift, shift+64) clipped to the key (for MSD bucketing).
+  // 64-bit mix of key ^ seed (the fmix64 finalizer of MurmurHash3).
   static CF1_HD uint64_t hash(uint64_t x, uint64_t seed) {
     x ^= seed;
     x ^= x >> 33; x *= 0xff51afd7ed558ccdull;
