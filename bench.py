@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import re
 import os
 import statistics
 import subprocess
@@ -74,11 +75,19 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def committed_traffic():
-    """dram bytes per classify launch from the committed ncu summary, if any."""
+TRAFFIC_MD = os.path.join(ROOT, "profiles", "classify_traffic_workload5_full.md")
+
+
+def committed_traffic(workload: int, scale: float, form: str):
+    """DRAM bytes (read + write) of one classify launch, from the committed
+    ncu summary of the full 3.1 Gbp workload's BBHash form; None for any
+    other workload, scale or form."""
+    if workload != 5 or scale != 1.0 or form != "bbhash":
+        return None
     try:
-        with open(os.path.join(ROOT, "profiles", "classify_traffic.json")) as f:
-            return json.load(f)
+        with open(TRAFFIC_MD) as f:
+            m = re.search(r"^traffic_bytes_per_launch = (\d+)$", f.read(), re.M)
+        return int(m.group(1)) if m else None
     except OSError:
         return None
 
@@ -313,10 +322,9 @@ def gpu_arm(args):
     # and one written per occurrence (state word RMW); MPHF probes excluded
     b4 = 0.25 * L + 64.0 * n_occ
     ach = b4 / (head["ms_classify_kernel"] / 1e3) / 1e9
-    traffic = committed_traffic()
     roofline = {"kernel": "classify_kernel", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "peak_kind": peak_kind,
-                "traffic": traffic.get("dram_bytes_per_launch_scaled") if traffic else None,
+                "traffic": committed_traffic(args.workload, args.scale, head_name),
                 "algorithmic_bytes": b4}
     # whole phases 1-4: input read once, records written + read, keys
     # written + read by the sort, distinct keys written and read by the MPHF

@@ -18,11 +18,12 @@ namespace cf1 {
 
 constexpr uint64_t SLOT_NONE = ~0ull;
 
-// BBHash hashing: one 64-bit hash H of the key; level l takes the top bits
-// of H * BB_MUL[l] (odd, independent per level), scaled to the block size.
-// Two keys that collide at one level differ in H, and the product's top bits
-// spread that difference afresh at every level, so their next collision is
-// as unlikely as a fresh one.
+// BBHash hashing (multiply-shift, Dietzfelbinger et al. 1997): a 64-bit key
+// H -- the k-mer itself for k <= 32, a mix of both words above -- and per
+// level l the top 32 bits of H * BB_MUL[l] (odd, independent per level),
+// scaled to the block size.  Two keys that collide at one level differ in H,
+// and the next level's multiplier spreads that difference afresh, so their
+// next collision is as unlikely as a fresh one.
 constexpr uint64_t BB_SEED = 0xD1B54A32D192ED03ull;
 constexpr uint32_t BB_MAX_LEVELS = 64;
 #define CF1_BB_MUL_TABLE                                                                       \
@@ -45,17 +46,19 @@ constexpr uint32_t BB_MAX_LEVELS = 64;
 static __constant__ uint64_t c_bb_mul[BB_MAX_LEVELS] = CF1_BB_MUL_TABLE;
 static const uint64_t h_bb_mul[BB_MAX_LEVELS] = CF1_BB_MUL_TABLE;
 
-template <class KeyT>
-CF1_HD uint64_t bb_key_hash(const KeyT &key) { return KOps<KeyT>::hash(key, BB_SEED); }
+CF1_HD uint64_t bb_key_hash(uint64_t key) { return key; }
+CF1_HD uint64_t bb_key_hash(const Key2 &key) { return KOps<Key2>::hash(key, BB_SEED); }
 
-// Bit of a key (hash H) in a block of nwords words at level l.
+// Bit of a key (hash H) in a block of nwords words at level l: a 32-bit hash
+// scaled to [0, 64 nwords).
 CF1_HD uint64_t bb_pos(uint64_t H, uint32_t l, uint32_t nwords) {
 #ifdef __CUDA_ARCH__
   const uint64_t mul = c_bb_mul[l];
 #else
   const uint64_t mul = h_bb_mul[l];
 #endif
-  return mulhi64(H * mul, (uint64_t)nwords << 6);
+  const uint32_t t = (uint32_t)((H * mul) >> 32);
+  return ((uint64_t)t * nwords) >> 26;
 }
 
 template <class KeyT>
