@@ -42,7 +42,7 @@ class Opts(C.Structure):
         ("batched", C.c_uint32), ("track_short_seqs", C.c_uint32), ("tuner_cache_path", C.c_char_p),
         ("learned_max_err", C.c_uint32), ("learned_train_steps", C.c_int32), ("learned_leaf_size", C.c_uint32),
         ("sk_tile", C.c_uint32), ("sort_mode", C.c_uint32), ("state_update", C.c_uint32),
-        ("reserved", C.c_uint32 * 2),
+        ("shard_index", C.c_uint32), ("shard_count", C.c_uint32),
     ]
 
 
@@ -69,7 +69,7 @@ f32p = C.POINTER(C.c_float)
 EXPORTED = [
     "cf1gpu_default_opts", "cf1gpu_create", "cf1gpu_add_record", "cf1gpu_add_records", "cf1gpu_add_fasta",
     "cf1gpu_reset_input", "cf1gpu_upload", "cf1gpu_run_resident", "cf1gpu_run_phases_1_4", "cf1gpu_get_stats",
-    "cf1gpu_total_kmers", "cf1gpu_copy_states", "cf1gpu_query", "cf1gpu_dump_states", "cf1gpu_verify_bijection",
+    "cf1gpu_total_kmers", "cf1gpu_bin_distinct_counts", "cf1gpu_copy_states", "cf1gpu_query", "cf1gpu_dump_states", "cf1gpu_verify_bijection",
     "cf1gpu_short_seq_count", "cf1gpu_short_seq", "cf1gpu_export_mphf", "cf1gpu_mphf_host_query",
     "cf1gpu_learned_stats", "cf1gpu_learned_grad", "cf1gpu_last_error", "cf1gpu_destroy", "cf1gpu_version",
     "cf1gpu_distinct_kmers_noalloc",
@@ -98,6 +98,7 @@ def lib():
     L.cf1gpu_get_stats.argtypes = [vp, C.POINTER(Stats)]
     L.cf1gpu_total_kmers.argtypes = [vp]
     L.cf1gpu_total_kmers.restype = C.c_uint64
+    L.cf1gpu_bin_distinct_counts.argtypes = [vp, u64p, C.c_size_t]
     L.cf1gpu_copy_states.argtypes = [vp, u64p, C.c_size_t]
     L.cf1gpu_query.argtypes = [vp, u64p, C.c_size_t, u64p]
     L.cf1gpu_dump_states.argtypes = [vp, u64p, u8p, C.c_size_t]
@@ -162,7 +163,8 @@ class Cf1Gpu:
     def __init__(self, k: int = 31, num_bins: int = 128, device: int = 0, mode: str = "bbhash",
                  batched: bool = False, track_short_seqs: bool = False, learned_max_err: int = 0,
                  learned_train_steps: int = 0, learned_leaf_size: int = 0, sk_tile: int = 0,
-                 sort_mode: str = "msd", state_update: str = "sideset"):
+                 sort_mode: str = "msd", state_update: str = "sideset", shard_index: int = 0,
+                 shard_count: int = 1):
         L = lib()
         o = Opts()
         L.cf1gpu_default_opts(C.byref(o))
@@ -176,12 +178,14 @@ class Cf1Gpu:
         o.sk_tile = sk_tile
         o.sort_mode = {"msd": 0, "lsd": 1}[sort_mode]
         o.state_update = {"sideset": 0, "cas": 1}[state_update]
+        o.shard_index, o.shard_count = shard_index, shard_count
         h = C.c_void_p()
         st = L.cf1gpu_create(C.byref(o), C.byref(h))
         if st != OK:
             raise Cf1Error(st, L.cf1gpu_last_error(None).decode())
         self.h = h
         self.k = k
+        self.num_bins = num_bins
         self.kw = 1 if k <= 32 else 2
 
     def _check(self, st):
@@ -247,6 +251,12 @@ class Cf1Gpu:
 
     def total_kmers(self) -> int:
         return int(lib().cf1gpu_total_kmers(self.h))
+
+    def bin_distinct_counts(self) -> np.ndarray:
+        """Distinct k-mers of every bin (0 for the bins of other shards)."""
+        out = np.empty(self.num_bins, np.uint64)
+        self._check(lib().cf1gpu_bin_distinct_counts(self.h, _p(out, u64p), self.num_bins))
+        return out
 
     def states(self, out: np.ndarray | None = None) -> np.ndarray:
         nw = (self.total_kmers() + 11) // 12

@@ -75,6 +75,11 @@ int cf1gpu_create(const cf1gpu_opts *opts, cf1gpu_ctx **out) {
     g_create_error = "state_update must be 0 (side sets) or 1 (CAS)";
     return CF1GPU_ERR_INVALID_ARG;
   }
+  if (opts->shard_count > cf1::MAX_BINS || (opts->shard_count > 1 && opts->shard_index >= opts->shard_count) ||
+      (opts->shard_count <= 1 && opts->shard_index != 0)) {
+    g_create_error = "shard_index must be below shard_count (at most 4096 shards)";
+    return CF1GPU_ERR_INVALID_ARG;
+  }
   cf1gpu_ctx *c = new (std::nothrow) cf1gpu_ctx();
   if (!c) return CF1GPU_ERR_OOM;
   int st = guard(nullptr, [&] {
@@ -129,6 +134,8 @@ int cf1gpu_add_fasta(cf1gpu_ctx *c, const char *path) {
 int cf1gpu_reset_input(cf1gpu_ctx *c) {
   if (!c) return CF1GPU_ERR_INVALID_ARG;
   c->L = 0;
+  c->dev_valid = 0;
+  c->ms_intake = 0;
   c->n_records = 0;
   c->n_bases = 0;
   c->short_seqs.clear();
@@ -162,6 +169,26 @@ int cf1gpu_get_stats(const cf1gpu_ctx *c, cf1gpu_stats *out) {
 }
 
 uint64_t cf1gpu_total_kmers(const cf1gpu_ctx *c) { return (c && c->ran) ? c->n_distinct : 0; }
+
+int cf1gpu_bin_distinct_counts(const cf1gpu_ctx *c, uint64_t *counts, size_t nbins) {
+  if (!c || (nbins && !counts)) return CF1GPU_ERR_INVALID_ARG;
+  cf1gpu_ctx *m = const_cast<cf1gpu_ctx *>(c);
+  if (!c->ran) {
+    m->last_error = "no results: run phases 1-4 first";
+    return CF1GPU_ERR_STATE;
+  }
+  if (nbins != c->opts.num_bins) {
+    m->last_error = "nbins must be num_bins = " + std::to_string(c->opts.num_bins);
+    return CF1GPU_ERR_INVALID_ARG;
+  }
+  return guard(m, [&] {
+    std::vector<uint64_t> off(nbins + 1);
+    CF1_CUDA(cudaMemcpyAsync(off.data(), c->d_dist_off.p, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CF1_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t b = 0; b < nbins; b++) counts[b] = off[b + 1] - off[b];
+  });
+}
 
 int cf1gpu_copy_states(cf1gpu_ctx *c, uint64_t *dst, size_t n_words) {
   if (!c || (!dst && n_words)) return CF1GPU_ERR_INVALID_ARG;

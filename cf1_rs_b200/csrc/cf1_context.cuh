@@ -60,10 +60,15 @@ struct cf1gpu_ctx {
   uint64_t n_bases = 0;
   std::vector<std::pair<std::string, uint64_t>> short_seqs;
   bool uploaded = false;
+  // Leading bytes of the concatenation already on the device: records given
+  // in page-locked host memory are copied there directly (no staging), the
+  // rest wait in `host` for cf1gpu_upload.
+  uint64_t dev_valid = 0;
+  double ms_intake = 0;  // device time of those direct copies since the last upload
   bool ran = false;
 
   // device buffers
-  cf1::DevBuf d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
+  cf1::DevBuf d_raw, d_intake, d_shard, d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
       d_keys, d_dist, d_dist_off, d_states, d_scan, d_seen, d_qin, d_qout, d_queue;
   uint64_t rec_cap_hint = 0;  // phase-1 record list size of the last run
   cf1::Backend<uint64_t> b64;

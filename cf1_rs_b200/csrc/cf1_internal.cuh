@@ -62,6 +62,22 @@ struct DevBuf {
   T *as() const { return static_cast<T *>(p); }
   template <class T>
   T *get(size_t n) { return static_cast<T *>(reserve(n * sizeof(T))); }
+  // Grows to at least `bytes` (by a quarter more), keeping the first `keep`
+  // bytes; synchronises the stream when it moves them.
+  void *reserve_keep(size_t bytes, size_t keep, cudaStream_t s) {
+    if (bytes <= cap && p) return p;
+    size_t b = bytes + bytes / 4 + 16;
+    void *np = nullptr;
+    CF1_CUDA(cudaMalloc(&np, b));
+    if (keep && p) {
+      CF1_CUDA(cudaMemcpyAsync(np, p, keep, cudaMemcpyDeviceToDevice, s));
+      CF1_CUDA(cudaStreamSynchronize(s));
+    }
+    release();
+    p = np;
+    cap = b;
+    return p;
+  }
 };
 
 inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }

@@ -46,6 +46,24 @@ __global__ void seg_gather_kernel(const uint64_t *kpre, const uint64_t *rec_off,
   if (b <= nbins) seg[b] = kpre[rec_off[b]];
 }
 
+// Bin sharding: records of the bins this shard keeps (b % shards == idx).
+__global__ void shard_counts_kernel(const uint64_t *rec_off, uint32_t nbins, uint32_t idx, uint32_t shards,
+                                    uint64_t *cnt) {
+  uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nbins) cnt[b] = b % shards == idx ? rec_off[b + 1] - rec_off[b] : 0;
+}
+
+constexpr uint32_t SH_TILE = 4096;
+__global__ void shard_copy_kernel(const uint64_t *in, const uint64_t *rec_off, const uint32_t *tile_off, uint32_t nbins,
+                                  uint32_t idx, uint32_t shards, const uint64_t *new_off, uint64_t *out) {
+  const uint32_t t = blockIdx.x;
+  if (t >= tile_off[nbins]) return;
+  TileSpan sp = tile_span(rec_off, tile_off, nbins, t, SH_TILE);
+  if (sp.seg % shards != idx) return;
+  const uint64_t delta = new_off[sp.seg] - rec_off[sp.seg];
+  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += blockDim.x) out[i + delta] = in[i];
+}
+
 template <class KeyT>
 Backend<KeyT> &backend(cf1gpu_ctx *c) {
   return ctx_backend<KeyT>(c);
@@ -145,14 +163,39 @@ void run_impl(cf1gpu_ctx *c) {
   CF1_CUDA(cudaEventRecord(c->ev[1], s));
 
   // ---- phase 2: route super k-mers into bins
-  const uint64_t NS = c->n_super;
+  uint64_t NS = c->n_super;
   uint64_t *records = c->d_records.get<uint64_t>(NS + 1);
   CF1_CUDA(cudaMemsetAsync(records, 0, (NS + 1) * sizeof(uint64_t), s));
   uint32_t *cursor = c->d_cursor.get<uint32_t>(B);
   CF1_CUDA(cudaMemsetAsync(cursor, 0, B * sizeof(uint32_t), s));
   launch_bin_scatter(a.rec_tmp, a.rec_bucket, NS, lut, B, rec_off, cursor, records, &sm->err, s);
+  const uint32_t shards = c->opts.shard_count > 1 ? c->opts.shard_count : 1;
+  if (shards > 1) {
+    // Keep this shard's bins: their records, moved to the front through the
+    // free key buffer (the phase-1 list in it has been routed); the other
+    // bins keep empty ranges, so they get no keys, slots or states.
+    uint64_t *cnt = c->d_shard.get<uint64_t>(3 * (size_t)(B + 1));
+    uint64_t *new_off = cnt + (B + 1);
+    uint32_t *tile_off = reinterpret_cast<uint32_t *>(new_off + (B + 1));
+    shard_counts_kernel<<<(unsigned)ceil_div(B, 256), 256, 0, s>>>(rec_off, B, c->opts.shard_index, shards, cnt);
+    CF1_LAUNCH_CHECK();
+    exclusive_scan_u64(cnt, new_off, B, c->d_scan, s);
+    segment_tiles(rec_off, B, SH_TILE, tile_off, s);
+    uint64_t *tmp = static_cast<uint64_t *>(c->d_keys.reserve((NS + 1) * sizeof(uint64_t)));
+    shard_copy_kernel<<<(unsigned)(ceil_div(NS, SH_TILE) + B), 256, 0, s>>>(records, rec_off, tile_off, B,
+                                                                            c->opts.shard_index, shards, new_off, tmp);
+    CF1_LAUNCH_CHECK();
+    CF1_CUDA(cudaMemcpyAsync(&NS, new_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+    if (NS) CF1_CUDA(cudaMemcpyAsync(records, tmp, NS * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    CF1_CUDA(cudaMemcpyAsync(rec_off, new_off, (B + 1) * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+  }
   uint64_t *kpre = c->d_kpre.get<uint64_t>(NS + 1);
   record_kmer_prefix(records, NS, kpre, c->d_lens, c->d_scan, s);
+  if (shards > 1) {  // the k-mer windows of this shard's records
+    CF1_CUDA(cudaMemcpyAsync(&c->n_occ, kpre + NS, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+  }
   CF1_CUDA(cudaEventRecord(c->ev[2], s));
 
   // ---- phase 3a: expand, sort per bin, unique
@@ -299,6 +342,61 @@ void query_impl(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots) 
   CF1_CUDA(cudaStreamSynchronize(s));
 }
 
+// Direct intake of records given in page-locked host memory: one DMA of the
+// caller's bytes into a device buffer, then tiles of it are moved to their
+// places in the concatenation, a placeholder after each record.
+struct IntakeTile {
+  uint64_t src, dst;
+  uint32_t len, last;  // last: the tile ends its record
+};
+constexpr uint32_t INTAKE_TILE = 1u << 16;
+
+__global__ void intake_kernel(const uint8_t *raw, const IntakeTile *tiles, uint8_t *out) {
+  const IntakeTile t = tiles[blockIdx.x];
+  for (uint32_t i = threadIdx.x; i < t.len; i += blockDim.x) out[t.dst + i] = raw[t.src + i];
+  if (t.last && threadIdx.x == 0) out[t.dst + t.len] = 'N';
+}
+
+bool page_locked(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();  // not a pointer CUDA knows: pageable
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// dst[i]: the record's place in the concatenation (~0 for records below k
+// bases); end: the concatenation's length after the records.
+void intake_direct(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, size_t n, const std::vector<uint64_t> &dst,
+                   uint64_t end) {
+  cudaStream_t s = c->stream;
+  const uint64_t first = off[0], raw = off[n] - first;
+  c->d_ascii.reserve_keep(end + 16, c->dev_valid, s);
+  std::vector<IntakeTile> tiles;
+  for (size_t i = 0; i < n; i++) {
+    if (dst[i] == ~0ull) continue;
+    const uint64_t len = off[i + 1] - off[i];
+    for (uint64_t t = 0; t < len; t += INTAKE_TILE) {
+      const uint64_t m = std::min<uint64_t>(INTAKE_TILE, len - t);
+      tiles.push_back(IntakeTile{off[i] - first + t, dst[i] + t, (uint32_t)m, t + m == len ? 1u : 0u});
+    }
+  }
+  if (!tiles.empty()) {
+    uint8_t *r = c->d_raw.get<uint8_t>(raw + 1);
+    IntakeTile *dt = c->d_intake.get<IntakeTile>(tiles.size());
+    CF1_CUDA(cudaEventRecord(c->ev[10], s));
+    CF1_CUDA(cudaMemcpyAsync(r, seqs + first, raw, cudaMemcpyHostToDevice, s));
+    CF1_CUDA(cudaEventRecord(c->ev[11], s));
+    CF1_CUDA(cudaMemcpyAsync(dt, tiles.data(), tiles.size() * sizeof(IntakeTile), cudaMemcpyHostToDevice, s));
+    intake_kernel<<<(unsigned)tiles.size(), 256, 0, s>>>(r, dt, c->d_ascii.as<uint8_t>());
+    CF1_LAUNCH_CHECK();
+    CF1_CUDA(cudaStreamSynchronize(s));  // the caller may free its buffer on return
+    c->ms_intake += elapsed(c->ev[10], c->ev[11]);
+  }
+  c->L = c->dev_valid = end;
+}
+
 void append_record(cf1gpu_ctx *c, const uint8_t *seq, size_t len) {
   c->host.reserve(c->L + len + 1, c->L);
   if (len) std::memcpy(c->host.p + c->L, seq, len);
@@ -326,14 +424,17 @@ void run_resident(cf1gpu_ctx *c) {
 
 void upload(cf1gpu_ctx *c) {
   cudaStream_t s = c->stream;
-  uint8_t *d = c->d_ascii.get<uint8_t>(c->L + 16);
+  uint8_t *d = static_cast<uint8_t *>(c->d_ascii.reserve_keep(c->L + 16, c->dev_valid, s));
   CF1_CUDA(cudaEventRecord(c->ev[8], s));
-  if (c->L) CF1_CUDA(cudaMemcpyAsync(d, c->host.p, c->L, cudaMemcpyHostToDevice, s));
+  if (c->L > c->dev_valid)
+    CF1_CUDA(cudaMemcpyAsync(d + c->dev_valid, c->host.p + c->dev_valid, c->L - c->dev_valid, cudaMemcpyHostToDevice, s));
   CF1_CUDA(cudaEventRecord(c->ev[9], s));
   CF1_CUDA(cudaEventSynchronize(c->ev[9]));
   float ms = 0;
   CF1_CUDA(cudaEventElapsedTime(&ms, c->ev[8], c->ev[9]));
-  c->stats.ms_h2d = ms;
+  c->stats.ms_h2d = ms + c->ms_intake;
+  c->ms_intake = 0;
+  c->dev_valid = c->L;
   c->uploaded = true;
 }
 
@@ -350,7 +451,8 @@ void add_record(cf1gpu_ctx *c, const char *name, size_t name_len, const uint8_t 
 
 void add_records(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, size_t n) {
   // Records of k bases or more are copied into the pinned buffer by several
-  // threads; shorter ones only update the short-sequence list.
+  // threads (or, when the caller's buffer is page-locked, DMA'd to the
+  // device); shorter ones only update the short-sequence list.
   std::vector<uint64_t> dst(n + 1);
   uint64_t pos = c->L;
   for (size_t i = 0; i < n; i++) {
@@ -364,6 +466,12 @@ void add_records(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, size_t
       continue;
     }
     pos += len + 1;
+  }
+  // page-locked records go straight to the device while nothing is staged
+  if (n && c->dev_valid == c->L && page_locked(seqs + off[0])) {
+    intake_direct(c, seqs, off, n, dst, pos);
+    c->uploaded = false;
+    return;
   }
   c->host.reserve(pos + 1, c->L);
   uint8_t *h = c->host.p;

@@ -78,7 +78,11 @@ typedef struct cf1gpu_opts {
   uint32_t state_update;      /* phase-4 state update: 0 = side-set bytes joined by atomic OR, then packed;
                                  1 = atomicCAS loop on the packed words (src/state_vector.rs:47-70).
                                  Both give the same words. */
-  uint32_t reserved[2];
+  uint32_t shard_index;       /* bin sharding over shard_count devices: this context keeps the bins b with
+                                 b % shard_count == shard_index for phases 3-4 (phases 1-2 still route the
+                                 whole input, so every shard sees the same partition); slots, states and
+                                 total_kmers are then those of its own bins */
+  uint32_t shard_count;       /* 0 or 1 = no sharding */
 } cf1gpu_opts;
 
 typedef struct cf1gpu_stats {
@@ -143,6 +147,13 @@ int cf1gpu_get_stats(const cf1gpu_ctx *ctx, cf1gpu_stats *out);
 
 /* Mphf::total_kmers (src/mphf.rs:278-280). */
 uint64_t cf1gpu_total_kmers(const cf1gpu_ctx *ctx);
+
+/* Distinct k-mers of every bin (counts[b], b < nbins = num_bins; 0 for the
+ * bins of other shards): bin b owns the slots from the sum of the counts
+ * before it.  Across shards these give the global slot offsets -- the one
+ * exchange bin sharding needs (no counterpart in the reference, which runs
+ * on one host). */
+int cf1gpu_bin_distinct_counts(const cf1gpu_ctx *ctx, uint64_t *counts, size_t nbins);
 
 /* The state vector words (src/state_vector.rs:7-71 layout); n_words must be
  * ceil(total_kmers / 12). */

@@ -69,6 +69,39 @@ def test_state_update_modes(k, mode):
     assert np.array_equal(words["sideset"], words["cas"])
 
 
+def _pinned_copy(a):
+    import torch
+
+    t = torch.empty(max(1, a.nbytes), dtype=torch.uint8, pin_memory=True)
+    v = t.numpy()[: a.nbytes].view(a.dtype)
+    v[:] = a
+    return t, v
+
+
+@pytest.mark.parametrize("k", [21, 33])
+def test_page_locked_intake(k):
+    # records in page-locked memory are DMA'd to the device directly; mixed
+    # with staged (pageable) calls the result equals one staged run
+    recs = random_records(4242 + k, k, n_records=90, max_len=9000)
+    seq, off = o.concat_records(recs)
+    ref, _ = assert_parity(seq, off, k, num_bins=8)
+    want = ref.states()
+    ref.close()
+    a, b = len(recs) // 3, 2 * len(recs) // 3
+    parts = [o.concat_records(recs[:a]), o.concat_records(recs[a:b]), o.concat_records(recs[b:])]
+    for pinned in ([True, False, True], [True, True, True], [False, True, True]):
+        g = cg.Cf1Gpu(k=k, num_bins=8)
+        keep = []
+        for (ps, po), pin in zip(parts, pinned):
+            if pin:
+                t, ps = _pinned_copy(ps)
+                keep.append(t)
+            g.add_records(ps, po)
+        g.run()
+        assert np.array_equal(g.states(), want)
+        g.close()
+
+
 @pytest.mark.parametrize("k", [31, 63])
 def test_oversized_subbucket(k):
     # a long homopolymer and a tandem repeat put tens of thousands of copies of
