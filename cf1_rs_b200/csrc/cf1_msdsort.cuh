@@ -12,7 +12,7 @@ struct MsdScratch {
 // Top bits to split on so that the largest bin's sub-buckets hold about a
 // third of the shared-memory capacity.
 template <class KeyT>
-int msd_prefix_bits(uint64_t max_bin_keys);
+int msd_prefix_bits(uint64_t max_bin_keys, bool sorted);
 
 // keys: n keys segmented by bin (seg_off[0..nbins]); alt: n scratch keys.
 // Writes the distinct keys of every bin to dist and their offsets to

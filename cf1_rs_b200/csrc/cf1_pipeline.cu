@@ -213,9 +213,10 @@ void run_impl(cf1gpu_ctx *c) {
   uint64_t max_bin = 0;
   for (uint32_t b = 0; b < B; b++) max_bin = std::max(max_bin, hseg[b + 1] - hseg[b]);
   KeyT *alt = be.sort.alt.template get<KeyT>(NO + 1);
-  int P = c->force_lsd ? -1 : msd_prefix_bits<KeyT>(max_bin);
-  // The learned index needs each bin's keys sorted; BBHash needs them distinct.
-  const bool sorted = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED || c->opts.sort_mode == 1;
+  // The learned index needs each bin's keys sorted; BBHash needs them
+  // distinct (128-bit keys always take the sorted path).
+  const bool sorted = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED || c->opts.sort_mode == 1 || KOps<KeyT>::WORDS == 2;
+  int P = c->force_lsd ? -1 : msd_prefix_bits<KeyT>(max_bin, sorted);
   bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist, dist_off, be.msd, s, sorted);
   c->msd_bits = done ? P : -1;
   if (!done) {  // a sub-bucket overflowed shared memory: expand again, LSD path
