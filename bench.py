@@ -35,6 +35,7 @@ import re
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import threading
 import time
@@ -67,6 +68,8 @@ def parse():
     p.add_argument("--cpu-sample-mbp", type=float, default=40.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--tuner-cache", default=os.path.join(tempfile.gettempdir(), "cf1_tuner_cache.txt"),
+                   help="autotuner cache file (first warm-up run of an input class measures; '' = off)")
     return p.parse_args()
 
 
@@ -260,13 +263,16 @@ def gpu_arm(args):
     # strong scaling: every rank routes the same genome and keeps the bins
     # b with b % world == rank (bin sharding, cf1_rs_b200.sharded)
     x = cg.SynthInput(args.workload, scale=args.scale, seed=0)
+    # one cache file per rank (ranks run the same classes; no shared writes)
+    tuner_path = (args.tuner_cache + (f".rank{rank}" if world > 1 else "")) if args.tuner_cache else None
     forms = {}
     clocks = Clocks(local)
     clock_info = None
     for form in args.forms.split(","):
         batched = form == "learned"
         g = cg.Cf1Gpu(k=k, num_bins=bins, device=local, mode=form, batched=batched,
-                      track_short_seqs=bool(wl.get("short")), shard_index=rank, shard_count=world)
+                      track_short_seqs=bool(wl.get("short")), shard_index=rank, shard_count=world,
+                      tuner_cache=tuner_path)
         g.add_records(x.seq, x.offsets)
         g.upload()
         for _ in range(args.warmup):
@@ -310,7 +316,8 @@ def gpu_arm(args):
         g = head["ctx"]
         if g is None:
             g = cg.Cf1Gpu(k=k, num_bins=bins, device=local, mode=head_name, batched=head_name == "learned",
-                          track_short_seqs=bool(wl.get("short")), shard_index=rank, shard_count=world)
+                          track_short_seqs=bool(wl.get("short")), shard_index=rank, shard_count=world,
+                          tuner_cache=tuner_path)
         # inputs and the result in page-locked host memory: the records go to
         # the device in one DMA, the state words come back in one
         pin_seq = torch.empty(max(1, x.seq.nbytes), dtype=torch.uint8, pin_memory=True)
@@ -389,6 +396,8 @@ def gpu_arm(args):
                       "sort": ("lsd" if v["stats"]["sort_msd_bits"] == 2**64 - 1
                                else f"msd{v['stats']['sort_msd_bits']}"),
                       "learned_bins": int(v["stats"]["learned_bins"]), "fallback_bins": int(v["stats"]["fallback_bins"]),
+                      "sk_tile": int(v["stats"]["sk_tile"]),
+                      "tuner": ["off", "cache", "measured"][int(v["stats"]["tuner_state"])],
                       "learned": v["learned"]} for f, v in forms.items()},
     }
     print(json.dumps(line), flush=True)

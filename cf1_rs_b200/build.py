@@ -33,6 +33,7 @@ SOURCES = [
     "cf1_fasta.cu",
     "cf1_capi.cu",
     "cf1_noalloc.cu",
+    "cf1_tuner.cu",
 ]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []
 

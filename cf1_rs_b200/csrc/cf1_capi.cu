@@ -85,6 +85,7 @@ int cf1gpu_create(const cf1gpu_opts *opts, cf1gpu_ctx **out) {
   int st = guard(nullptr, [&] {
     c->opts = *opts;
     c->opts.tuner_cache_path = nullptr;
+    if (opts->tuner_cache_path) c->tuner_path = opts->tuner_cache_path;
     c->k = (int)opts->k;
     c->m = minimizer_len(c->k);
     c->w = c->k - c->m + 1;

@@ -9,6 +9,7 @@
 #include "cf1_internal.cuh"
 #include "cf1_learned.cuh"
 #include "cf1_msdsort.cuh"
+#include "cf1_tuner.cuh"
 
 namespace cf1 {
 
@@ -38,6 +39,7 @@ struct Tuning {
   uint32_t sk_tile = 2048;      // k-mer positions per minimizer tile (1024/2048/4096)
   int persistent_ctas = 0;      // 0: derived from the SM count in batched mode
   uint32_t leaf_size = 32;      // learned index keys per leaf
+  int msd_delta = 0;            // added to the phase-3 MSD split width
 };
 
 }  // namespace cf1
@@ -71,6 +73,11 @@ struct cf1gpu_ctx {
   cf1::DevBuf d_raw, d_intake, d_shard, d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
       d_keys, d_dist, d_dist_off, d_states, d_scan, d_seen, d_qin, d_qout, d_queue;
   uint64_t rec_cap_hint = 0;  // phase-1 record list size of the last run
+  // autotuner: cache file ("" = off), the key the current tuning is for
+  std::string tuner_path;
+  cf1::TuneKey tuned_key;
+  bool tune_valid = false;
+  int tuner_state = 0;  // last run: 0 off, 1 from the cache, 2 measured
   cf1::Backend<uint64_t> b64;
   cf1::Backend<cf1::Key2> b128;
 

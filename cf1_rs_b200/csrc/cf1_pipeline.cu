@@ -105,6 +105,36 @@ void run_impl(cf1gpu_ctx *c) {
   const bool batched = c->opts.batched != 0;
   c->nbins = B;
   const uint64_t launches0 = g_launches.load();
+  // The learned index needs each bin's keys sorted; BBHash needs them
+  // distinct (128-bit keys always take the sorted path).
+  const bool sorted = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED || c->opts.sort_mode == 1 || KOps<KeyT>::WORDS == 2;
+  // autotuner: parameters of this input class from the cache, or measured
+  // in this run and stored
+  bool tune_now = false;
+  TuneValue tuned;
+  tuned.sk_tile = c->tune.sk_tile;
+  c->tuner_state = 0;
+  if (!c->tuner_path.empty()) {
+    TuneKey key;
+    key.wide = c->wide;
+    key.sorted = sorted;
+    key.batched = batched;
+    for (uint64_t x = L; x > 1; x >>= 1) key.size_class++;
+    TuneValue v;
+    if (c->tune_valid && c->tuned_key == key) {
+      c->tuner_state = 1;
+    } else if (tuner_lookup(c->tuner_path, key, v)) {
+      if (c->opts.sk_tile == 0) c->tune.sk_tile = v.sk_tile;
+      c->tune.msd_delta = v.msd_delta;
+      c->tuned_key = key;
+      c->tune_valid = true;
+      c->tuner_state = 1;
+    } else {
+      c->tuned_key = key;
+      c->tune_valid = false;
+      tune_now = true;
+    }
+  }
   Small *sm = c->d_small.get<Small>(1);
   CF1_CUDA(cudaMemsetAsync(sm, 0, sizeof(Small), s));
   CF1_CUDA(cudaEventRecord(c->ev[0], s));
@@ -124,8 +154,6 @@ void run_impl(cf1gpu_ctx *c) {
   a.k = k;
   a.m = c->m;
   a.w = c->w;
-  a.tile = c->tune.sk_tile;
-  a.n_tiles = L >= (uint64_t)k ? ceil_div(L - k + 1, a.tile) : 0;
   a.hist = hist;
   a.n_kmers = &sm->n_kmers;
   a.rec_count = &sm->rec_count;
@@ -141,23 +169,45 @@ void run_impl(cf1gpu_ctx *c) {
   // The list lives in the key buffer, which phase 3 only fills after phase 2
   // has routed the list.
   Small hs;
-  for (int attempt = 0;; attempt++) {
-    a.rec_cap = std::max<uint64_t>(c->rec_cap_hint, L / 4 + 1024);
-    uint8_t *rbuf = static_cast<uint8_t *>(c->d_keys.reserve(a.rec_cap * (sizeof(uint64_t) + sizeof(uint16_t))));
-    a.rec_tmp = reinterpret_cast<uint64_t *>(rbuf);
-    a.rec_bucket = reinterpret_cast<uint16_t *>(rbuf + a.rec_cap * sizeof(uint64_t));
-    CF1_CUDA(cudaMemsetAsync(hist, 0, NUM_BUCKETS * sizeof(uint32_t), s));
-    CF1_CUDA(cudaMemsetAsync(sm, 0, sizeof(Small), s));
-    launch_superkmer_scan(a, pctas, s);
-    launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
-    CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
-    CF1_CUDA(cudaMemcpyAsync(&c->n_super, rec_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-    CF1_CUDA(cudaStreamSynchronize(s));
-    if (hs.rec_count != c->n_super) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record count != histogram total");
-    if (hs.rec_count <= a.rec_cap) break;
-    if (attempt) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record list overflowed twice");
-    c->rec_cap_hint = hs.rec_count;
+  auto phase1 = [&](uint32_t tile) {
+    a.tile = tile;
+    a.n_tiles = L >= (uint64_t)k ? ceil_div(L - k + 1, a.tile) : 0;
+    for (int attempt = 0;; attempt++) {
+      a.rec_cap = std::max<uint64_t>(c->rec_cap_hint, L / 4 + 1024);
+      uint8_t *rbuf = static_cast<uint8_t *>(c->d_keys.reserve(a.rec_cap * (sizeof(uint64_t) + sizeof(uint16_t))));
+      a.rec_tmp = reinterpret_cast<uint64_t *>(rbuf);
+      a.rec_bucket = reinterpret_cast<uint16_t *>(rbuf + a.rec_cap * sizeof(uint64_t));
+      CF1_CUDA(cudaMemsetAsync(hist, 0, NUM_BUCKETS * sizeof(uint32_t), s));
+      CF1_CUDA(cudaMemsetAsync(sm, 0, sizeof(Small), s));
+      launch_superkmer_scan(a, pctas, s);
+      launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
+      CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
+      CF1_CUDA(cudaMemcpyAsync(&c->n_super, rec_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+      CF1_CUDA(cudaStreamSynchronize(s));
+      if (hs.rec_count != c->n_super)
+        throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record count != histogram total");
+      if (hs.rec_count <= a.rec_cap) break;
+      if (attempt) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record list overflowed twice");
+      c->rec_cap_hint = hs.rec_count;
+    }
+  };
+  if (tune_now && c->opts.sk_tile == 0) {  // autotuner: time each tile, keep the fastest
+    double best = 1e30;
+    for (uint32_t t : TUNE_TILES) {
+      CF1_CUDA(cudaEventRecord(c->ev[10], s));
+      phase1(t);
+      CF1_CUDA(cudaEventRecord(c->ev[11], s));
+      CF1_CUDA(cudaEventSynchronize(c->ev[11]));
+      const double ms = elapsed(c->ev[10], c->ev[11]);
+      if (ms < best) {
+        best = ms;
+        tuned.sk_tile = t;
+        tuned.p1_ms = ms;
+      }
+    }
+    c->tune.sk_tile = tuned.sk_tile;
   }
+  phase1(c->tune.sk_tile);
   c->n_occ = hs.n_kmers;
   c->n_bins_eff = hs.n_bins_eff;
   CF1_CUDA(cudaEventRecord(c->ev[1], s));
@@ -213,15 +263,50 @@ void run_impl(cf1gpu_ctx *c) {
   uint64_t max_bin = 0;
   for (uint32_t b = 0; b < B; b++) max_bin = std::max(max_bin, hseg[b + 1] - hseg[b]);
   KeyT *alt = be.sort.alt.template get<KeyT>(NO + 1);
-  // The learned index needs each bin's keys sorted; BBHash needs them
-  // distinct (128-bit keys always take the sorted path).
-  const bool sorted = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED || c->opts.sort_mode == 1 || KOps<KeyT>::WORDS == 2;
-  int P = c->force_lsd ? -1 : msd_prefix_bits<KeyT>(max_bin, sorted);
+  const int P0 = c->force_lsd ? -1 : msd_prefix_bits<KeyT>(max_bin, sorted);
+  auto msd_width = [&](int delta) { return P0 < 0 ? -1 : std::min(16, std::max(0, P0 + delta)); };
+  auto expand_again = [&]() {
+    launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[4] : nullptr, &sm->err, pctas, s);
+  };
+  if (tune_now && P0 >= 0) {  // autotuner: time each MSD width, keep the fastest
+    double best = 1e30;
+    int tried = -2;
+    for (int d : TUNE_MSD_DELTAS) {
+      const int P = msd_width(d);
+      if (P == tried) continue;
+      if (tried != -2) expand_again();  // the previous try consumed the keys
+      if (batched) CF1_CUDA(cudaMemsetAsync(&sm->queues[4], 0, sizeof(uint32_t), s));
+      CF1_CUDA(cudaEventRecord(c->ev[10], s));
+      const bool ok = msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist, dist_off, be.msd, s, sorted);
+      CF1_CUDA(cudaEventRecord(c->ev[11], s));
+      CF1_CUDA(cudaEventSynchronize(c->ev[11]));
+      const double ms = elapsed(c->ev[10], c->ev[11]);
+      if (ok && ms < best) {
+        best = ms;
+        tuned.msd_delta = d;
+        tuned.p3_ms = ms;
+      }
+      tried = P;
+    }
+    c->tune.msd_delta = tuned.msd_delta;
+    expand_again();
+    if (batched) CF1_CUDA(cudaMemsetAsync(&sm->queues[4], 0, sizeof(uint32_t), s));
+  }
+  int P = msd_width(c->tune.msd_delta);
   bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist, dist_off, be.msd, s, sorted);
   c->msd_bits = done ? P : -1;
+  if (tune_now) {
+    tuned.sk_tile = c->tune.sk_tile;
+    tuned.msd_delta = c->tune.msd_delta;
+    tuner_store(c->tuner_path, c->tuned_key, tuned);
+    c->tune_valid = true;
+    c->tuner_state = 2;
+  }
   if (!done) {  // a sub-bucket overflowed shared memory: expand again, LSD path
-    if (P >= 0)
-      launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[4] : nullptr, &sm->err, pctas, s);
+    if (P >= 0) {
+      if (batched) CF1_CUDA(cudaMemsetAsync(&sm->queues[5], 0, sizeof(uint32_t), s));
+      launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[5] : nullptr, &sm->err, pctas, s);
+    }
     segmented_sort<KeyT>(keys, NO, seg, B, 2 * k, be.sort, s);
     segmented_unique<KeyT>(keys, NO, seg, B, dist, dist_off, be.sort, s);
   }
@@ -296,6 +381,8 @@ void run_impl(cf1gpu_ctx *c) {
   st.classify_cas_retries = c->cas_retries;
   st.n_kernel_launches = g_launches.load() - launches0;
   st.sort_msd_bits = c->msd_bits >= 0 ? (uint64_t)c->msd_bits : ~0ull;
+  st.tuner_state = (uint64_t)c->tuner_state;
+  st.sk_tile = c->tune.sk_tile;
   st.ms_phase1 = elapsed(c->ev[0], c->ev[1]);
   st.ms_phase2 = elapsed(c->ev[1], c->ev[2]);
   st.ms_phase3_sort = elapsed(c->ev[2], c->ev[3]);

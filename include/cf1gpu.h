@@ -68,7 +68,11 @@ typedef struct cf1gpu_opts {
   uint32_t batched;           /* 1: persistent work-queue kernels (one full-occupancy wave per phase kernel
                                  pulling fixed-size chunks from an atomic queue) */
   uint32_t track_short_seqs;  /* --track-short-seqs (src/params.rs:45-47) */
-  const char *tuner_cache_path; /* autotuner cache file, NULL = built-in defaults */
+  const char *tuner_cache_path; /* autotuner cache file, NULL = built-in defaults.  With a path, the first run
+                                 of each (k <= 32 or not, sorted bins or not, batched or not, log2 input
+                                 bases) measures the phase-1 tile (1024/2048/4096, unless sk_tile is set)
+                                 and the phase-3 MSD split width (-1..+2 bits), keeps the fastest and
+                                 writes them to the file; later runs and contexts read them back */
   uint32_t learned_max_err;   /* learned index: per-bin error bound above which the bin falls back to BBHash (0 = default 1024) */
   int32_t learned_train_steps; /* learned index root training steps: 0 = default (300), < 0 = no training (identity root) */
   uint32_t learned_leaf_size; /* learned index target keys per leaf (0 = default 32) */
@@ -102,7 +106,9 @@ typedef struct cf1gpu_stats {
   uint64_t classify_cas_retries; /* failed CAS attempts in phase 4 */
   uint64_t n_kernel_launches;  /* kernels this library launched during the last run */
   uint64_t sort_msd_bits;      /* top bits the MSD sort split bins on; UINT64_MAX when the LSD path ran */
-  uint64_t reserved_u[4];
+  uint64_t tuner_state;        /* 0 no autotuner, 1 parameters from the cache, 2 measured in this run */
+  uint64_t sk_tile;            /* phase-1 tile this run used */
+  uint64_t reserved_u[2];
   double ms_h2d;               /* host->device copy of the input */
   double ms_phase1;            /* pack + minimizer histogram + partition */
   double ms_phase2;            /* super k-mer routing */

@@ -182,6 +182,33 @@ def test_short_seqs_and_fasta():
         g.close()
 
 
+@pytest.mark.parametrize("mode,batched", [("bbhash", False), ("learned", True)])
+def test_autotuner_cache(mode, batched):
+    # the first run of an input class measures the tile and the MSD width and
+    # writes them to the cache; a second context reads them back; results
+    # stay bit-exact either way
+    recs = random_records(808, 31, n_records=120, max_len=9000)
+    seq, off = o.concat_records(recs)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "tune.txt")
+        with open(path, "w") as f:
+            f.write("not a tuner line\ncf1tune 1 wide=0 sorted=0 size=3\n")  # ignored
+        g, _ = assert_parity(seq, off, 31, mode=mode, batched=batched, num_bins=16, tuner_cache=path)
+        s1 = g.stats()
+        assert s1["tuner_state"] == 2 and s1["sk_tile"] in (1024, 2048, 4096)
+        g.upload()
+        g.run_resident()
+        assert g.stats()["tuner_state"] == 1
+        g.close()
+        lines = [l for l in open(path).read().splitlines() if l.startswith("cf1tune 1 ")]
+        assert len(lines) == 1 and f"sk_tile={s1['sk_tile']}" in lines[0]
+        g2, _ = assert_parity(seq, off, 31, mode=mode, batched=batched, num_bins=16, tuner_cache=path)
+        s2 = g2.stats()
+        assert s2["tuner_state"] == 1 and s2["sk_tile"] == s1["sk_tile"]
+        assert s2["sort_msd_bits"] == s1["sort_msd_bits"]
+        g2.close()
+
+
 def test_deterministic_repeat_runs():
     recs = random_records(3, 31, n_records=100, max_len=8000)
     seq, off = o.concat_records(recs)
