@@ -180,6 +180,15 @@ CF1_HD uint32_t mix_order(uint32_t x) {
   x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
   return x;
 }
+// Inverse of mix_order (the multipliers' inverses mod 2^32; x ^= x >> 15 is
+// undone by x ^= (x >> 15) ^ (x >> 30)).  mix_order is a bijection, so the
+// order key (mix_order(c) << 32) | c ranks m-mers exactly as mix_order(c)
+// alone, and c = mix_order_inv(mix_order(c)).  No canonical m-mer (c < 2^30)
+// has mix_order(c) = 0xFFFFFFFF (its preimage is 0xD5F9EFC4).
+CF1_HD uint32_t mix_order_inv(uint32_t x) {
+  x ^= x >> 16; x *= 0x43021123u; x ^= (x >> 15) ^ (x >> 30); x *= 0x1d69e2a5u; x ^= x >> 16;
+  return x;
+}
 CF1_HD uint32_t mix_bucket(uint32_t x) {
   x ^= 0x5bd1e995u;
   x ^= x >> 16; x *= 0x21f0aaadu; x ^= x >> 15; x *= 0x735a2d97u; x ^= x >> 15;

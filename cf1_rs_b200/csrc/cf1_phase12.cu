@@ -69,21 +69,27 @@ __global__ void pack_kernel(const uint8_t *ascii, uint64_t L, uint64_t *W, uint6
 // One CTA per tile of T = BLOCK*ITEMS k-mer start positions (or, in persistent
 // mode, tiles pulled from an atomic counter).  The tile's bases span
 // T + k - 1 positions, so consecutive tiles overlap by k-1 bases.
-//   1. order keys of the T + w - 1 m-mers into shared memory;
-//   2. sliding-window minimum over w by log2(w) doubling passes;
-//   3. a k-mer is valid when its window holds no placeholder; a super k-mer
-//      starts at a valid k-mer whose predecessor in the tile is invalid or has
-//      another minimizer, and runs while the minimizer stays the same;
-//   4. each super k-mer counts once in the histogram of its minimizer bucket
-//      (phase 1) and is written once, with its bucket, to an unordered record
-//      list that phase 2 routes by bin (a tile reserves its slots with one
-//      atomic add).
+//   1. the 32-bit order values mix_order(c) of the T + w - 1 canonical m-mers
+//      into shared memory (mix_order is a bijection, so they rank m-mers as
+//      the spec's 64-bit order keys do);
+//   2. sliding-window minimum over w by log2(w) doubling passes; a window
+//      that holds a placeholder gets the value 0xFFFFFFFF, which no m-mer has;
+//   3. each thread takes ITEMS consecutive k-mers: a segment starts where the
+//      window minimum changes; one block scan numbers the segments, their
+//      starts go to shared memory, and a segment's length is the distance to
+//      the next start -- no thread walks a run;
+//   4. each valid segment is a super k-mer: it counts once in the histogram of
+//      its minimizer bucket (phase 1) and is written once, with its bucket, to
+//      an unordered record list that phase 2 routes by bin (a tile reserves
+//      its slots with one atomic add).
+constexpr uint32_t SK_INVALID = 0xFFFFFFFFu;
+
 template <int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
   constexpr uint32_t T = BLOCK * ITEMS;
-  extern __shared__ uint64_t dyn[];
-  uint64_t *bufA = dyn;
-  uint64_t *bufB = dyn + T + 64;
+  extern __shared__ uint32_t dyn32[];
+  uint32_t *bufA = dyn32;
+  uint32_t *bufB = dyn32 + T + 64;
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_base;
   __shared__ uint32_t sm[BLOCK / 32];
@@ -104,63 +110,73 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
     const uint32_t nm = nk + w - 1;
     for (uint32_t q = tid; q < nm; q += BLOCK) {
       uint32_t fw = (uint32_t)KOps<uint64_t>::extract(a.W, P0 + q, m);
-      bufA[q] = mmer_order(fw, m);
+      uint32_t r = mmer_rc(fw, m);
+      bufA[q] = mix_order(fw < r ? fw : r);
     }
     __syncthreads();
-    uint64_t *src = bufA, *dst = bufB;
+    uint32_t *src = bufA, *dst = bufB;
     uint32_t len = nm, span = 1;
     while (span * 2 <= (uint32_t)w) {
-      for (uint32_t q = tid; q + span < len; q += BLOCK) {
-        uint64_t x = src[q], y = src[q + span];
-        dst[q] = x < y ? x : y;
-      }
+      for (uint32_t q = tid; q + span < len; q += BLOCK) dst[q] = min(src[q], src[q + span]);
       __syncthreads();
-      uint64_t *t2 = src; src = dst; dst = t2;
+      uint32_t *t2 = src;
+      src = dst;
+      dst = t2;
       len -= span;
       span *= 2;
     }
     for (uint32_t p = tid; p < nk; p += BLOCK) {
-      uint64_t x = src[p], y = src[p + w - span];
-      uint64_t v = x < y ? x : y;
-      if (!window_clean(a.NM, P0 + p, k)) v = ~0ull;
-      dst[p] = v;
+      uint32_t v = min(src[p], src[p + w - span]);
+      dst[p] = window_clean(a.NM, P0 + p, k) ? v : SK_INVALID;
     }
     __syncthreads();
-    const uint64_t *z = dst;
-    uint32_t rn[ITEMS], rbk[ITEMS];
-    uint32_t mine = 0;
+    const uint32_t *z = dst;
+    uint32_t *starts = src;  // free now: segment starts
+    // thread tid owns k-mers [p0, p0 + ITEMS)
+    const uint32_t p0 = tid * ITEMS;
+    uint32_t zv[ITEMS];
+    uint32_t bflags = 0, nb = 0, nv = 0;
+    uint32_t prev = p0 > 0 && p0 <= nk ? z[p0 - 1] : SK_INVALID;
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
-      uint32_t p = i * BLOCK + tid;
-      rn[i] = 0;
-      rbk[i] = 0;
-      if (p < nk) {
-        uint64_t v = z[p];
-        if (v != ~0ull && (p == 0 || z[p - 1] != v)) {
-          uint32_t e = p + 1;
-          while (e < nk && z[e] == v) e++;
-          rn[i] = e - p;
-          rbk[i] = mix_bucket((uint32_t)v);
-          atomicAdd(&a.hist[rbk[i]], 1u);
-          my_kmers += rn[i];
-          mine++;
-        }
-      }
+      const uint32_t p = p0 + i;
+      zv[i] = p < nk ? z[p] : SK_INVALID;
+      const bool b = p < nk && (p == 0 || zv[i] != prev);
+      bflags |= (uint32_t)b << i;
+      nb += b;
+      nv += b && zv[i] != SK_INVALID;
+      prev = zv[i];
     }
+    // one scan numbers both the segments (high half) and the valid ones (low)
     uint32_t tot;
-    uint32_t pre = block_exclusive_scan<BLOCK>(mine, sm, tot);
-    if (tid == 0) s_base = atomicAdd(a.rec_count, (unsigned long long)tot);
+    const uint32_t pre = block_exclusive_scan<BLOCK>((nb << 16) | nv, sm, tot);
+    const uint32_t nseg = tot >> 16, nrec = tot & 0xFFFFu;
+    uint32_t seg = pre >> 16;
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++)
+      if ((bflags >> i) & 1) starts[seg++] = p0 + i;
+    if (tid == 0) {
+      starts[nseg] = nk;
+      s_base = nrec ? atomicAdd(a.rec_count, (unsigned long long)nrec) : 0;
+    }
     __syncthreads();
-    uint64_t o = s_base + pre;
+    uint64_t o = s_base + (pre & 0xFFFFu);
+    seg = pre >> 16;
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
-      if (rn[i]) {
-        if (o < a.rec_cap) {
-          a.rec_tmp[o] = rec_pack(P0 + i * BLOCK + tid, rn[i], 0);
-          a.rec_bucket[o] = (uint16_t)rbk[i];
-        }
-        o++;
+      if (!((bflags >> i) & 1)) continue;
+      const uint32_t e = starts[seg + 1];
+      seg++;
+      if (zv[i] == SK_INVALID) continue;
+      const uint32_t n = e - (p0 + i);
+      const uint32_t bk = mix_bucket(mix_order_inv(zv[i]));
+      atomicAdd(&a.hist[bk], 1u);
+      my_kmers += n;
+      if (o < a.rec_cap) {
+        a.rec_tmp[o] = rec_pack(P0 + p0 + i, n, 0);
+        a.rec_bucket[o] = (uint16_t)bk;
       }
+      o++;
     }
     __syncthreads();
     if (!a.tile_counter) break;
@@ -216,7 +232,7 @@ __global__ void __launch_bounds__(BS_BLOCK) bin_scatter_kernel(const uint64_t *r
 
 void launch_sk(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
   if (a.n_tiles == 0) return;
-  size_t smem = 2 * (a.tile + 64) * sizeof(uint64_t);
+  size_t smem = 2 * (a.tile + 64) * sizeof(uint32_t);
   switch (a.tile) {
 #define CF1_SK_CASE(IT)                                                                              \
   case SK_BLOCK * IT: {                                                                            \
