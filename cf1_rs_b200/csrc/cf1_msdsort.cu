@@ -73,12 +73,13 @@ __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, con
     H[(uint64_t)sp.first_tile * DIG + (uint64_t)d * sp.ntiles + (t - sp.first_tile)] = h[d];
 }
 
-// Stable multisplit of one tile: warp w ranks the w-th 512-key slice of the
-// tile round by round (match_any inside a round, a running per-warp digit
-// count across rounds), a per-digit prefix over warps gives tile-local
-// positions, the tile is staged in shared memory in digit order, and each
-// digit's run is written out with consecutive threads on consecutive
-// addresses.
+// Multisplit of one tile: warp w ranks the keys of the w-th 512-key slice of
+// the tile by a shared-memory atomic add on its per-warp digit count (the
+// order inside a digit does not matter: every sub-bucket is sorted or
+// deduplicated whole afterwards), a per-digit prefix over warps gives
+// tile-local positions, the tile is staged in shared memory in digit order,
+// and each digit's run is written out with consecutive threads on
+// consecutive addresses.
 template <class KeyT, int BITS>
 __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
                                                                  const uint32_t *tile_off, uint32_t nseg, int shift,
@@ -103,22 +104,15 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
   // for lanes past the tile; keys are read again when staged, which keeps
   // the register count (and so the occupancy) down
   uint32_t pk[MS_ITEMS];
-  const unsigned lt = lanemask_lt();
   uint32_t *wh = whist + warp * DIG;
 #pragma unroll
   for (int r = 0; r < MS_ITEMS; r++) {
     uint32_t li = warp * (MS_ITEMS * 32) + r * 32 + lane;
-    bool act = li < n;
-    uint32_t d = act ? ms_digit(in[sp.start + li], shift, DIG - 1, hashed) : 0xFFFFFFFFu;
-    unsigned peers = __match_any_sync(FULL, d);
-    unsigned leader = __ffs(peers) - 1;
-    uint32_t old = 0;
-    if (act && lane == leader) {
-      old = wh[d];
-      wh[d] = old + __popc(peers);
+    pk[r] = 0xFFFFFFFFu;
+    if (li < n) {
+      uint32_t d = ms_digit(in[sp.start + li], shift, DIG - 1, hashed);
+      pk[r] = (atomicAdd(&wh[d], 1u) << 8) | d;
     }
-    old = __shfl_sync(FULL, old, leader);
-    pk[r] = act ? ((old + __popc(peers & lt)) << 8) | d : 0xFFFFFFFFu;
   }
   __syncthreads();
   // per digit: exclusive prefix over warps; tile total per digit
