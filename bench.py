@@ -68,6 +68,7 @@ def parse():
     p.add_argument("--cpu-sample-mbp", type=float, default=40.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--leaf-size", type=int, default=0, help="learned index keys per leaf (0 = library default)")
     p.add_argument("--tuner-cache", default=os.path.join(tempfile.gettempdir(), "cf1_tuner_cache.txt"),
                    help="autotuner cache file (first warm-up run of an input class measures; '' = off)")
     return p.parse_args()
@@ -272,7 +273,7 @@ def gpu_arm(args):
         batched = form == "learned"
         g = cg.Cf1Gpu(k=k, num_bins=bins, device=local, mode=form, batched=batched,
                       track_short_seqs=bool(wl.get("short")), shard_index=rank, shard_count=world,
-                      tuner_cache=tuner_path)
+                      tuner_cache=tuner_path, learned_leaf_size=args.leaf_size)
         g.add_records(x.seq, x.offsets)
         g.upload()
         for _ in range(args.warmup):
@@ -317,7 +318,7 @@ def gpu_arm(args):
         if g is None:
             g = cg.Cf1Gpu(k=k, num_bins=bins, device=local, mode=head_name, batched=head_name == "learned",
                           track_short_seqs=bool(wl.get("short")), shard_index=rank, shard_count=world,
-                          tuner_cache=tuner_path)
+                          tuner_cache=tuner_path, learned_leaf_size=args.leaf_size)
         # inputs and the result in page-locked host memory: the records go to
         # the device in one DMA, the state words come back in one
         pin_seq = torch.empty(max(1, x.seq.nbytes), dtype=torch.uint8, pin_memory=True)
