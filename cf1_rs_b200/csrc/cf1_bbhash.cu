@@ -65,15 +65,57 @@ __global__ void bb_sizes_kernel(const uint64_t *cnt, uint32_t nbins, uint32_t ga
 // half (y) collects the bits that more than one key set; AR points at this
 // level's first entry and woff are the level-relative block offsets.  Keys
 // of bin b are rem[start[b], start[b] + cnt[b]).
+//
+// When a tile's keys fall in a narrow stretch of the block -- at level 0 the
+// unsorted phase-3 output is ordered by the same hash's top bits -- the tile
+// marks a shared-memory copy of that stretch and merges it with one atomicOr
+// per word (and one more per word with a collision) instead of one per key.
+constexpr uint32_t BB_WIN = 2048;  // words of the shared-memory stretch
 template <class KeyT>
 __global__ void __launch_bounds__(BB_BLOCK) bb_mark_kernel(const KeyT *rem, const uint64_t *start, const uint64_t *cnt,
                                                            const uint32_t *tile_off, uint32_t nbins,
                                                            const uint64_t *woff, uint32_t level, ulonglong2 *AR) {
+  __shared__ unsigned long long s_set[BB_WIN], s_col[BB_WIN];
+  __shared__ unsigned long long s_lo, s_hi;
   const uint32_t t = blockIdx.x;
   if (t >= tile_off[nbins]) return;
   TileSpan sp = tile_span_gapped(start, cnt, tile_off, nbins, t, BB_TILE);
   const uint64_t w0 = woff[sp.seg];
   const uint32_t nw = (uint32_t)(woff[sp.seg + 1] - w0);
+  if (threadIdx.x == 0) {
+    s_lo = ~0ull;
+    s_hi = 0;
+  }
+  __syncthreads();
+  unsigned long long lo = ~0ull, hi = 0;
+  for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) {
+    const unsigned long long wi = bb_pos(bb_key_hash(rem[i]), level, nw) >> 6;
+    lo = wi < lo ? wi : lo;
+    hi = wi > hi ? wi : hi;
+  }
+  atomicMin(&s_lo, lo);
+  atomicMax(&s_hi, hi);
+  __syncthreads();
+  const uint64_t wlo = s_lo, span = s_hi >= s_lo ? s_hi - s_lo + 1 : 0;
+  if (span > 0 && span <= BB_WIN) {
+    for (uint32_t j = threadIdx.x; j < span; j += BB_BLOCK) s_set[j] = s_col[j] = 0;
+    __syncthreads();
+    for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) {
+      const uint64_t pos = bb_pos(bb_key_hash(rem[i]), level, nw);
+      const uint32_t j = (uint32_t)((pos >> 6) - wlo);
+      const unsigned long long bit = 1ull << (pos & 63);
+      if (atomicOr(&s_set[j], bit) & bit) atomicOr(&s_col[j], bit);
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < span; j += BB_BLOCK) {
+      const unsigned long long set = s_set[j];
+      if (!set) continue;
+      ulonglong2 *e = AR + w0 + wlo + j;
+      const unsigned long long col = s_col[j] | (atomicOr(&e->x, set) & set);
+      if (col) atomicOr(&e->y, col);
+    }
+    return;
+  }
   for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += BB_BLOCK) {
     uint64_t pos = bb_pos(bb_key_hash(rem[i]), level, nw);
     ulonglong2 *e = AR + w0 + (pos >> 6);

@@ -180,6 +180,12 @@ CF1_HD uint32_t mix_order(uint32_t x) {
   x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
   return x;
 }
+// Odd multiplier whose product's top bits spread 64-bit keys evenly.  The
+// unsorted phase-3 split (sub-bucket = top bits of key * KEY_SPREAD_MUL) and
+// BBHash level 0 (bit = top bits of key * KEY_SPREAD_MUL, scaled) use the same
+// one, so the keys of one sub-bucket land in one stretch of level 0's bits.
+constexpr uint64_t KEY_SPREAD_MUL = 0xD6E8FEB86659FD93ull;
+
 // Inverse of mix_order (the multipliers' inverses mod 2^32; x ^= x >> 15 is
 // undone by x ^= (x >> 15) ^ (x >> 30)).  mix_order is a bijection, so the
 // order key (mix_order(c) << 32) | c ranks m-mers exactly as mix_order(c)

@@ -20,14 +20,14 @@ constexpr uint64_t SLOT_NONE = ~0ull;
 
 // BBHash hashing (multiply-shift, Dietzfelbinger et al. 1997): a 64-bit key
 // H -- the k-mer itself for k <= 32, a mix of both words above -- and per
-// level l the top 32 bits of H * BB_MUL[l] (odd, independent per level),
-// scaled to the block size.  Two keys that collide at one level differ in H,
+// level l the top 32 bits of H * BB_MUL[l] (odd, independent per level;
+// level 0's is KEY_SPREAD_MUL), scaled to the block size.  Two keys that collide at one level differ in H,
 // and the next level's multiplier spreads that difference afresh, so their
 // next collision is as unlikely as a fresh one.
 constexpr uint64_t BB_SEED = 0xD1B54A32D192ED03ull;
 constexpr uint32_t BB_MAX_LEVELS = 64;
 #define CF1_BB_MUL_TABLE                                                                       \
-  {0x9444bd23aedfa6f5ull, 0x358e91a8e48b97dbull, 0x970f24b9078ea7c7ull, 0x8f4bacefadb4bcb1ull, \
+  {0xd6e8feb86659fd93ull, 0x358e91a8e48b97dbull, 0x970f24b9078ea7c7ull, 0x8f4bacefadb4bcb1ull, \
    0xa1802fdd5c8f452bull, 0xde85f58b25603303ull, 0x364762f470077587ull, 0x7f864ce0775a0c77ull, \
    0x73cc8629f782b791ull, 0x5b3cac1b3a1059edull, 0xf3f2d21e76f5d423ull, 0x5311b35a85f468b1ull, \
    0x9e88fd5a131be1adull, 0x9e9c01811d2017e5ull, 0x129062e2de60e9ffull, 0x56392910d55d4001ull, \
@@ -44,7 +44,8 @@ constexpr uint32_t BB_MAX_LEVELS = 64;
    0x723c864e2ada4953ull, 0x533aa12154e09b8full, 0x516fa0ddd045e98bull, 0x8da77e07eff2b063ull, \
    0xe9b3bdcdc9c409cdull, 0x9b6df4ffc06e320full, 0x0550f8043685bb11ull, 0x42c2a6bcdd74430bull}
 static __constant__ uint64_t c_bb_mul[BB_MAX_LEVELS] = CF1_BB_MUL_TABLE;
-static const uint64_t h_bb_mul[BB_MAX_LEVELS] = CF1_BB_MUL_TABLE;
+static constexpr uint64_t h_bb_mul[BB_MAX_LEVELS] = CF1_BB_MUL_TABLE;
+static_assert(h_bb_mul[0] == KEY_SPREAD_MUL, "level 0 must hash like the unsorted phase-3 split");
 
 CF1_HD uint64_t bb_key_hash(uint64_t key) { return key; }
 CF1_HD uint64_t bb_key_hash(const Key2 &key) { return KOps<Key2>::hash(key, BB_SEED); }

@@ -39,7 +39,7 @@ constexpr uint32_t cs_cap() { return KOps<KeyT>::WORDS == 1 ? 8192u : 4096u; }
 // of key * MS_HASH_MUL.  The product's top bits spread any key set evenly,
 // where the key's own top bits -- the first bases of a canonical k-mer --
 // are skewed several-fold.  (64-bit keys; wider keys always sort.)
-constexpr uint64_t MS_HASH_MUL = 0xD6E8FEB86659FD93ull;
+constexpr uint64_t MS_HASH_MUL = KEY_SPREAD_MUL;
 template <class KeyT>
 CF1_D uint32_t ms_digit(const KeyT &k, int shift, uint32_t mask, bool hashed);
 template <>
