@@ -31,8 +31,12 @@ constexpr uint32_t CS_BUCKETS = 1u << CS_BITS;
 constexpr uint32_t CS_SMALL = 512;
 constexpr uint32_t CS_DEDUP_MIN = 64;  // 64-bit sub-buckets above this size are deduplicated first
 
-template <class KeyT>
-constexpr uint32_t cs_cap() { return KOps<KeyT>::WORDS == 1 ? 8192u : 4096u; }
+// Keys a sub-bucket's shared-memory sort holds.  The unsorted (deduplicate
+// only) path keeps 64-bit sub-buckets at half that size, so its shared memory
+// fits four CTAs per SM instead of two.
+constexpr uint32_t cs_cap_for(bool wide, bool sorted) { return wide ? 4096u : (sorted ? 8192u : 4096u); }
+template <class KeyT, bool SORTED = true>
+constexpr uint32_t cs_cap() { return cs_cap_for(KOps<KeyT>::WORDS == 2, SORTED); }
 
 // Digit of a key in a multisplit pass: bits [shift, shift + width) of the key
 // or, when only the distinct keys and not their order are needed (hashed),
@@ -361,7 +365,7 @@ template <class KeyT, bool SORTED>
 __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT *U, const uint64_t *sb_off,
                                                                   uint64_t nsub, int shift, int bits, uint32_t *cnt,
                                                                   uint32_t *oversize) {
-  constexpr uint32_t CAP = cs_cap<KeyT>();
+  constexpr uint32_t CAP = cs_cap<KeyT, SORTED>();
   extern __shared__ __align__(16) unsigned char cs_smem[];
   KeyT *S = reinterpret_cast<KeyT *>(cs_smem);                    // [CAP]
   uint32_t *hist = reinterpret_cast<uint32_t *>(S + CAP);         // [CS_BUCKETS]
@@ -566,7 +570,8 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted) {
   // size run several times over it (the first bases of canonical k-mers are
   // skewed ~5x), so 64-bit keys aim lower to stay within shared memory
   // (3.1 Gbp, k = 31: 14 bits instead of 12, phase 3 245 -> 230 ms).
-  const uint64_t target = sorted && KOps<KeyT>::WORDS == 1 ? cs_cap<KeyT>() / 8 : cs_cap<KeyT>() / 2;
+  const uint64_t target = sorted && KOps<KeyT>::WORDS == 1 ? cs_cap<KeyT, true>() / 8
+                                                            : cs_cap_for(KOps<KeyT>::WORDS == 2, sorted) / 2;
   int p = 0;
   while (p < 16 && (max_bin_keys >> p) > target) p++;
   return p;
@@ -619,7 +624,7 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
     shift = 0;
   }
   // S, hist, cur, pstart (u32) and the chunk bounds (u16)
-  size_t smem = cs_cap<KeyT>() * sizeof(KeyT) + (3 * CS_BUCKETS + 1) * sizeof(uint32_t) +
+  size_t smem = cs_cap_for(KOps<KeyT>::WORDS == 2, sorted) * sizeof(KeyT) + (3 * CS_BUCKETS + 1) * sizeof(uint32_t) +
                 (CS_BUCKETS + 1) * sizeof(uint16_t);
   auto kern = sorted ? cs_sort_unique_kernel<KeyT, true> : cs_sort_unique_kernel<KeyT, false>;
   CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
