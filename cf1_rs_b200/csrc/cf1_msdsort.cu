@@ -1,11 +1,13 @@
-// Phase 3a, MSD form: sorted distinct canonical k-mers per bin.
+// Phase 3a, MSD form: distinct canonical k-mers per bin, sorted or not.
 //
-//   1. one or two stable multisplit passes on the top P bits of the keys,
-//      segmented by bin (P chosen so a sub-bucket holds ~CAP/3 keys);
-//   2. one CTA per sub-bucket: counting sort on the next 10 bits in shared
-//      memory, insertion sort of the small buckets (bitonic sort of the whole
-//      sub-bucket if any bucket is large), adjacent-unique, distinct keys
-//      written back at the sub-bucket's start;
+//   1. one or two multisplit passes on the top P bits of the keys (sorted) or
+//      of key * KEY_SPREAD_MUL (distinct only), segmented by bin (P chosen so
+//      a sub-bucket fits shared memory);
+//   2. one CTA per sub-bucket: a shared-memory hash set keeps one copy of
+//      each key; the sorted form then counting-sorts on the next 10 bits,
+//      insertion-sorts the small buckets (bitonic sort of the whole
+//      sub-bucket if any bucket is large); distinct keys are written back at
+//      the sub-bucket's start;
 //   3. a scan of the per-sub-bucket counts and a copy into the dense distinct
 //      array; a bin's first sub-bucket gives its slot offset.
 // A sub-bucket above CAP keys (long homopolymers, huge tandem arrays) makes
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, con
 // and each digit's run is written out with consecutive threads on
 // consecutive addresses.
 template <class KeyT, int BITS>
-__global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
+__global__ void __launch_bounds__(MS_BLOCK, KOps<KeyT>::WORDS == 1 ? 3 : 4) ms_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
                                                                  const uint32_t *tile_off, uint32_t nseg, int shift,
                                                                  bool hashed, const uint64_t *Hs) {
   constexpr uint32_t DIG = 1u << BITS;
@@ -105,16 +107,27 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
   __syncthreads();
   const uint32_t n = (uint32_t)(sp.end - sp.start);
   // per key: (rank in the warp's slice for its digit) << 8 | digit, or ~0
-  // for lanes past the tile; keys are read again when staged, which keeps
-  // the register count (and so the occupancy) down
+  // for lanes past the tile (128-bit keys are read again when staged, which
+  // keeps their register count down)
   uint32_t pk[MS_ITEMS];
   uint32_t *wh = whist + warp * DIG;
+  // 64-bit keys: all of the thread's loads are issued before the first is
+  // used, and the keys stay in registers for the staging step
+  constexpr bool HOLD = KOps<KeyT>::WORDS == 1;
+  KeyT kk[HOLD ? MS_ITEMS : 1];
+  if constexpr (HOLD) {
+#pragma unroll
+    for (int r = 0; r < MS_ITEMS; r++) {
+      uint32_t li = warp * (MS_ITEMS * 32) + r * 32 + lane;
+      kk[r] = li < n ? in[sp.start + li] : KeyT{};
+    }
+  }
 #pragma unroll
   for (int r = 0; r < MS_ITEMS; r++) {
     uint32_t li = warp * (MS_ITEMS * 32) + r * 32 + lane;
     pk[r] = 0xFFFFFFFFu;
     if (li < n) {
-      uint32_t d = ms_digit(in[sp.start + li], shift, DIG - 1, hashed);
+      uint32_t d = ms_digit(HOLD ? kk[HOLD ? r : 0] : in[sp.start + li], shift, DIG - 1, hashed);
       pk[r] = (atomicAdd(&wh[d], 1u) << 8) | d;
     }
   }
@@ -150,7 +163,7 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
   for (int r = 0; r < MS_ITEMS; r++) {
     if (pk[r] != 0xFFFFFFFFu) {
       uint32_t d = pk[r] & 0xFF, li = warp * (MS_ITEMS * 32) + r * 32 + lane;
-      stage[lstart[d] + wh[d] + (pk[r] >> 8)] = in[sp.start + li];
+      stage[lstart[d] + wh[d] + (pk[r] >> 8)] = HOLD ? kk[HOLD ? r : 0] : in[sp.start + li];
     }
   }
   __syncthreads();
@@ -200,8 +213,8 @@ CF1_D uint32_t cs_hash_dedup(uint64_t *T, uint64_t a, uint64_t n, uint64_t *S, u
   (void)sm;
   const unsigned tid = threadIdx.x, lane = lane_id();
   const uint64_t EMPTY = ~0ull;  // above every key (keys use at most 62 bits)
-  uint32_t tsize = 64, tbits = 6;  // a power of two >= 2n, at most cap
-  while (tsize < cap && (uint64_t)tsize < 2 * n) {
+  uint32_t tsize = 64, tbits = 6;  // a power of two >= 1.5 n, at most cap
+  while (tsize < cap && (uint64_t)tsize < n + n / 2) {
     tsize <<= 1;
     tbits++;
   }
