@@ -70,7 +70,7 @@ EXPORTED = [
     "cf1gpu_default_opts", "cf1gpu_create", "cf1gpu_add_record", "cf1gpu_add_records", "cf1gpu_add_fasta",
     "cf1gpu_reset_input", "cf1gpu_upload", "cf1gpu_run_resident", "cf1gpu_run_phases_1_4", "cf1gpu_get_stats",
     "cf1gpu_total_kmers", "cf1gpu_bin_distinct_counts", "cf1gpu_copy_states", "cf1gpu_query", "cf1gpu_dump_states", "cf1gpu_verify_bijection",
-    "cf1gpu_short_seq_count", "cf1gpu_short_seq", "cf1gpu_export_mphf", "cf1gpu_mphf_host_query",
+    "cf1gpu_short_seq_count", "cf1gpu_short_seq", "cf1gpu_export_mphf", "cf1gpu_export_bin", "cf1gpu_mphf_host_query",
     "cf1gpu_learned_stats", "cf1gpu_learned_grad", "cf1gpu_last_error", "cf1gpu_destroy", "cf1gpu_version",
     "cf1gpu_distinct_kmers_noalloc",
 ]
@@ -107,6 +107,7 @@ def lib():
     L.cf1gpu_short_seq.argtypes = [vp, C.c_size_t, C.c_char_p, C.c_size_t, u64p]
     L.cf1gpu_export_mphf.argtypes = [vp, vp, C.POINTER(C.c_size_t)]
     L.cf1gpu_mphf_host_query.argtypes = [vp, C.c_size_t, u64p, C.c_size_t, u64p]
+    L.cf1gpu_export_bin.argtypes = [vp, C.c_uint32, u8p, C.POINTER(C.c_size_t)]
     L.cf1gpu_learned_stats.argtypes = [vp, C.POINTER(C.c_double)]
     L.cf1gpu_learned_grad.argtypes = [C.c_int, f32p, f32p, f32p, C.c_size_t, f32p, f32p]
     L.cf1gpu_last_error.argtypes = [vp]
@@ -293,6 +294,21 @@ class Cf1Gpu:
             self._check(lib().cf1gpu_short_seq(self.h, i, buf, 4096, C.byref(ln)))
             out.append((buf.value.decode(), ln.value))
         return out
+
+    def export_bin(self, b: int) -> bytes:
+        """Bin b's super k-mers in the reference's on-disk bin record format."""
+        need = C.c_size_t(0)
+        self._check(lib().cf1gpu_export_bin(self.h, b, None, C.byref(need)))
+        buf = np.empty(max(1, need.value), np.uint8)
+        size = C.c_size_t(need.value)
+        self._check(lib().cf1gpu_export_bin(self.h, b, _p(buf, u8p), C.byref(size)))
+        return buf[: size.value].tobytes()
+
+    def write_bin_files(self, work_dir: str) -> None:
+        """cf1_bin_%05d.bin for every bin, as route_superkmers names them."""
+        for b in range(self.num_bins):
+            with open(os.path.join(work_dir, f"cf1_bin_{b:05d}.bin"), "wb") as f:
+                f.write(self.export_bin(b))
 
     def export_mphf(self) -> np.ndarray:
         need = C.c_size_t(0)

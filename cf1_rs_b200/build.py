@@ -34,6 +34,7 @@ SOURCES = [
     "cf1_capi.cu",
     "cf1_noalloc.cu",
     "cf1_tuner.cu",
+    "cf1_binfile.cu",
 ]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] if os.path.isdir(CSRC) else []
 

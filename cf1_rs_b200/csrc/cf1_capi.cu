@@ -171,6 +171,19 @@ int cf1gpu_get_stats(const cf1gpu_ctx *c, cf1gpu_stats *out) {
 
 uint64_t cf1gpu_total_kmers(const cf1gpu_ctx *c) { return (c && c->ran) ? c->n_distinct : 0; }
 
+int cf1gpu_export_bin(cf1gpu_ctx *c, uint32_t bin, uint8_t *dst, size_t *bytes) {
+  if (!c || !bytes) return CF1GPU_ERR_INVALID_ARG;
+  if (!c->ran) {
+    c->last_error = "no results: run phases 1-4 first";
+    return CF1GPU_ERR_STATE;
+  }
+  if (bin >= c->opts.num_bins) {
+    c->last_error = "bin must be below num_bins = " + std::to_string(c->opts.num_bins);
+    return CF1GPU_ERR_INVALID_ARG;
+  }
+  return guard(c, [&] { *bytes = cf1::export_bin(c, bin, dst, dst ? *bytes : 0); });
+}
+
 int cf1gpu_bin_distinct_counts(const cf1gpu_ctx *c, uint64_t *counts, size_t nbins) {
   if (!c || (nbins && !counts)) return CF1GPU_ERR_INVALID_ARG;
   cf1gpu_ctx *m = const_cast<cf1gpu_ctx *>(c);

@@ -16,5 +16,6 @@ void verify_bijection(cf1gpu_ctx *c);
 void query(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots);
 void learned_summary(const cf1gpu_ctx *c, double out5[5]);
 size_t export_mphf(cf1gpu_ctx *c, void *dst, size_t cap);
+size_t export_bin(cf1gpu_ctx *c, uint32_t bin, uint8_t *dst, size_t cap);
 void host_query(const void *image, size_t bytes, const uint64_t *keys, size_t n, uint64_t *slots);
 }  // namespace cf1

@@ -186,6 +186,16 @@ int cf1gpu_short_seq(const cf1gpu_ctx *ctx, size_t i, char *name_buf, size_t nam
  * be 16-byte aligned. */
 int cf1gpu_export_mphf(cf1gpu_ctx *ctx, void *dst, size_t *bytes);
 
+/* Bin `bin`'s super k-mers in the reference's on-disk bin record format
+ * (src/superkmer.rs:181-202: per super k-mer a little-endian u16 base count,
+ * then the bases 2-bit packed four per byte, first base in the top bits --
+ * the bytes route_superkmers writes to cf1_bin_%05d.bin, superkmer.rs:224-226,
+ * and BinReader::read_packed_superkmer reads, superkmer.rs:283-298).  Super
+ * k-mers in this library's routing order.  Call with dst NULL to get the size
+ * in *bytes; otherwise *bytes is the buffer's size and receives the size
+ * written. */
+int cf1gpu_export_bin(cf1gpu_ctx *ctx, uint32_t bin, uint8_t *dst, size_t *bytes);
+
 /* Mphf::hash on the host over an exported image (thread-safe, no device);
  * image must be 16-byte aligned. */
 int cf1gpu_mphf_host_query(const void *image, size_t bytes, const uint64_t *keys, size_t n, uint64_t *slots);

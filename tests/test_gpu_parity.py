@@ -209,6 +209,59 @@ def test_autotuner_cache(mode, batched):
         g2.close()
 
 
+def _read_bin_records(data: bytes):
+    """Super k-mers of a bin file (the reader of src/superkmer.rs:283-298)."""
+    out, i = [], 0
+    while i < len(data):
+        n = data[i] | (data[i + 1] << 8)
+        nb = (n + 3) // 4
+        packed = data[i + 2: i + 2 + nb]
+        out.append("".join("ACGT"[(packed[j // 4] >> (6 - 2 * (j % 4))) & 3] for j in range(n)))
+        i += 2 + nb
+    assert i == len(data)
+    return out
+
+
+def _canon(kmer: str) -> str:
+    rc = kmer.translate(str.maketrans("ACGT", "TGCA"))[::-1]
+    return min(kmer, rc)
+
+
+@pytest.mark.parametrize("k", [21, 31, 45])
+def test_bin_files_match_routing(k):
+    # every k-mer occurrence is in exactly one exported super k-mer, and a
+    # bin file's k-mers are the distinct k-mers the device put in that bin
+    recs = random_records(31337 + k, k, n_records=40, max_len=3000)
+    seq, off = o.concat_records(recs)
+    g, ref = assert_parity(seq, off, k, num_bins=8, mode="learned")
+    keys, _ = g.dump_states()
+    counts = g.bin_distinct_counts()
+    ends = np.cumsum(counts)
+    occ = 0
+    with tempfile.TemporaryDirectory() as d:
+        g.write_bin_files(d)
+        for b in range(8):
+            data = open(os.path.join(d, f"cf1_bin_{b:05d}.bin"), "rb").read()
+            assert data == g.export_bin(b)
+            kmers = set()
+            for sk in _read_bin_records(data):
+                assert len(sk) >= k
+                occ += len(sk) - k + 1
+                for i in range(len(sk) - k + 1):
+                    kmers.add(_canon(sk[i: i + k]))
+            lo = int(ends[b] - counts[b])
+            want = set()
+            for kk in keys[lo: int(ends[b])]:
+                if keys.ndim == 1:
+                    v = int(kk)
+                else:
+                    v = int(kk[0]) | (int(kk[1]) << 64)
+                want.add("".join("ACGT"[(v >> (2 * (k - 1 - j))) & 3] for j in range(k)))
+            assert kmers == want, f"bin {b}"
+    assert occ == ref.n_occ
+    g.close()
+
+
 def test_deterministic_repeat_runs():
     recs = random_records(3, 31, n_records=100, max_len=8000)
     seq, off = o.concat_records(recs)
