@@ -11,10 +11,11 @@ classification into the 5-bit state vector.
   value : distinct k-mers / device time of a step, input resident in HBM
           (library CUDA events on its stream; the input is 3.1 GB, larger
           than the 126 MB L2, so steps do not reuse cached data)
-  e2e   : the same metric through the C ABI from host buffers: records in
-          page-locked host memory DMA'd to the device, phases 1-4, and the
-          state vector copied back into page-locked memory, timed on the host
-          around synchronous calls
+  e2e   : the same metric through the C ABI from host buffers, one
+          cf1gpu_run_streamed call per step: records in page-locked host
+          memory DMA'd to the device in chunks while phase 1 scans, phases
+          1-4, and the state words copied back into page-locked memory stage
+          by stage while phase 4 runs; timed on the host around the call
 
 With N GPUs (torchrun, one rank per GPU) the genome is sharded by bin: every
 rank routes it whole, keeps the bins b with b % N == rank for phases 3-4, and
@@ -331,11 +332,8 @@ def gpu_arm(args):
         for i in range(args.warmup + args.steps):
             barrier()
             t0 = time.perf_counter()
-            g.reset_input()
-            g.add_records(seq_h, x.offsets)
-            g.run()
+            g.run_streamed(seq_h, x.offsets, words)  # copies overlapped with phases 1 and 4
             exchange_ms(g)
-            g.states(out=words)
             dt = time.perf_counter() - t0
             if i >= args.warmup:
                 times.append(dt)

@@ -68,7 +68,8 @@ f32p = C.POINTER(C.c_float)
 # Every symbol include/cf1gpu.h declares.
 EXPORTED = [
     "cf1gpu_default_opts", "cf1gpu_create", "cf1gpu_add_record", "cf1gpu_add_records", "cf1gpu_add_fasta",
-    "cf1gpu_reset_input", "cf1gpu_upload", "cf1gpu_run_resident", "cf1gpu_run_phases_1_4", "cf1gpu_get_stats",
+    "cf1gpu_reset_input", "cf1gpu_upload", "cf1gpu_run_resident", "cf1gpu_run_phases_1_4", "cf1gpu_run_streamed",
+    "cf1gpu_get_stats",
     "cf1gpu_total_kmers", "cf1gpu_bin_distinct_counts", "cf1gpu_copy_states", "cf1gpu_query", "cf1gpu_dump_states", "cf1gpu_verify_bijection",
     "cf1gpu_short_seq_count", "cf1gpu_short_seq", "cf1gpu_export_mphf", "cf1gpu_export_bin", "cf1gpu_mphf_host_query",
     "cf1gpu_learned_stats", "cf1gpu_learned_grad", "cf1gpu_last_error", "cf1gpu_destroy", "cf1gpu_version",
@@ -96,6 +97,7 @@ def lib():
               "cf1gpu_verify_bijection"):
         getattr(L, n).argtypes = [vp]
     L.cf1gpu_get_stats.argtypes = [vp, C.POINTER(Stats)]
+    L.cf1gpu_run_streamed.argtypes = [vp, u8p, u64p, C.c_size_t, u64p, C.c_size_t, C.POINTER(C.c_size_t)]
     L.cf1gpu_total_kmers.argtypes = [vp]
     L.cf1gpu_total_kmers.restype = C.c_uint64
     L.cf1gpu_bin_distinct_counts.argtypes = [vp, u64p, C.c_size_t]
@@ -260,6 +262,21 @@ class Cf1Gpu:
         out = np.empty(self.num_bins, np.uint64)
         self._check(lib().cf1gpu_bin_distinct_counts(self.h, _p(out, u64p), self.num_bins))
         return out
+
+    def run_streamed(self, seq: np.ndarray, offsets: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        """Input in, state words out, copies overlapped with phases 1 and 4
+        (see cf1gpu_run_streamed).  `out` (u64) must hold the words; by
+        default it is sized for every k-mer window being distinct."""
+        seq = np.ascontiguousarray(seq, np.uint8)
+        offsets = np.ascontiguousarray(offsets, np.uint64)
+        if seq.size == 0:
+            seq = np.zeros(1, np.uint8)
+        if out is None:
+            out = np.empty(int(offsets[-1]) // 12 + 2 if len(offsets) else 1, np.uint64)
+        nw = C.c_size_t(0)
+        self._check(lib().cf1gpu_run_streamed(self.h, _p(seq, u8p), _p(offsets, u64p), len(offsets) - 1,
+                                              _p(out, u64p), out.size, C.byref(nw)))
+        return out[: nw.value]
 
     def states(self, out: np.ndarray | None = None) -> np.ndarray:
         nw = (self.total_kmers() + 11) // 12

@@ -99,7 +99,9 @@ int cf1gpu_create(const cf1gpu_opts *opts, cf1gpu_ctx **out) {
     CF1_CUDA(cudaGetDeviceProperties(&prop, opts->device));
     c->num_sms = prop.multiProcessorCount;
     CF1_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CF1_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     for (auto &e : c->ev) CF1_CUDA(cudaEventCreate(&e));
+    for (auto &e : c->stage_ev) CF1_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if (opts->sk_tile) c->tune.sk_tile = opts->sk_tile;
     if (opts->learned_max_err) c->learned.max_err = opts->learned_max_err;
     if (opts->learned_train_steps > 0) c->learned.train_steps = opts->learned_train_steps;
@@ -170,6 +172,15 @@ int cf1gpu_get_stats(const cf1gpu_ctx *c, cf1gpu_stats *out) {
 }
 
 uint64_t cf1gpu_total_kmers(const cf1gpu_ctx *c) { return (c && c->ran) ? c->n_distinct : 0; }
+
+int cf1gpu_run_streamed(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *offsets, size_t n_records,
+                        uint64_t *state_words, size_t words_cap, size_t *n_words) {
+  if (!c || !n_words || (n_records && (!seqs || !offsets)) || (words_cap && !state_words))
+    return CF1GPU_ERR_INVALID_ARG;
+  for (size_t i = 0; i < n_records; i++)
+    if (offsets[i + 1] < offsets[i]) return CF1GPU_ERR_INVALID_ARG;
+  return guard(c, [&] { *n_words = cf1::run_streamed(c, seqs, offsets, n_records, state_words, words_cap); });
+}
 
 int cf1gpu_export_bin(cf1gpu_ctx *c, uint32_t bin, uint8_t *dst, size_t *bytes) {
   if (!c || !bytes) return CF1GPU_ERR_INVALID_ARG;
@@ -317,9 +328,13 @@ const char *cf1gpu_last_error(const cf1gpu_ctx *c) { return c ? c->last_error.c_
 void cf1gpu_destroy(cf1gpu_ctx *c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto &e : c->stage_ev)
+    if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   delete c;
 }
 

@@ -50,7 +50,9 @@ struct cf1gpu_ctx {
   bool wide = false;  // k > 32: 128-bit keys
   std::string last_error;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // streamed runs: host<->device copies beside the kernels
   cudaEvent_t ev[12] = {};
+  cudaEvent_t stage_ev[8] = {};        // streamed runs: a phase-4 stage's words are packed
   int num_sms = 148;
   cf1::Tuning tune;
   cf1::LearnedOpts learned;

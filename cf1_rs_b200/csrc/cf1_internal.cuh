@@ -116,6 +116,9 @@ void segment_tiles_counts(const uint64_t *cnt, uint32_t nseg, uint32_t tile, uin
 
 // ------------------------------------------------------------ phase kernels ----
 void launch_pack(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, cudaStream_t s);
+// The same for the W/NM words [w0, w1) only (64 bases per word of NM).
+void launch_pack_words(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, uint64_t w0, uint64_t w1,
+                       cudaStream_t s);
 
 struct SuperkmerArgs {
   const uint64_t *W;
@@ -123,7 +126,8 @@ struct SuperkmerArgs {
   uint64_t L;
   int k, m, w;
   uint32_t tile;          // k-mer positions per tile
-  uint64_t n_tiles;
+  uint64_t n_tiles;       // tiles [tile_begin, n_tiles) of this launch
+  uint64_t tile_begin;    // first tile (one CTA per tile from here; 0 in persistent mode)
   uint32_t *tile_counter; // persistent mode: atomic work queue (zeroed); nullptr = one CTA per tile
   uint32_t *hist;         // [65536] super k-mers per bucket (zeroed)
   unsigned long long *n_kmers;    // valid k-mer windows (zeroed)

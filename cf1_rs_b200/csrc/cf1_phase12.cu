@@ -18,8 +18,8 @@ namespace {
 // a base when (byte & 0xDF) is one of 'A' 'C' 'G' 'T' (upper- or lower-case,
 // src/dna.rs:64-92); bits 1-2 of the upper-case letter give A0 C1 G3 T2, and
 // one xor fixes G/T.
-__global__ void pack_kernel(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, uint64_t n_nm) {
-  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void pack_kernel(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, uint64_t t0, uint64_t n_nm) {
+  uint64_t t = t0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_nm) return;
   uint64_t base = t * 64;
   uint64_t bytes[8];
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
   const int k = a.k, m = a.m, w = a.w;
   const unsigned tid = threadIdx.x;
   const uint64_t NK = a.L - (uint64_t)k + 1;
-  uint64_t tile = blockIdx.x;
+  uint64_t tile = a.tile_begin + blockIdx.x;
   unsigned long long my_kmers = 0;
   for (;;) {
     if (a.tile_counter) {
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(BS_BLOCK) bin_scatter_kernel(const uint64_t *r
 }
 
 void launch_sk(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
-  if (a.n_tiles == 0) return;
+  if (a.n_tiles <= a.tile_begin) return;
   size_t smem = 2 * (a.tile + 64) * sizeof(uint32_t);
   switch (a.tile) {
 #define CF1_SK_CASE(IT)                                                                              \
@@ -239,7 +239,7 @@ void launch_sk(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
     auto kern = superkmer_kernel<SK_BLOCK, IT>;                                                    \
     CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
     unsigned grid = persistent_ctas ? persistent_grid(kern, SK_BLOCK, smem, persistent_ctas, a.n_tiles) \
-                                    : (unsigned)a.n_tiles;                                         \
+                                    : (unsigned)(a.n_tiles - a.tile_begin);                        \
     kern<<<grid, SK_BLOCK, smem, s>>>(a);                                                          \
     break;                                                                                         \
   }
@@ -324,9 +324,13 @@ __global__ void __launch_bounds__(1024) partition_kernel(const uint32_t *hist, u
 }  // namespace
 
 void launch_pack(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, cudaStream_t s) {
-  uint64_t n_nm = ceil_div(L, 64);
-  if (n_nm == 0) return;
-  pack_kernel<<<(unsigned)ceil_div(n_nm, 256), 256, 0, s>>>(ascii, L, W, NM, n_nm);
+  launch_pack_words(ascii, L, W, NM, 0, ceil_div(L, 64), s);
+}
+
+void launch_pack_words(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, uint64_t w0, uint64_t w1,
+                       cudaStream_t s) {
+  if (w1 <= w0) return;
+  pack_kernel<<<(unsigned)ceil_div(w1 - w0, 256), 256, 0, s>>>(ascii, L, W, NM, w0, w1);
   CF1_LAUNCH_CHECK();
 }
 

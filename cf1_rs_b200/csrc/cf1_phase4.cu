@@ -106,13 +106,13 @@ __global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a
 
 // Word w of the state vector from side-set bytes 12w .. 12w+11 (three u32).
 constexpr int PK_BLOCK = 256;
-__global__ void __launch_bounds__(PK_BLOCK) sideset_pack_kernel(const uint32_t *sides, uint64_t nwords,
+__global__ void __launch_bounds__(PK_BLOCK) sideset_pack_kernel(const uint32_t *sides, uint64_t w0, uint64_t w1,
                                                                 unsigned long long *states) {
   __shared__ uint8_t lut[256];  // side-set byte -> 5-bit state
   lut[threadIdx.x] = (uint8_t)state_of_sideset(threadIdx.x);
   __syncthreads();
-  uint64_t w = (uint64_t)blockIdx.x * PK_BLOCK + threadIdx.x;
-  if (w >= nwords) return;
+  uint64_t w = w0 + (uint64_t)blockIdx.x * PK_BLOCK + threadIdx.x;
+  if (w >= w1) return;
   const uint32_t *q = sides + 3 * w;
   uint32_t b[3] = {q[0], q[1], q[2]};
   unsigned long long out = 0;
@@ -196,9 +196,10 @@ void launch_classify(const ClassifyArgs<KeyT> &a, int persistent_ctas, cudaStrea
   CF1_LAUNCH_CHECK();
 }
 
-void launch_sideset_pack(const uint32_t *sides, uint64_t nwords, unsigned long long *states, cudaStream_t s) {
-  if (!nwords) return;
-  sideset_pack_kernel<<<(unsigned)ceil_div(nwords, PK_BLOCK), PK_BLOCK, 0, s>>>(sides, nwords, states);
+void launch_sideset_pack(const uint32_t *sides, uint64_t w0, uint64_t w1, unsigned long long *states,
+                         cudaStream_t s) {
+  if (w1 <= w0) return;
+  sideset_pack_kernel<<<(unsigned)ceil_div(w1 - w0, PK_BLOCK), PK_BLOCK, 0, s>>>(sides, w0, w1, states);
   CF1_LAUNCH_CHECK();
 }
 

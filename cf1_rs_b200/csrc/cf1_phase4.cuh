@@ -23,8 +23,9 @@ struct ClassifyArgs {
 template <class KeyT>
 void launch_classify(const ClassifyArgs<KeyT> &a, int persistent_ctas, cudaStream_t s);
 
-// Packs side-set bytes (3 u32 per state word) into nwords state words.
-void launch_sideset_pack(const uint32_t *sides, uint64_t nwords, unsigned long long *states, cudaStream_t s);
+// Packs side-set bytes (3 u32 per state word) into state words [w0, w1).
+void launch_sideset_pack(const uint32_t *sides, uint64_t w0, uint64_t w1, unsigned long long *states,
+                         cudaStream_t s);
 
 template <class KeyT>
 void launch_dump(const MphfView<KeyT> &m, uint32_t nbins, uint64_t n, const unsigned long long *states, uint64_t *keys_out,

@@ -95,8 +95,41 @@ MphfView<KeyT> make_view(cf1gpu_ctx *c) {
   return v;
 }
 
+// Direct intake of records given in page-locked host memory: one DMA of the
+// caller's bytes into a device buffer, then tiles of it are moved to their
+// places in the concatenation, a placeholder after each record.
+struct IntakeTile {
+  uint64_t src, dst;
+  uint32_t len, last;  // last: the tile ends its record
+};
+constexpr uint32_t INTAKE_TILE = 1u << 16;
+
+__global__ void intake_kernel(const uint8_t *raw, const IntakeTile *tiles, uint8_t *out) {
+  const IntakeTile t = tiles[blockIdx.x];
+  for (uint32_t i = threadIdx.x; i < t.len; i += blockDim.x) out[t.dst + i] = raw[t.src + i];
+  if (t.last && threadIdx.x == 0) out[t.dst + t.len] = 'N';
+}
+
+// The host ends of a streamed run (cf1gpu_run_streamed).  In: the caller's
+// record bytes arrive in d_raw chunk by chunk on the copy stream; phase 1
+// places, packs and scans each stretch as soon as its chunk is in.  Out:
+// phase 4 runs in stages of whole bins, and the state words every stage
+// completes go back to the caller on the copy stream while the next stage
+// classifies.
+struct StreamIO {
+  const uint8_t *raw = nullptr;            // device copy of the record bytes
+  const IntakeTile *tiles = nullptr;       // device intake tiles, in source order
+  std::vector<IntakeTile> htiles;          // the same on the host
+  std::vector<uint64_t> chunk_end;         // raw bytes in place after chunk c
+  std::vector<cudaEvent_t> chunk_ev;       // recorded on the copy stream after chunk c
+  uint64_t *host_words = nullptr;          // caller's state-word buffer
+  uint64_t host_cap = 0;                   // its size in words
+  bool words_done = false;                 // the run copied all words back
+};
+constexpr int STREAM_STAGES = 8;
+
 template <class KeyT>
-void run_impl(cf1gpu_ctx *c) {
+void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
   cudaStream_t s = c->stream;
   Backend<KeyT> &be = backend<KeyT>(c);
   const uint64_t L = c->L;
@@ -110,7 +143,7 @@ void run_impl(cf1gpu_ctx *c) {
   const bool sorted = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED || c->opts.sort_mode == 1 || KOps<KeyT>::WORDS == 2;
   // autotuner: parameters of this input class from the cache, or measured
   // in this run and stored
-  bool tune_now = false;
+  bool tune_now = false;  // (streamed runs do not measure: their phase 1 waits on the input)
   TuneValue tuned;
   tuned.sk_tile = c->tune.sk_tile;
   c->tuner_state = 0;
@@ -129,7 +162,7 @@ void run_impl(cf1gpu_ctx *c) {
       c->tuned_key = key;
       c->tune_valid = true;
       c->tuner_state = 1;
-    } else {
+    } else if (!io) {
       c->tuned_key = key;
       c->tune_valid = false;
       tune_now = true;
@@ -145,7 +178,7 @@ void run_impl(cf1gpu_ctx *c) {
   uint64_t *NM = c->d_NM.get<uint64_t>(n_nm + 2);
   CF1_CUDA(cudaMemsetAsync(W + 2 * n_nm, 0, 4 * sizeof(uint64_t), s));
   CF1_CUDA(cudaMemsetAsync(NM + n_nm, 0xFF, 2 * sizeof(uint64_t), s));
-  launch_pack(c->d_ascii.as<uint8_t>(), L, W, NM, s);
+  if (!io) launch_pack(c->d_ascii.as<uint8_t>(), L, W, NM, s);
   uint32_t *hist = c->d_hist.get<uint32_t>(NUM_BUCKETS);
   SuperkmerArgs a{};
   a.W = W;
@@ -191,7 +224,65 @@ void run_impl(cf1gpu_ctx *c) {
       c->rec_cap_hint = hs.rec_count;
     }
   };
-  if (tune_now && c->opts.sk_tile == 0) {  // autotuner: time each tile, keep the fastest
+  if (io) {
+    // Streamed intake: as chunk c of the record bytes lands, place the intake
+    // tiles it completes, pack the W/NM words wholly inside the placed
+    // prefix, and scan the minimizer tiles whose bases are all packed.  The
+    // scan is the usual one, launched over tile ranges (no persistent queue).
+    uint8_t *ascii = c->d_ascii.as<uint8_t>();
+    a.tile = c->tune.sk_tile;
+    a.n_tiles = L >= (uint64_t)k ? ceil_div(L - k + 1, a.tile) : 0;
+    a.tile_counter = nullptr;
+    a.rec_cap = std::max<uint64_t>(c->rec_cap_hint, L / 4 + 1024);
+    uint8_t *rbuf = static_cast<uint8_t *>(c->d_keys.reserve(a.rec_cap * (sizeof(uint64_t) + sizeof(uint16_t))));
+    a.rec_tmp = reinterpret_cast<uint64_t *>(rbuf);
+    a.rec_bucket = reinterpret_cast<uint16_t *>(rbuf + a.rec_cap * sizeof(uint64_t));
+    CF1_CUDA(cudaMemsetAsync(hist, 0, NUM_BUCKETS * sizeof(uint32_t), s));
+    CF1_CUDA(cudaMemsetAsync(sm, 0, sizeof(Small), s));
+    const uint64_t ntiles_in = io->htiles.size(), T = a.tile;
+    uint64_t placed = 0, packed = 0, scanned = 0;
+    for (size_t ch = 0; ch < io->chunk_ev.size(); ch++) {
+      const bool last = ch + 1 == io->chunk_ev.size();
+      CF1_CUDA(cudaStreamWaitEvent(s, io->chunk_ev[ch], 0));
+      uint64_t t_end = placed;
+      while (t_end < ntiles_in && io->htiles[t_end].src + io->htiles[t_end].len <= io->chunk_end[ch]) t_end++;
+      if (t_end > placed) {
+        intake_kernel<<<(unsigned)(t_end - placed), 256, 0, s>>>(io->raw, io->tiles + placed, ascii);
+        CF1_LAUNCH_CHECK();
+        placed = t_end;
+      }
+      const uint64_t prefix = (last || placed == ntiles_in) ? L : io->htiles[placed].dst;
+      const uint64_t pw = last ? n_nm : prefix / 64;
+      launch_pack_words(ascii, L, W, NM, packed, pw, s);
+      packed = std::max(packed, pw);
+      // a tile reads bases up to (t+1) T + k - 1, W and NM one word beyond
+      uint64_t ready = a.n_tiles;
+      if (!last) {
+        const uint64_t bases = packed * 64;
+        ready = bases > (uint64_t)k + 128 + T ? (bases - k - 128) / T : 0;
+        if (ready > a.n_tiles) ready = a.n_tiles;
+      }
+      if (ready > scanned) {
+        a.tile_begin = scanned;
+        const uint64_t nt = a.n_tiles;
+        a.n_tiles = ready;
+        launch_superkmer_scan(a, 0, s);
+        a.n_tiles = nt;
+        scanned = ready;
+      }
+    }
+    a.tile_begin = 0;
+    launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
+    CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaMemcpyAsync(&c->n_super, rec_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+    if (hs.rec_count != c->n_super) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record count != histogram total");
+    if (hs.rec_count > a.rec_cap) {  // the list overflowed: all bases are in place now, scan again
+      c->rec_cap_hint = hs.rec_count;
+      a.tile_counter = batched ? &sm->queues[0] : nullptr;
+      phase1(c->tune.sk_tile);
+    }
+  } else if (tune_now && c->opts.sk_tile == 0) {  // autotuner: time each tile, keep the fastest
     double best = 1e30;
     for (uint32_t t : TUNE_TILES) {
       CF1_CUDA(cudaEventRecord(c->ev[10], s));
@@ -206,8 +297,10 @@ void run_impl(cf1gpu_ctx *c) {
       }
     }
     c->tune.sk_tile = tuned.sk_tile;
+    phase1(c->tune.sk_tile);
+  } else {
+    phase1(c->tune.sk_tile);
   }
-  phase1(c->tune.sk_tile);
   c->n_occ = hs.n_kmers;
   c->n_bins_eff = hs.n_bins_eff;
   CF1_CUDA(cudaEventRecord(c->ev[1], s));
@@ -352,9 +445,47 @@ void run_impl(cf1gpu_ctx *c) {
   ca.err = &sm->err;
   ca.cas_retries = &sm->cas_retries;
   CF1_CUDA(cudaEventRecord(c->ev[5], s));
-  launch_classify<KeyT>(ca, pctas, s);
-  CF1_CUDA(cudaEventRecord(c->ev[6], s));
-  if (sideset) launch_sideset_pack(sides, nwords, states, s);
+  if (io && io->host_cap >= nwords && nwords) {
+    // Staged: bins in STREAM_STAGES groups of about equal record counts; the
+    // words whose slots all belong to finished bins go back while the next
+    // group classifies.
+    std::vector<uint64_t> hro(B + 1), hdo(B + 1);
+    CF1_CUDA(cudaMemcpyAsync(hro.data(), rec_off, (B + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaMemcpyAsync(hdo.data(), dist_off, (B + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+    uint32_t b0 = 0;
+    uint64_t w_done = 0;
+    for (int st = 0; st < STREAM_STAGES && b0 < B; st++) {
+      uint32_t b1 = B;
+      if (st + 1 < STREAM_STAGES) {
+        const uint64_t target = hro[B] * (uint64_t)(st + 1) / STREAM_STAGES;
+        b1 = b0 + 1;
+        while (b1 < B && hro[b1] < target) b1++;
+      }
+      ClassifyArgs<KeyT> cs = ca;
+      cs.records = records + hro[b0];
+      cs.n_rec = hro[b1] - hro[b0];
+      if (batched) CF1_CUDA(cudaMemsetAsync(ca.queue, 0, sizeof(uint32_t), s));
+      launch_classify<KeyT>(cs, pctas, s);
+      const uint64_t w_fin = b1 == B ? nwords : hdo[b1] / 12;
+      if (w_fin > w_done) {
+        if (sideset) launch_sideset_pack(sides, w_done, w_fin, states, s);
+        CF1_CUDA(cudaEventRecord(c->stage_ev[st], s));
+        CF1_CUDA(cudaStreamWaitEvent(c->copy_stream, c->stage_ev[st], 0));
+        CF1_CUDA(cudaMemcpyAsync(io->host_words + w_done, states + w_done, (w_fin - w_done) * sizeof(uint64_t),
+                                 cudaMemcpyDeviceToHost, c->copy_stream));
+        w_done = w_fin;
+      }
+      b0 = b1;
+    }
+    CF1_CUDA(cudaEventRecord(c->ev[6], s));
+    CF1_CUDA(cudaStreamSynchronize(c->copy_stream));
+    io->words_done = true;
+  } else {
+    launch_classify<KeyT>(ca, pctas, s);
+    CF1_CUDA(cudaEventRecord(c->ev[6], s));
+    if (sideset) launch_sideset_pack(sides, 0, nwords, states, s);
+  }
   CF1_CUDA(cudaEventRecord(c->ev[7], s));
   CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaStreamSynchronize(s));
@@ -430,21 +561,6 @@ void query_impl(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots) 
   CF1_CUDA(cudaStreamSynchronize(s));
 }
 
-// Direct intake of records given in page-locked host memory: one DMA of the
-// caller's bytes into a device buffer, then tiles of it are moved to their
-// places in the concatenation, a placeholder after each record.
-struct IntakeTile {
-  uint64_t src, dst;
-  uint32_t len, last;  // last: the tile ends its record
-};
-constexpr uint32_t INTAKE_TILE = 1u << 16;
-
-__global__ void intake_kernel(const uint8_t *raw, const IntakeTile *tiles, uint8_t *out) {
-  const IntakeTile t = tiles[blockIdx.x];
-  for (uint32_t i = threadIdx.x; i < t.len; i += blockDim.x) out[t.dst + i] = raw[t.src + i];
-  if (t.last && threadIdx.x == 0) out[t.dst + t.len] = 'N';
-}
-
 bool page_locked(const void *p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -508,6 +624,87 @@ void run_resident(cf1gpu_ctx *c) {
   if (c->wide) run_impl<Key2>(c);
   else run_impl<uint64_t>(c);
   c->ran = true;
+}
+
+size_t run_streamed(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, size_t n, uint64_t *words, size_t cap) {
+  // the input of cf1gpu_reset_input + cf1gpu_add_records, without staging
+  c->L = 0;
+  c->dev_valid = 0;
+  c->ms_intake = 0;
+  c->n_records = 0;
+  c->n_bases = 0;
+  c->short_seqs.clear();
+  c->uploaded = false;
+  c->ran = false;
+  std::vector<uint64_t> dst(n + 1);
+  uint64_t pos = 0;
+  for (size_t i = 0; i < n; i++) {
+    const uint64_t len = off[i + 1] - off[i];
+    dst[i] = pos;
+    c->n_records++;
+    c->n_bases += len;
+    if (len < (uint64_t)c->k) {
+      if (c->opts.track_short_seqs) c->short_seqs.emplace_back(std::string(), len);
+      dst[i] = ~0ull;
+      continue;
+    }
+    pos += len + 1;
+  }
+  cudaStream_t s = c->stream, cs = c->copy_stream;
+  StreamIO io;
+  const uint64_t first = n ? off[0] : 0, raw = n ? off[n] - first : 0;
+  for (size_t i = 0; i < n; i++) {
+    if (dst[i] == ~0ull) continue;
+    const uint64_t len = off[i + 1] - off[i];
+    for (uint64_t t = 0; t < len; t += INTAKE_TILE) {
+      const uint64_t m = std::min<uint64_t>(INTAKE_TILE, len - t);
+      io.htiles.push_back(IntakeTile{off[i] - first + t, dst[i] + t, (uint32_t)m, t + m == len ? 1u : 0u});
+    }
+  }
+  c->d_ascii.reserve_keep(pos + 16, 0, s);
+  uint8_t *r = c->d_raw.get<uint8_t>(raw + 1);
+  IntakeTile *dt = c->d_intake.get<IntakeTile>(io.htiles.size() + 1);
+  if (!io.htiles.empty())
+    CF1_CUDA(cudaMemcpyAsync(dt, io.htiles.data(), io.htiles.size() * sizeof(IntakeTile), cudaMemcpyHostToDevice, s));
+  CF1_CUDA(cudaStreamSynchronize(s));  // buffers in place before the copy stream writes them
+  io.raw = r;
+  io.tiles = dt;
+  io.host_words = words;
+  io.host_cap = cap;
+  // the record bytes in about 16 chunks (1 MB to 256 MB each) on the copy stream
+  const uint64_t CHUNK = std::max<uint64_t>(1ull << 20, std::min<uint64_t>(256ull << 20, ceil_div(raw, 16)));
+  const size_t nch = raw ? (size_t)ceil_div(raw, CHUNK) : 1;
+  io.chunk_ev.resize(nch);
+  io.chunk_end.resize(nch);
+  for (auto &e : io.chunk_ev) CF1_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  struct EvGuard {
+    std::vector<cudaEvent_t> &v;
+    ~EvGuard() {
+      for (auto e : v) cudaEventDestroy(e);
+    }
+  } guard_ev{io.chunk_ev};
+  CF1_CUDA(cudaEventRecord(c->ev[8], cs));
+  for (size_t ch = 0; ch < nch; ch++) {
+    const uint64_t b = ch * CHUNK, e = std::min(raw, b + CHUNK);
+    if (e > b) CF1_CUDA(cudaMemcpyAsync(r + b, seqs + first + b, e - b, cudaMemcpyHostToDevice, cs));
+    CF1_CUDA(cudaEventRecord(io.chunk_ev[ch], cs));
+    io.chunk_end[ch] = e;
+  }
+  CF1_CUDA(cudaEventRecord(c->ev[9], cs));
+  c->L = pos;
+  c->dev_valid = pos;
+  c->uploaded = true;
+  if (c->wide) run_impl<Key2>(c, &io);
+  else run_impl<uint64_t>(c, &io);
+  c->ran = true;
+  c->stats.ms_h2d = elapsed(c->ev[8], c->ev[9]);
+  const uint64_t nw = ceil_div(c->n_distinct, 12);
+  if (!io.words_done && nw) {  // staged copy-back skipped (no buffer or too small)
+    if (cap < nw) throw Error(CF1GPU_ERR_INVALID_ARG, "state word buffer too small: need " + std::to_string(nw));
+    CF1_CUDA(cudaMemcpyAsync(words, c->d_states.p, nw * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+  }
+  return nw;
 }
 
 void upload(cf1gpu_ctx *c) {

@@ -11,6 +11,7 @@ void add_records(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, size_t
 void add_fasta(cf1gpu_ctx *c, const char *path);
 void upload(cf1gpu_ctx *c);
 void run_resident(cf1gpu_ctx *c);
+size_t run_streamed(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, size_t n, uint64_t *words, size_t cap);
 void dump_states(cf1gpu_ctx *c, uint64_t *keys, uint8_t *states);
 void verify_bijection(cf1gpu_ctx *c);
 void query(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots);

@@ -149,6 +149,18 @@ int cf1gpu_run_resident(cf1gpu_ctx *ctx);
 /* cf1gpu_upload + cf1gpu_run_resident: pipeline.rs:76-105 in one call. */
 int cf1gpu_run_phases_1_4(cf1gpu_ctx *ctx);
 
+/* cf1gpu_reset_input + cf1gpu_add_records + cf1gpu_run_phases_1_4 +
+ * cf1gpu_copy_states in one call, with the copies overlapped: the record
+ * bytes go to the device in chunks while phase 1 scans the part already
+ * there, and phase 4 runs in stages of whole bins while the state words of
+ * finished stages come back.  Give seqs and state_words in page-locked host
+ * memory (cudaHostAlloc / cudaHostRegister) for the overlap; pageable buffers
+ * work, with the copies in series.  words_cap is state_words' size in words;
+ * *n_words receives ceil(total_kmers / 12).  A buffer too small is an error
+ * after the run (the results stay on the device for cf1gpu_copy_states). */
+int cf1gpu_run_streamed(cf1gpu_ctx *ctx, const uint8_t *seqs, const uint64_t *offsets, size_t n_records,
+                        uint64_t *state_words, size_t words_cap, size_t *n_words);
+
 int cf1gpu_get_stats(const cf1gpu_ctx *ctx, cf1gpu_stats *out);
 
 /* Mphf::total_kmers (src/mphf.rs:278-280). */

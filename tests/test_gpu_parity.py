@@ -209,6 +209,52 @@ def test_autotuner_cache(mode, batched):
         g2.close()
 
 
+@pytest.mark.parametrize("mode,batched,k,pinned", [("bbhash", False, 31, True), ("learned", True, 31, True),
+                                                    ("bbhash", False, 63, False), ("bbhash", True, 21, True)])
+def test_streamed_run_matches_staged(mode, batched, k, pinned):
+    # several 1 MB input chunks (5 Mbp) and eight phase-4 stages; the words
+    # equal those of the usual calls, and a second streamed run reuses the
+    # context
+    x = cg.SynthInput(1)
+    ref = gpu_run(x.seq, x.offsets, k, mode=mode, batched=batched, num_bins=64)
+    want = ref.states().copy()
+    ref.close()
+    g = cg.Cf1Gpu(k=k, mode=mode, batched=batched, num_bins=64)
+    seq = x.seq
+    keep = []
+    if pinned:
+        t, seq = _pinned_copy(np.asarray(x.seq, np.uint8))
+        keep.append(t)
+    for _ in range(2):
+        out = None
+        if pinned:
+            t, out = _pinned_copy(np.zeros(len(want) + 3, np.uint64))
+            keep.append(t)
+        w = g.run_streamed(seq, x.offsets, out)
+        assert np.array_equal(w, want)
+    s = g.stats()
+    assert s["ms_h2d"] > 0 and s["n_distinct"] == g.total_kmers()
+    g.close()
+
+
+def test_streamed_run_small_inputs_and_short_buffer():
+    recs = random_records(2718, 31, n_records=50, max_len=4000)
+    seq, off = o.concat_records(recs)
+    g, ref = assert_parity(seq, off, 31, num_bins=8, track_short_seqs=True)
+    want = g.states().copy()
+    shorts = g.short_seqs()
+    g.close()
+    g = cg.Cf1Gpu(k=31, num_bins=8, track_short_seqs=True)
+    assert np.array_equal(g.run_streamed(seq, off), want)
+    assert [n for _, n in g.short_seqs()] == [n for _, n in shorts]
+    with pytest.raises(cg.Cf1Error):
+        g.run_streamed(seq, off, np.zeros(1, np.uint64))  # too small: an error after the run
+    assert np.array_equal(g.states(), want)  # the results stay on the device
+    keys, st = sort_by_key(*g.dump_states())
+    assert np.array_equal(keys, ref.keys) and np.array_equal(st, ref.states)
+    g.close()
+
+
 def _read_bin_records(data: bytes):
     """Super k-mers of a bin file (the reader of src/superkmer.rs:283-298)."""
     out, i = [], 0
