@@ -221,41 +221,51 @@ void BBHashBuild<KeyT>::reserve_entries(uint64_t words, uint64_t keep, cudaStrea
 }
 
 template <class KeyT>
-void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_t nb, const uint32_t *sel,
-                              cudaStream_t s, KeyT *ws0, KeyT *ws1, uint64_t ws_cap) {
+void BBHashBuild<KeyT>::begin(uint32_t nb, cudaStream_t s) {
   clear();
   nbins = nb;
-  std::vector<uint64_t> hoff(nbins + 1);
-  CF1_CUDA(cudaMemcpyAsync(hoff.data(), seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-  CF1_CUDA(cudaStreamSynchronize(s));
-  for (uint32_t b = 0; b < nbins; b++)  // local slots are 32-bit
-    if (hoff[b + 1] - hoff[b] >= (1ull << 32))
-      throw Error(CF1GPU_ERR_INVALID_ARG, "BBHash: a bin holds 2^32 or more distinct keys; use more bins");
-  const uint64_t n_all = hoff[nbins];
   uint64_t *base = base_.get<uint64_t>(nbins);
   CF1_CUDA(cudaMemsetAsync(base, 0, nbins * sizeof(uint64_t), s));
   BBMeta *meta = meta_.get<BBMeta>((size_t)BB_MAX_LEVELS * nbins);
   CF1_CUDA(cudaMemsetAsync(meta, 0, (size_t)BB_MAX_LEVELS * nbins * sizeof(BBMeta), s));
-  // Keys of bin b at every level sit at [seg_off[b], seg_off[b] + cnt[b]) of
-  // the level's key array: the distinct keys at level 0, then the two
-  // workspaces in turn (the caller's, when big enough).
-  uint64_t *cnt[2] = {cnt_[0].get<uint64_t>(nbins), cnt_[1].get<uint64_t>(nbins)};
-  uint64_t *wcnt = wcnt_.get<uint64_t>(nbins + 1);
-  uint64_t *woff = woff_.get<uint64_t>(nbins + 1);
-  uint32_t *tile_off = tile_off_.get<uint32_t>(nbins + 1);
-  unsigned long long *tot = reinterpret_cast<unsigned long long *>(tot_.get<uint64_t>(2));
-  KeyT *r[2];
-  r[0] = (ws0 && ws_cap >= n_all + 1) ? ws0 : rem_[0].get<KeyT>(n_all + 1);
-  r[1] = (ws1 && ws_cap >= n_all + 1) ? ws1 : rem_[1].get<KeyT>(n_all + 1);
-  bb_init_counts_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(seg_off, sel, nbins, cnt[0]);
+  cnt_[0].get<uint64_t>(nbins);
+  cnt_[1].get<uint64_t>(nbins);
+  wcnt_.get<uint64_t>(nbins + 1);
+  woff_.get<uint64_t>(nbins + 1);
+  tile_off_.get<uint32_t>(nbins + 1);
+  tot_.get<uint64_t>(2);
+}
+
+// Ranks and metadata of a level whose cleaned bits are in place: AR =
+// entries [total_words, total_words + nw), woff = the bins' level-relative
+// block offsets.
+template <class KeyT>
+void BBHashBuild<KeyT>::finish_level(uint32_t l, const uint64_t *woff, uint64_t nw, cudaStream_t s) {
+  ulonglong2 *Al = ar_.as<ulonglong2>() + total_words;
+  uint64_t *Rl = rtmp_.get<uint64_t>(nw + 1);
+  uint32_t *pc = pc_.get<uint32_t>(nw);
+  bb_clean_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, pc, nw);
   CF1_LAUNCH_CHECK();
-  // room for the usual level sizes (gamma0 bits per key, then ~12% and
-  // fewer keys per level) so that the entry array rarely grows in mid-build
-  reserve_entries((BB_GAMMA0 * n_all / 64 + nbins) * 3 / 2 + 64 * nbins + 64, 0, s);
-  const KeyT *rem = keys;
-  uint32_t l = 0;
+  exclusive_scan_u32(pc, Rl, nw, scan_tmp_, s);
+  bb_rank_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, Rl, nw);
+  CF1_LAUNCH_CHECK();
+  bb_meta_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(woff, Rl, total_words, base_.as<uint64_t>(),
+                                                                meta_.as<BBMeta>() + (size_t)l * nbins, nbins);
+  CF1_LAUNCH_CHECK();
+}
+
+// Levels l, l+1, ... until no key is left.  Level l's keys: bin b's are
+// rem[start[b], start[b] + cnt_[l & 1][b]); each level writes the keys it
+// does not place to r0 / r1 in turn at the same offsets.
+template <class KeyT>
+void BBHashBuild<KeyT>::run_levels(uint32_t l, const KeyT *rem, const uint64_t *start, KeyT *r0, KeyT *r1,
+                                   cudaStream_t s) {
+  KeyT *r[2] = {r0, r1};
+  uint64_t *wcnt = wcnt_.as<uint64_t>(), *woff = woff_.as<uint64_t>();
+  uint32_t *tile_off = tile_off_.as<uint32_t>();
+  unsigned long long *tot = reinterpret_cast<unsigned long long *>(tot_.as<uint64_t>());
   for (;; l++) {
-    uint64_t *cur = cnt[l & 1], *nxt_cnt = cnt[(l + 1) & 1];
+    uint64_t *cur = cnt_[l & 1].as<uint64_t>(), *nxt_cnt = cnt_[(l + 1) & 1].as<uint64_t>();
     CF1_CUDA(cudaMemsetAsync(tot, 0, 2 * sizeof(unsigned long long), s));
     bb_sizes_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(cur, nbins, l ? BB_GAMMA : BB_GAMMA0, wcnt, tot);
     CF1_LAUNCH_CHECK();
@@ -270,24 +280,15 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
     nwords.push_back(nw);
     level_off.push_back(total_words);
     ulonglong2 *Al = ar_.as<ulonglong2>() + total_words;
-    uint64_t *Rl = rtmp_.get<uint64_t>(nw + 1);
-    uint32_t *pc = pc_.get<uint32_t>(nw);
     CF1_CUDA(cudaMemsetAsync(Al, 0, nw * sizeof(ulonglong2), s));
     uint32_t ub = (uint32_t)(ceil_div(remaining, BB_TILE) + nbins);
     segment_tiles_counts(cur, nbins, BB_TILE, tile_off, s);
-    bb_mark_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, seg_off, cur, tile_off, nbins, woff, l, Al);
+    bb_mark_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, start, cur, tile_off, nbins, woff, l, Al);
     CF1_LAUNCH_CHECK();
-    bb_clean_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, pc, nw);
-    CF1_LAUNCH_CHECK();
-    exclusive_scan_u32(pc, Rl, nw, scan_tmp_, s);
-    bb_rank_kernel<<<(unsigned)ceil_div(nw, 256), 256, 0, s>>>(Al, Rl, nw);
-    CF1_LAUNCH_CHECK();
-    bb_meta_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(woff, Rl, total_words, base, meta + (size_t)l * nbins,
-                                                                  nbins);
-    CF1_LAUNCH_CHECK();
+    finish_level(l, woff, nw, s);
     KeyT *out = r[l & 1];
     CF1_CUDA(cudaMemsetAsync(nxt_cnt, 0, nbins * sizeof(uint64_t), s));
-    bb_filter_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, seg_off, cur, tile_off, nbins, woff, l, Al,
+    bb_filter_kernel<KeyT><<<ub, BB_BLOCK, 0, s>>>(rem, start, cur, tile_off, nbins, woff, l, Al,
                                                    reinterpret_cast<unsigned long long *>(nxt_cnt), out);
     CF1_LAUNCH_CHECK();
     total_words += nw;
@@ -296,6 +297,51 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
   levels = l;
   bytes = total_words * sizeof(ulonglong2) + (size_t)levels * nbins * sizeof(BBMeta);
   CF1_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class KeyT>
+void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_t nb, const uint32_t *sel,
+                              cudaStream_t s, KeyT *ws0, KeyT *ws1, uint64_t ws_cap) {
+  begin(nb, s);
+  std::vector<uint64_t> hoff(nbins + 1);
+  CF1_CUDA(cudaMemcpyAsync(hoff.data(), seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  for (uint32_t b = 0; b < nbins; b++)  // local slots are 32-bit
+    if (hoff[b + 1] - hoff[b] >= (1ull << 32))
+      throw Error(CF1GPU_ERR_INVALID_ARG, "BBHash: a bin holds 2^32 or more distinct keys; use more bins");
+  const uint64_t n_all = hoff[nbins];
+  // Keys of bin b at every level sit at [seg_off[b], seg_off[b] + cnt[b]) of
+  // the level's key array: the distinct keys at level 0, then the two
+  // workspaces in turn (the caller's, when big enough).
+  KeyT *r0 = (ws0 && ws_cap >= n_all + 1) ? ws0 : rem_[0].get<KeyT>(n_all + 1);
+  KeyT *r1 = (ws1 && ws_cap >= n_all + 1) ? ws1 : rem_[1].get<KeyT>(n_all + 1);
+  bb_init_counts_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(seg_off, sel, nbins, cnt_[0].as<uint64_t>());
+  CF1_LAUNCH_CHECK();
+  // room for the usual level sizes (gamma0 bits per key, then ~12% and
+  // fewer keys per level) so that the entry array rarely grows in mid-build
+  reserve_entries((BB_GAMMA0 * n_all / 64 + nbins) * 3 / 2 + 64 * nbins + 64, 0, s);
+  run_levels(0, keys, seg_off, r0, r1, s);
+}
+
+template <class KeyT>
+ulonglong2 *BBHashBuild<KeyT>::prepare_level0(uint64_t words, cudaStream_t s) {
+  reserve_entries(words + words / 2 + 64 * 1024, 0, s);
+  return ar_.as<ulonglong2>();
+}
+
+template <class KeyT>
+void BBHashBuild<KeyT>::build_from_level0(uint32_t nb, const uint64_t *woff0, uint64_t words0, const KeyT *surv,
+                                          const uint64_t *surv_off, const uint64_t *surv_cnt, uint64_t surv_total,
+                                          cudaStream_t s, KeyT *ws0, KeyT *ws1, uint64_t ws_cap) {
+  begin(nb, s);
+  nwords.push_back(words0);
+  level_off.push_back(0);
+  finish_level(0, woff0, words0, s);
+  total_words = words0;
+  CF1_CUDA(cudaMemcpyAsync(cnt_[1].as<uint64_t>(), surv_cnt, nbins * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+  KeyT *r0 = (ws0 && ws_cap >= surv_total + 1) ? ws0 : rem_[0].get<KeyT>(surv_total + 1);
+  KeyT *r1 = (ws1 && ws_cap >= surv_total + 1) ? ws1 : rem_[1].get<KeyT>(surv_total + 1);
+  run_levels(1, surv, surv_off, r1, r0, s);  // level 1 writes r[1 & 1] = r0
 }
 
 template <class KeyT>

@@ -22,6 +22,16 @@ struct BBHashBuild {
   // still unplaced between levels; without them the builder allocates.
   void build(const KeyT *keys, const uint64_t *seg_off, uint32_t nbins, const uint32_t *sel, cudaStream_t s,
              KeyT *ws0 = nullptr, KeyT *ws1 = nullptr, uint64_t ws_cap = 0);
+  // Level 0 built elsewhere (the unsorted phase-3 dedup, one exclusive slice
+  // per sub-bucket): prepare_level0 gives the entry array to fill with level
+  // 0's cleaned bit words ({bits, 0}); build_from_level0 ranks it and builds
+  // the later levels over the keys level 0 left (bin b's at
+  // surv[surv_off[b] + [0, surv_cnt[b])]).  woff0: the bins' block offsets
+  // [nbins + 1] of level 0 (words0 words in all).
+  ulonglong2 *prepare_level0(uint64_t words, cudaStream_t s);
+  void build_from_level0(uint32_t nbins, const uint64_t *woff0, uint64_t words0, const KeyT *surv,
+                         const uint64_t *surv_off, const uint64_t *surv_cnt, uint64_t surv_total, cudaStream_t s,
+                         KeyT *ws0 = nullptr, KeyT *ws1 = nullptr, uint64_t ws_cap = 0);
   BBView view() const;
   void clear();
   uint64_t level_words(uint32_t l) const;
@@ -32,6 +42,9 @@ struct BBHashBuild {
  private:
   // Grows the entry array to hold `words` entries, keeping the first `keep`.
   void reserve_entries(uint64_t words, uint64_t keep, cudaStream_t s);
+  void begin(uint32_t nbins, cudaStream_t s);
+  void finish_level(uint32_t l, const uint64_t *woff, uint64_t nw, cudaStream_t s);
+  void run_levels(uint32_t l, const KeyT *rem, const uint64_t *start, KeyT *r0, KeyT *r1, cudaStream_t s);
 
   // The entry array and the level buffers are kept across builds and grown on
   // demand, so a rebuild allocates nothing once sizes settle.

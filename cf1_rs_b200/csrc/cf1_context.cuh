@@ -72,7 +72,7 @@ struct cf1gpu_ctx {
   bool ran = false;
 
   // device buffers
-  cf1::DevBuf d_binfile, d_binimg, d_raw, d_intake, d_shard, d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
+  cf1::DevBuf d_l0, d_l0surv, d_binfile, d_binimg, d_raw, d_intake, d_shard, d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
       d_keys, d_dist, d_dist_off, d_states, d_scan, d_seen, d_qin, d_qout, d_queue;
   uint64_t rec_cap_hint = 0;  // phase-1 record list size of the last run
   // autotuner: cache file ("" = off), the key the current tuning is for

@@ -14,6 +14,7 @@
 // the caller fall back to the LSD path (cf1_phase3_sort.cu) for the run.
 #include "cf1_device_util.cuh"
 #include "cf1_internal.cuh"
+#include "cf1_mphf.cuh"
 #include "cf1_msdsort.cuh"
 
 namespace cf1 {
@@ -365,6 +366,72 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
       sh.sm);
 }
 
+// Level-0 slice of sub-bucket j (bin j >> P, slice j mod 2^P) over its n
+// distinct keys (see Level0Out); set/col: L0_SW_MAX words of shared memory
+// each.  All threads call it.
+constexpr uint32_t L0_SW_MAX = 768;
+CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const Level0Out &o,
+                    unsigned long long *set, unsigned long long *col, uint32_t *sm, unsigned long long *s_base) {
+  const unsigned tid = threadIdx.x;
+  const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
+  const uint64_t W = o.woff[bin + 1] - o.woff[bin];
+  const uint32_t sw = (uint32_t)(W >> P);
+  if (n == 0) return;
+  if (sw > L0_SW_MAX || sw == 0) {
+    if (tid == 0) atomicOr(o.err, 1u);
+    return;
+  }
+  const uint64_t first = o.woff[bin] + (uint64_t)sub * sw;  // the slice's first entry
+  for (uint32_t w = tid; w < sw; w += CS_BLOCK) set[w] = col[w] = 0;
+  __syncthreads();
+  for (uint32_t i = tid; i < n; i += CS_BLOCK) {
+    const uint64_t pos = bb_pos(keys[i], 0, (uint32_t)W);
+    const uint64_t wl = (pos >> 6) - (uint64_t)sub * sw;
+    if (wl >= sw) {  // not this slice's key: cannot happen with the shared hash
+      atomicOr(o.err, 1u);
+      continue;
+    }
+    const unsigned long long bit = 1ull << (pos & 63);
+    if (atomicOr(&set[wl], bit) & bit) atomicOr(&col[wl], bit);
+  }
+  __syncthreads();
+  for (uint32_t w = tid; w < sw; w += CS_BLOCK) {
+    const unsigned long long x = set[w] & ~col[w];
+    if (x) o.AR[first + w].x = x;
+  }
+  // the keys whose bit collided go on to level 1
+  uint32_t c = 0;
+  for (uint32_t i = tid; i < n; i += CS_BLOCK) {
+    const uint64_t pos = bb_pos(keys[i], 0, (uint32_t)W);
+    const uint64_t wl = (pos >> 6) - (uint64_t)sub * sw;
+    c += wl < sw && ((col[wl] >> (pos & 63)) & 1);
+  }
+  uint32_t tot;
+  uint32_t pre = block_exclusive_scan<CS_BLOCK>(c, sm, tot);
+  if (tid == 0) {
+    unsigned long long b = ~0ull;
+    if (tot) {
+      b = atomicAdd(&o.surv_cnt[bin], (unsigned long long)tot);
+      if (b + tot > o.surv_off[bin + 1] - o.surv_off[bin]) {
+        atomicOr(o.err, 1u);
+        b = ~0ull;
+      }
+    }
+    *s_base = b;
+  }
+  __syncthreads();
+  if (*s_base != ~0ull) {
+    uint64_t out = o.surv_off[bin] + *s_base + pre;
+    for (uint32_t i = tid; i < n; i += CS_BLOCK) {
+      const uint64_t key = keys[i];
+      const uint64_t pos = bb_pos(key, 0, (uint32_t)W);
+      const uint64_t wl = (pos >> 6) - (uint64_t)sub * sw;
+      if (wl < sw && ((col[wl] >> (pos & 63)) & 1)) o.surv[out++] = key;
+    }
+  }
+  __syncthreads();
+}
+
 // Sorted distinct keys of one sub-bucket T[a, a+n), written back at a
 // (SORTED = false: distinct keys in any order -- 64-bit keys then skip the
 // sort whenever the shared-memory set holds the sub-bucket).
@@ -377,8 +444,10 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
 template <class KeyT, bool SORTED>
 __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT *U, const uint64_t *sb_off,
                                                                   uint64_t nsub, int shift, int bits, uint32_t *cnt,
-                                                                  uint32_t *oversize) {
+                                                                  uint32_t *oversize, int P, Level0Out l0) {
   constexpr uint32_t CAP = cs_cap<KeyT, SORTED>();
+  constexpr bool L0 = !SORTED && KOps<KeyT>::WORDS == 1;
+  __shared__ unsigned long long s_l0base;
   extern __shared__ __align__(16) unsigned char cs_smem[];
   KeyT *S = reinterpret_cast<KeyT *>(cs_smem);                    // [CAP]
   uint32_t *hist = reinterpret_cast<uint32_t *>(S + CAP);         // [CS_BUCKETS]
@@ -409,6 +478,10 @@ __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT 
       distinct = true;
       if (!SORTED) {  // distinct keys are all that is needed
         if (tid == 0) cnt[j] = d;
+        if constexpr (L0) {
+          unsigned long long *h64 = reinterpret_cast<unsigned long long *>(hist);
+          if (l0.AR) l0_slice(reinterpret_cast<const uint64_t *>(T) + a, d, j, P, l0, h64, h64 + L0_SW_MAX, sm, &s_l0base);
+        }
         return;
       }
     }
@@ -416,6 +489,10 @@ __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT 
   if (m <= CAP) {
     uint32_t tot = cs_sort_unique_range<KeyT>(T + a, m, plain, S, sh, T + a, distinct);
     if (tid == 0) cnt[j] = tot;
+    if constexpr (L0) {
+      unsigned long long *h64 = reinterpret_cast<unsigned long long *>(hist);
+      if (l0.AR) l0_slice(reinterpret_cast<const uint64_t *>(T) + a, tot, j, P, l0, h64, h64 + L0_SW_MAX, sm, &s_l0base);
+    }
     return;
   }
   // local split on the next `bits` bits into U[a, a+n)
@@ -500,6 +577,11 @@ __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT 
     outc += cs_sort_unique_range<KeyT>(U + a + pstart[p0], len, dig, S, sh, T + a + outc, dd);
   }
   if (tid == 0) cnt[j] = outc;
+  if constexpr (L0) {
+    __syncthreads();
+    unsigned long long *h64 = reinterpret_cast<unsigned long long *>(hist);
+    if (l0.AR) l0_slice(reinterpret_cast<const uint64_t *>(T) + a, outc, j, P, l0, h64, h64 + L0_SW_MAX, sm, &s_l0base);
+  }
 }
 
 // One warp per sub-bucket: copy its distinct keys to the dense array.
@@ -592,7 +674,8 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted) {
 
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
-                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted) {
+                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted,
+                     const Level0Out *l0) {
   // passes on the top P bits: P1 then P2 (P2 may be 0) -- of the key, or of
   // its hash when only distinct keys are wanted (64-bit keys)
   const bool hashed = !sorted && KOps<KeyT>::WORDS == 1;
@@ -643,7 +726,9 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
   CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   KeyT *U = T == keys ? alt : keys;
   if (nsub) {
-    kern<<<(unsigned)nsub, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over);
+    Level0Out lo;
+    if (l0 && hashed) lo = *l0;
+    kern<<<(unsigned)nsub, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over, P, lo);
     CF1_LAUNCH_CHECK();
   }
   uint32_t h_over = 0;
@@ -664,7 +749,7 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
 #define CF1_INST(KT)                                                                                              \
   template int msd_prefix_bits<KT>(uint64_t, bool);                                                                     \
   template bool msd_sort_unique<KT>(KT *, KT *, uint64_t, const uint64_t *, uint32_t, int, int, KT *, uint64_t *, \
-                                    MsdScratch &, cudaStream_t, bool);
+                                    MsdScratch &, cudaStream_t, bool, const Level0Out *);
 CF1_INST(uint64_t)
 CF1_INST(Key2)
 #undef CF1_INST

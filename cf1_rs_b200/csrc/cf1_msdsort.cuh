@@ -21,8 +21,24 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted);
 // (nothing written) when a sub-bucket is larger than the shared-memory
 // capacity; keys are then clobbered and the caller re-expands and takes the
 // LSD path.
+// Level 0 of the BBHash form, built by the unsorted (64-bit) dedup: with the
+// sub-buckets split on the top P bits of key * KEY_SPREAD_MUL -- level 0's own
+// hash -- and every bin's level-0 block a multiple of 2^P words, sub-bucket
+// j of bin b owns words [j, j + 1) * (block / 2^P) of it alone, so its CTA
+// marks, clears and writes them with no atomics in global memory and lists
+// the keys it does not place.
+struct Level0Out {
+  ulonglong2 *AR = nullptr;                // level-0 entries (zeroed); nullptr: off
+  const uint64_t *woff = nullptr;          // [nbins + 1] block offsets
+  uint64_t *surv = nullptr;                // keys level 0 leaves: bin b's from surv_off[b]
+  const uint64_t *surv_off = nullptr;      // [nbins + 1]; bin b's room is surv_off[b+1] - surv_off[b]
+  unsigned long long *surv_cnt = nullptr;  // [nbins], zeroed
+  uint32_t *err = nullptr;                 // set when a slice or a bin's room is too small
+};
+
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
-                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted = true);
+                     KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted = true,
+                     const Level0Out *l0 = nullptr);
 
 }  // namespace cf1

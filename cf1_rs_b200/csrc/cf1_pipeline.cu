@@ -38,6 +38,7 @@ struct Small {
   unsigned long long rec_count;
   uint32_t err;
   uint32_t n_bins_eff;
+  uint32_t l0_err;  // the phase-3 dedup could not build BBHash level 0
   uint32_t queues[8];
 };
 
@@ -386,7 +387,40 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
     if (batched) CF1_CUDA(cudaMemsetAsync(&sm->queues[4], 0, sizeof(uint32_t), s));
   }
   int P = msd_width(c->tune.msd_delta);
-  bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist, dist_off, be.msd, s, sorted);
+  // BBHash form, 64-bit keys: the dedup builds BBHash level 0 on the way
+  // (Level0Out), 8 bits per k-mer occurrence of the bin rounded up to a
+  // multiple of the bin's 2^P slices; the keys it leaves go to a list with
+  // room for a quarter of the bin's occurrences.
+  const bool l0_fuse = !sorted && !c->wide && c->opts.mphf_mode == CF1GPU_MPHF_BBHASH && P >= 0;
+  Level0Out l0;
+  uint64_t l0_words = 0, l0_room = 0;
+  if (l0_fuse) {
+    std::vector<uint64_t> hw(B + 1, 0), hr(B + 1, 0);
+    const uint64_t slices = 1ull << P;
+    for (uint32_t b = 0; b < B; b++) {
+      const uint64_t occ = hseg[b + 1] - hseg[b];
+      const uint64_t wb = occ ? ceil_div(ceil_div(8 * occ, 64), slices) * slices : 0;
+      hw[b + 1] = hw[b] + wb;
+      hr[b + 1] = hr[b] + (occ ? occ / 4 + 64 : 0);
+    }
+    l0_words = hw[B];
+    l0_room = hr[B];
+    uint64_t *woff0 = c->d_l0.get<uint64_t>(3 * (size_t)(B + 1));
+    uint64_t *room_off = woff0 + (B + 1);
+    unsigned long long *scnt = reinterpret_cast<unsigned long long *>(room_off + (B + 1));
+    CF1_CUDA(cudaMemcpyAsync(woff0, hw.data(), (B + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    CF1_CUDA(cudaMemcpyAsync(room_off, hr.data(), (B + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    CF1_CUDA(cudaMemsetAsync(scnt, 0, B * sizeof(uint64_t), s));
+    l0.AR = be.bb.prepare_level0(l0_words, s);
+    CF1_CUDA(cudaMemsetAsync(l0.AR, 0, l0_words * sizeof(ulonglong2), s));
+    l0.woff = woff0;
+    l0.surv = c->d_l0surv.get<uint64_t>(l0_room + 1);
+    l0.surv_off = room_off;
+    l0.surv_cnt = scnt;
+    l0.err = &sm->l0_err;
+  }
+  bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist, dist_off, be.msd, s, sorted,
+                                              l0_fuse ? &l0 : nullptr);
   c->msd_bits = done ? P : -1;
   if (tune_now) {
     tuned.sk_tile = c->tune.sk_tile;
@@ -404,7 +438,10 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
     segmented_unique<KeyT>(keys, NO, seg, B, dist, dist_off, be.sort, s);
   }
   CF1_CUDA(cudaMemcpyAsync(&c->n_distinct, dist_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  uint32_t l0_err = 1;
+  if (l0_fuse) CF1_CUDA(cudaMemcpyAsync(&l0_err, &sm->l0_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaStreamSynchronize(s));
+  const bool l0_ready = l0_fuse && done && l0_err == 0;
   CF1_CUDA(cudaEventRecord(c->ev[3], s));
 
   // ---- phase 3b: MPHF
@@ -413,6 +450,9 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
   if (c->opts.mphf_mode == CF1GPU_MPHF_LEARNED) {
     be.li.build(dist, dist_off, B, k, c->learned, s);
     be.bb.build(dist, dist_off, B, be.li.fallback_sel(), s, keys, ws1, NO + 1);
+  } else if (l0_ready) {
+    be.bb.build_from_level0(B, l0.woff, l0_words, reinterpret_cast<const KeyT *>(l0.surv), l0.surv_off,
+                            reinterpret_cast<const uint64_t *>(l0.surv_cnt), l0_room, s, keys, ws1, NO + 1);
   } else {
     be.bb.build(dist, dist_off, B, nullptr, s, keys, ws1, NO + 1);
   }
