@@ -368,65 +368,67 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
 
 // Level-0 slice of sub-bucket j (bin j >> P, slice j mod 2^P) over its n
 // distinct keys (see Level0Out); set/col: L0_SW_MAX words of shared memory
-// each.  All threads call it.
+// each; lb: lb_cap u16 of shared memory for the keys' bits in the slice (a
+// slice has at most L0_SW_MAX * 64 < 2^16 bits).  All threads call it.
 constexpr uint32_t L0_SW_MAX = 768;
 CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const Level0Out &o,
-                    unsigned long long *set, unsigned long long *col, uint32_t *sm, unsigned long long *s_base) {
+                    unsigned long long *set, unsigned long long *col, uint16_t *lb, uint32_t lb_cap, uint32_t *sm,
+                    unsigned long long *s_base) {
   const unsigned tid = threadIdx.x;
   const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
   const uint64_t W = o.woff[bin + 1] - o.woff[bin];
   const uint32_t sw = (uint32_t)(W >> P);
-  if (n == 0) return;
-  if (sw > L0_SW_MAX || sw == 0) {
+  if (n == 0) {  // every slice writes all its entries (the array is not cleared first)
+    for (uint32_t w = tid; w < sw; w += CS_BLOCK)
+      o.AR[o.woff[bin] + (uint64_t)sub * sw + w] = make_ulonglong2(0ull, 0ull);
+    return;
+  }
+  if (sw > L0_SW_MAX || sw == 0 || n > lb_cap) {
     if (tid == 0) atomicOr(o.err, 1u);
     return;
   }
   const uint64_t first = o.woff[bin] + (uint64_t)sub * sw;  // the slice's first entry
+  const uint64_t lo_bit = (uint64_t)sub * sw * 64;
   for (uint32_t w = tid; w < sw; w += CS_BLOCK) set[w] = col[w] = 0;
   __syncthreads();
   for (uint32_t i = tid; i < n; i += CS_BLOCK) {
-    const uint64_t pos = bb_pos(keys[i], 0, (uint32_t)W);
-    const uint64_t wl = (pos >> 6) - (uint64_t)sub * sw;
-    if (wl >= sw) {  // not this slice's key: cannot happen with the shared hash
+    const uint64_t b = bb_pos(keys[i], 0, (uint32_t)W) - lo_bit;
+    if (b >= (uint64_t)sw * 64) {  // not this slice's key: cannot happen with the shared hash
       atomicOr(o.err, 1u);
+      lb[i] = 0xFFFF;
       continue;
     }
-    const unsigned long long bit = 1ull << (pos & 63);
-    if (atomicOr(&set[wl], bit) & bit) atomicOr(&col[wl], bit);
+    lb[i] = (uint16_t)b;
+    const unsigned long long bit = 1ull << (b & 63);
+    if (atomicOr(&set[b >> 6], bit) & bit) atomicOr(&col[b >> 6], bit);
   }
   __syncthreads();
-  for (uint32_t w = tid; w < sw; w += CS_BLOCK) {
-    const unsigned long long x = set[w] & ~col[w];
-    if (x) o.AR[first + w].x = x;
-  }
+  for (uint32_t w = tid; w < sw; w += CS_BLOCK) o.AR[first + w] = make_ulonglong2(set[w] & ~col[w], 0ull);
   // the keys whose bit collided go on to level 1
   uint32_t c = 0;
   for (uint32_t i = tid; i < n; i += CS_BLOCK) {
-    const uint64_t pos = bb_pos(keys[i], 0, (uint32_t)W);
-    const uint64_t wl = (pos >> 6) - (uint64_t)sub * sw;
-    c += wl < sw && ((col[wl] >> (pos & 63)) & 1);
+    const uint32_t b = lb[i];
+    c += b != 0xFFFF && ((col[b >> 6] >> (b & 63)) & 1);
   }
   uint32_t tot;
   uint32_t pre = block_exclusive_scan<CS_BLOCK>(c, sm, tot);
   if (tid == 0) {
-    unsigned long long b = ~0ull;
+    unsigned long long base = ~0ull;
     if (tot) {
-      b = atomicAdd(&o.surv_cnt[bin], (unsigned long long)tot);
-      if (b + tot > o.surv_off[bin + 1] - o.surv_off[bin]) {
+      base = atomicAdd(&o.surv_cnt[bin], (unsigned long long)tot);
+      if (base + tot > o.surv_off[bin + 1] - o.surv_off[bin]) {
         atomicOr(o.err, 1u);
-        b = ~0ull;
+        base = ~0ull;
       }
     }
-    *s_base = b;
+    *s_base = base;
   }
   __syncthreads();
   if (*s_base != ~0ull) {
     uint64_t out = o.surv_off[bin] + *s_base + pre;
     for (uint32_t i = tid; i < n; i += CS_BLOCK) {
-      const uint64_t key = keys[i];
-      const uint64_t pos = bb_pos(key, 0, (uint32_t)W);
-      const uint64_t wl = (pos >> 6) - (uint64_t)sub * sw;
-      if (wl < sw && ((col[wl] >> (pos & 63)) & 1)) o.surv[out++] = key;
+      const uint32_t b = lb[i];
+      if (b != 0xFFFF && ((col[b >> 6] >> (b & 63)) & 1)) o.surv[out++] = keys[i];
     }
   }
   __syncthreads();
@@ -442,7 +444,7 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
 // distinct keys are appended at T[a].  Only a single piece above CAP keys
 // makes the kernel report the sub-bucket as oversized.
 template <class KeyT, bool SORTED>
-__global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT *U, const uint64_t *sb_off,
+__global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kernel(KeyT *T, KeyT *U, const uint64_t *sb_off,
                                                                   uint64_t nsub, int shift, int bits, uint32_t *cnt,
                                                                   uint32_t *oversize, int P, Level0Out l0) {
   constexpr uint32_t CAP = cs_cap<KeyT, SORTED>();
@@ -461,126 +463,107 @@ __global__ void __launch_bounds__(CS_BLOCK) cs_sort_unique_kernel(KeyT *T, KeyT 
   if (j >= nsub) return;
   const uint64_t a = sb_off[j], n = sb_off[j + 1] - a;
   const unsigned tid = threadIdx.x;
-  if (n == 0) {
-    if (tid == 0) cnt[j] = 0;
-    return;
-  }
-  CsShared sh{hist, cur, sm, &s_big};
-  CsDigit plain{shift, bits, 0, 0, 0u};
-  uint32_t m = (uint32_t)n;
-  bool distinct = false;
-  // 64-bit keys: one copy of each key first.  Repeats put hundreds of copies
-  // of a k-mer in one bucket, where sorting copies would dominate the work.
-  if ((!SORTED || n > CS_DEDUP_MIN) && KOps<KeyT>::WORDS == 1) {
-    uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(T), a, n, reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
-    if (d != ~0u) {
-      m = d;
-      distinct = true;
-      if (!SORTED) {  // distinct keys are all that is needed
-        if (tid == 0) cnt[j] = d;
-        if constexpr (L0) {
-          unsigned long long *h64 = reinterpret_cast<unsigned long long *>(hist);
-          if (l0.AR) l0_slice(reinterpret_cast<const uint64_t *>(T) + a, d, j, P, l0, h64, h64 + L0_SW_MAX, sm, &s_l0base);
-        }
-        return;
+  // the sub-bucket's distinct keys end at T[a, a + result); ~0u: oversized
+  auto body = [&]() -> uint32_t {
+    if (n == 0) return 0;
+    CsShared sh{hist, cur, sm, &s_big};
+    CsDigit plain{shift, bits, 0, 0, 0u};
+    uint32_t m = (uint32_t)n;
+    bool distinct = false;
+    // 64-bit keys: one copy of each key first.  Repeats put hundreds of
+    // copies of a k-mer in one bucket, where sorting copies would dominate.
+    if ((!SORTED || n > CS_DEDUP_MIN) && KOps<KeyT>::WORDS == 1) {
+      uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(T), a, n, reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
+      if (d != ~0u) {
+        m = d;
+        distinct = true;
+        if (!SORTED) return d;  // distinct keys are all that is needed
       }
     }
-  }
-  if (m <= CAP) {
-    uint32_t tot = cs_sort_unique_range<KeyT>(T + a, m, plain, S, sh, T + a, distinct);
-    if (tid == 0) cnt[j] = tot;
-    if constexpr (L0) {
-      unsigned long long *h64 = reinterpret_cast<unsigned long long *>(hist);
-      if (l0.AR) l0_slice(reinterpret_cast<const uint64_t *>(T) + a, tot, j, P, l0, h64, h64 + L0_SW_MAX, sm, &s_l0base);
-    }
-    return;
-  }
-  // local split on the next `bits` bits into U[a, a+n)
-  const uint32_t npieces = 1u << bits, pmask = npieces - 1;
-  for (uint32_t i = tid; i <= CS_BUCKETS; i += CS_BLOCK) pstart[i] = 0;
-  __syncthreads();
-  for (uint64_t i = tid; i < n; i += CS_BLOCK) atomicAdd(&pstart[KOps<KeyT>::digit(T[a + i], shift, pmask)], 1u);
-  __syncthreads();
-  if (tid == 0) {
-    uint32_t run = 0;
-    for (uint32_t p = 0; p < npieces; p++) {
-      uint32_t v = pstart[p];
-      pstart[p] = run;
-      run += v;
-    }
-    pstart[npieces] = run;
-    // greedy runs of consecutive pieces up to CAP keys
-    int nc = 0, bad = 0;
-    uint32_t acc = 0;
-    cb[0] = 0;
-    for (uint32_t p = 0; p < npieces; p++) {
-      uint32_t sz = pstart[p + 1] - pstart[p];
-      if (sz > CAP) {  // a piece of its own, deduplicated before sorting (64-bit keys)
-        if (KOps<KeyT>::WORDS != 1) bad = 1;
-        if (acc > 0) cb[++nc] = (uint16_t)p;
-        cb[++nc] = (uint16_t)(p + 1);
-        acc = 0;
-        continue;
-      }
-      if (acc + sz > CAP && acc > 0) {
-        cb[++nc] = (uint16_t)p;
-        acc = 0;
-      }
-      acc += sz;
-    }
-    if (acc == 0) nc--;  // the loop already closed the last run
-    cb[++nc] = (uint16_t)npieces;
-    s_nchunks = nc;
-    s_bad = bad;
-  }
-  __syncthreads();
-  if (s_bad) {
-    if (tid == 0) {
-      cnt[j] = 0;
-      atomicOr(oversize, 1u);
-    }
-    return;
-  }
-  for (uint32_t p = tid; p < npieces; p += CS_BLOCK) cur[p] = pstart[p];
-  __syncthreads();
-  for (uint64_t i = tid; i < n; i += CS_BLOCK) {
-    KeyT key = T[a + i];
-    U[a + atomicAdd(&cur[KOps<KeyT>::digit(key, shift, pmask)], 1u)] = key;
-  }
-  __syncthreads();
-  uint32_t outc = 0;
-  for (int c = 0; c < s_nchunks; c++) {
-    uint32_t p0 = cb[c], p1 = cb[c + 1];
-    uint32_t span = p1 - p0;
-    int g = 0;
-    while ((1u << g) < span) g++;
-    int b2 = 10 - g;
-    if (b2 > shift) b2 = shift;
-    CsDigit dig{shift, bits, shift - b2, b2, p0};
-    uint32_t len = pstart[p1] - pstart[p0];
-    bool dd = false;
-    if (len > CS_DEDUP_MIN && KOps<KeyT>::WORDS == 1) {
-      uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(U), a + pstart[p0], len,
-                                 reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
-      if (d != ~0u) {  // (a failed pass leaves U untouched)
-        len = d;
-        dd = true;
-      }
-      if (len > CAP) {
-        if (tid == 0) {
-          cnt[j] = 0;
-          atomicOr(oversize, 1u);
-        }
-        return;
-      }
-    }
-    outc += cs_sort_unique_range<KeyT>(U + a + pstart[p0], len, dig, S, sh, T + a + outc, dd);
-  }
-  if (tid == 0) cnt[j] = outc;
-  if constexpr (L0) {
+    if (m <= CAP) return cs_sort_unique_range<KeyT>(T + a, m, plain, S, sh, T + a, distinct);
+    // local split on the next `bits` bits into U[a, a+n)
+    const uint32_t npieces = 1u << bits, pmask = npieces - 1;
+    for (uint32_t i = tid; i <= CS_BUCKETS; i += CS_BLOCK) pstart[i] = 0;
     __syncthreads();
-    unsigned long long *h64 = reinterpret_cast<unsigned long long *>(hist);
-    if (l0.AR) l0_slice(reinterpret_cast<const uint64_t *>(T) + a, outc, j, P, l0, h64, h64 + L0_SW_MAX, sm, &s_l0base);
+    for (uint64_t i = tid; i < n; i += CS_BLOCK) atomicAdd(&pstart[KOps<KeyT>::digit(T[a + i], shift, pmask)], 1u);
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t run = 0;
+      for (uint32_t p = 0; p < npieces; p++) {
+        uint32_t v = pstart[p];
+        pstart[p] = run;
+        run += v;
+      }
+      pstart[npieces] = run;
+      // greedy runs of consecutive pieces up to CAP keys
+      int nc = 0, bad = 0;
+      uint32_t acc = 0;
+      cb[0] = 0;
+      for (uint32_t p = 0; p < npieces; p++) {
+        uint32_t sz = pstart[p + 1] - pstart[p];
+        if (sz > CAP) {  // a piece of its own, deduplicated before sorting (64-bit keys)
+          if (KOps<KeyT>::WORDS != 1) bad = 1;
+          if (acc > 0) cb[++nc] = (uint16_t)p;
+          cb[++nc] = (uint16_t)(p + 1);
+          acc = 0;
+          continue;
+        }
+        if (acc + sz > CAP && acc > 0) {
+          cb[++nc] = (uint16_t)p;
+          acc = 0;
+        }
+        acc += sz;
+      }
+      if (acc == 0) nc--;  // the loop already closed the last run
+      cb[++nc] = (uint16_t)npieces;
+      s_nchunks = nc;
+      s_bad = bad;
+    }
+    __syncthreads();
+    if (s_bad) return ~0u;
+    for (uint32_t p = tid; p < npieces; p += CS_BLOCK) cur[p] = pstart[p];
+    __syncthreads();
+    for (uint64_t i = tid; i < n; i += CS_BLOCK) {
+      KeyT key = T[a + i];
+      U[a + atomicAdd(&cur[KOps<KeyT>::digit(key, shift, pmask)], 1u)] = key;
+    }
+    __syncthreads();
+    uint32_t outc = 0;
+    for (int c = 0; c < s_nchunks; c++) {
+      uint32_t p0 = cb[c], p1 = cb[c + 1];
+      uint32_t span = p1 - p0;
+      int g = 0;
+      while ((1u << g) < span) g++;
+      int b2 = 10 - g;
+      if (b2 > shift) b2 = shift;
+      CsDigit dig{shift, bits, shift - b2, b2, p0};
+      uint32_t len = pstart[p1] - pstart[p0];
+      bool dd = false;
+      if (len > CS_DEDUP_MIN && KOps<KeyT>::WORDS == 1) {
+        uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(U), a + pstart[p0], len,
+                                   reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
+        if (d != ~0u) {  // (a failed pass leaves U untouched)
+          len = d;
+          dd = true;
+        }
+        if (len > CAP) return ~0u;
+      }
+      outc += cs_sort_unique_range<KeyT>(U + a + pstart[p0], len, dig, S, sh, T + a + outc, dd);
+    }
+    return outc;
+  };
+  const uint32_t res = body();
+  if (tid == 0) {
+    cnt[j] = res == ~0u ? 0 : res;
+    if (res == ~0u) atomicOr(oversize, 1u);
+  }
+  if constexpr (L0) {
+    if (l0.AR && res != ~0u) {
+      __syncthreads();
+      unsigned long long *h64 = reinterpret_cast<unsigned long long *>(hist);
+      l0_slice(reinterpret_cast<const uint64_t *>(T) + a, res, j, P, l0, h64, h64 + L0_SW_MAX,
+               reinterpret_cast<uint16_t *>(S), CAP * sizeof(KeyT) / 2, sm, &s_l0base);
+    }
   }
 }
 

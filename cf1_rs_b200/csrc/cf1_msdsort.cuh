@@ -28,7 +28,7 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted);
 // marks, clears and writes them with no atomics in global memory and lists
 // the keys it does not place.
 struct Level0Out {
-  ulonglong2 *AR = nullptr;                // level-0 entries (zeroed); nullptr: off
+  ulonglong2 *AR = nullptr;                // level-0 entries (each slice writes all of its); nullptr: off
   const uint64_t *woff = nullptr;          // [nbins + 1] block offsets
   uint64_t *surv = nullptr;                // keys level 0 leaves: bin b's from surv_off[b]
   const uint64_t *surv_off = nullptr;      // [nbins + 1]; bin b's room is surv_off[b+1] - surv_off[b]

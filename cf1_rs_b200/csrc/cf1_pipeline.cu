@@ -411,8 +411,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
     CF1_CUDA(cudaMemcpyAsync(woff0, hw.data(), (B + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
     CF1_CUDA(cudaMemcpyAsync(room_off, hr.data(), (B + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
     CF1_CUDA(cudaMemsetAsync(scnt, 0, B * sizeof(uint64_t), s));
-    l0.AR = be.bb.prepare_level0(l0_words, s);
-    CF1_CUDA(cudaMemsetAsync(l0.AR, 0, l0_words * sizeof(ulonglong2), s));
+    l0.AR = be.bb.prepare_level0(l0_words, s);  // every slice writes all of its entries
     l0.woff = woff0;
     l0.surv = c->d_l0surv.get<uint64_t>(l0_room + 1);
     l0.surv_off = room_off;
