@@ -290,6 +290,28 @@ CF1_HD uint32_t sideset_of_state(uint32_t c) {
   decode_sides(c, f, b);
   return side_code(f) | (side_code(b) << 4);
 }
+// sideset_of_state of all 32 states, 8 bytes to a word, for a lookup by
+// shift: (SIDESET_TABLE[c >> 3] >> 8 (c & 7)) & 0xFF.
+constexpr uint32_t sideset_ce(uint32_t c) {
+  // decode_sides / side_code in constant-expression form
+  uint32_t f = SIDE_NONE, b = SIDE_NONE;
+  if (c == 3) f = b = SIDE_M;
+  else if (c >= 4 && c < 8) f = SIDE_M, b = c & 3;
+  else if (c >= 8 && c < 12) f = c & 3, b = SIDE_M;
+  else if (c >= 12) f = (c >> 2) & 3, b = c & 3;
+  auto code = [](uint32_t side) -> uint32_t { return side == SIDE_M ? 0xFu : side == SIDE_NONE ? 0u : (0x9653u >> (4 * side)) & 0xFu; };
+  return code(f) | (code(b) << 4);
+}
+constexpr uint64_t sideset_word_ce(uint32_t w) {
+  uint64_t x = 0;
+  for (uint32_t i = 0; i < 8; i++) x |= (uint64_t)sideset_ce(8 * w + i) << (8 * i);
+  return x;
+}
+CF1_HD uint32_t sideset_lookup(uint32_t c) {
+  constexpr uint64_t t0 = sideset_word_ce(0), t1 = sideset_word_ce(1), t2 = sideset_word_ce(2), t3 = sideset_word_ce(3);
+  const uint64_t w = c < 16 ? (c < 8 ? t0 : t1) : (c < 24 ? t2 : t3);
+  return (uint32_t)(w >> (8 * (c & 7))) & 0xFFu;
+}
 CF1_HD uint32_t state_of_sideset(uint32_t byte) {
   if (byte == 0) return 0;  // no occurrence reached the vertex
   return encode_sides(side_of_code(byte & 0xFu), side_of_code(byte >> 4));

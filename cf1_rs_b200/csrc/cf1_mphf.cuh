@@ -166,9 +166,15 @@ CF1_HD uint64_t li_local_slot(const LIView &v, const KeyT *bin_keys, uint64_t n_
   return SLOT_NONE;
 }
 
-template <class KeyT>
+// MEMBER: the caller knows the key is in the set (phase 4 queries only keys
+// of the input), so BBHash's slot needs no range check.
+template <class KeyT, bool MEMBER = false>
 CF1_HD uint64_t mphf_slot(const MphfView<KeyT> &v, uint32_t bin, const KeyT &key) {
   uint64_t base = v.dist_off[bin];
+  if (MEMBER && !v.learned) {
+    const uint64_t local = bb_local_slot(v.bb, bin, key);
+    return local == SLOT_NONE ? SLOT_NONE : base + local;
+  }
   uint64_t local;
   uint64_t n_bin = v.dist_off[bin + 1] - base;
   if (v.learned && v.li.roots[bin].use_learned)

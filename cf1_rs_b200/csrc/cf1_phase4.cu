@@ -92,9 +92,9 @@ __global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a
         uint32_t pb = hp ? base_at(a.W, p - 1) : 0;
         uint32_t nb = hn ? base_at(a.W, p + k) : 0;
         uint32_t c = contribution(fw, rc, hp, pb, hn, nb, k);
-        uint64_t slot = mphf_slot(a.mphf, bin, kmin(fw, rc));
+        uint64_t slot = mphf_slot<KeyT, true>(a.mphf, bin, kmin(fw, rc));
         if (slot == SLOT_NONE) atomicOr(a.err, (uint32_t)DEV_MPHF_MISS);
-        else if (SIDESET) atomicOr(a.sides + (slot >> 2), sideset_of_state(c) << (8 * (uint32_t)(slot & 3)));
+        else if (SIDESET) atomicOr(a.sides + (slot >> 2), sideset_lookup(c) << (8 * (uint32_t)(slot & 3)));
         else state_join_cas(a.states, slot, c, a.err, retries);
       }
     }
