@@ -17,11 +17,15 @@ classification into the 5-bit state vector.
           1-4, and the state words copied back into page-locked memory stage
           by stage while phase 4 runs; timed on the host around the call
 
-With N GPUs (torchrun, one rank per GPU) the genome is sharded by bin: every
-rank routes it whole, keeps the bins b with b % N == rank for phases 3-4, and
-the ranks all-gather their per-bin distinct counts (the global slot offsets)
-inside each timed step; `value` is the genome's distinct k-mers over the
-slowest rank's time (strong scaling).
+With N GPUs (torchrun, one rank per GPU) the genome is sharded by bin, rank r
+owning the bins b with b % N == r.  Default (--shard-mode exchange): every
+rank scans only its 1/N of the genome in phase 1, the ranks all-reduce their
+minimizer histograms (NCCL), route their super k-mer records to the bins'
+owners in one NCCL all-to-all, and each runs phases 2-4 on what it received;
+with --shard-mode replicated every rank routes the whole genome instead.
+Either way the ranks all-gather their per-bin distinct counts (the global
+slot offsets) inside each timed step; `value` is the genome's distinct
+k-mers over the slowest rank's time (strong scaling).
 
 Both MPHF forms run: plain per-bin GPU BBHash, and the learned index +
 batched (persistent queue kernels) form; the headline is the faster one,
@@ -70,6 +74,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--leaf-size", type=int, default=0, help="learned index keys per leaf (0 = library default)")
+    p.add_argument("--shard-mode", choices=["exchange", "replicated"], default="exchange",
+                   help="N > 1: scan 1/N of the input per rank and swap records, or route it all on every rank")
     p.add_argument("--tuner-cache", default=os.path.join(tempfile.gettempdir(), "cf1_tuner_cache.txt"),
                    help="autotuner cache file (first warm-up run of an input class measures; '' = off)")
     return p.parse_args()
@@ -260,10 +266,23 @@ def gpu_arm(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
+    xchg = world > 1 and args.shard_mode == "exchange"
+
+    def exchange_step(be) -> float:
+        """One exchange-sharded step (scan, histogram all-reduce, routing,
+        record all-to-all, phases 2-4, counts all-gather): device time on the
+        current stream from before the scan to after the last collective."""
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sharded.run_exchange(be, device="cuda", assemble=False)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
     wl = WORKLOADS[args.workload]
     k, bins = wl["k"], wl["bins"]
-    # strong scaling: every rank routes the same genome and keeps the bins
-    # b with b % world == rank (bin sharding, cf1_rs_b200.sharded)
+    # strong scaling over bin shards: rank r keeps the bins b with
+    # b % world == r (cf1_rs_b200.sharded)
     x = cg.SynthInput(args.workload, scale=args.scale, seed=0)
     # one cache file per rank (ranks run the same classes; no shared writes)
     tuner_path = (args.tuner_cache + (f".rank{rank}" if world > 1 else "")) if args.tuner_cache else None
@@ -272,22 +291,29 @@ def gpu_arm(args):
     clock_info = None
     for form in args.forms.split(","):
         batched = form == "learned"
-        g = cg.Cf1Gpu(k=k, num_bins=bins, device=local, mode=form, batched=batched,
-                      track_short_seqs=bool(wl.get("short")), shard_index=rank, shard_count=world,
-                      tuner_cache=tuner_path, learned_leaf_size=args.leaf_size)
+        copts = dict(mode=form, batched=batched, track_short_seqs=bool(wl.get("short")), tuner_cache=tuner_path,
+                     learned_leaf_size=args.leaf_size)
+        be = sharded.GpuExchangeBackend(k, bins, rank, world, device=local, **copts) if xchg else None
+        g = be.ctx if xchg else cg.Cf1Gpu(k=k, num_bins=bins, device=local, shard_index=rank, shard_count=world,
+                                          **copts)
         g.add_records(x.seq, x.offsets)
         g.upload()
-        for _ in range(args.warmup):
+
+        def step() -> float:
+            if xchg:
+                return exchange_step(be)
             g.run_resident()
-            exchange_ms(g)
+            return g.stats()["ms_total"] + exchange_ms(g)
+
+        for _ in range(args.warmup):
+            step()
         barrier()
         if clock_info is None:
             clocks.start()
         ms, ms_cls, launches, phase = [], [], 0, {}
         for _ in range(args.steps):
-            g.run_resident()
+            ms.append(step())
             s = g.stats()
-            ms.append(s["ms_total"] + exchange_ms(g))
             ms_cls.append(s["ms_classify_kernel"])
             launches += s["n_kernel_launches"]
             for key in ("ms_phase1", "ms_phase2", "ms_phase3_sort", "ms_phase3_mphf", "ms_phase4"):
@@ -301,7 +327,7 @@ def gpu_arm(args):
             value=distinct * args.steps / (total_ms / 1e3), ms_per_step=total_ms / args.steps,
             ms_classify_kernel=maxall(statistics.mean(ms_cls)), launches=launches, stats=s,
             phases_ms={k2: round(v, 3) for k2, v in phase.items()},
-            learned=g.learned_stats() if form == "learned" else None, ctx=g)
+            learned=g.learned_stats() if form == "learned" else None, ctx=g, be=be)
         if form != args.forms.split(",")[-1]:
             g.close()
             forms[form]["ctx"] = None
@@ -315,11 +341,13 @@ def gpu_arm(args):
     # ---- end to end through the C ABI from host buffers
     e2e = None
     if not args.no_e2e:
-        g = head["ctx"]
+        g, be = head["ctx"], head["be"]
         if g is None:
-            g = cg.Cf1Gpu(k=k, num_bins=bins, device=local, mode=head_name, batched=head_name == "learned",
-                          track_short_seqs=bool(wl.get("short")), shard_index=rank, shard_count=world,
-                          tuner_cache=tuner_path, learned_leaf_size=args.leaf_size)
+            copts = dict(mode=head_name, batched=head_name == "learned", track_short_seqs=bool(wl.get("short")),
+                         tuner_cache=tuner_path, learned_leaf_size=args.leaf_size)
+            be = sharded.GpuExchangeBackend(k, bins, rank, world, device=local, **copts) if xchg else None
+            g = be.ctx if xchg else cg.Cf1Gpu(k=k, num_bins=bins, device=local, shard_index=rank,
+                                              shard_count=world, **copts)
         # inputs and the result in page-locked host memory: the records go to
         # the device in one DMA, the state words come back in one
         pin_seq = torch.empty(max(1, x.seq.nbytes), dtype=torch.uint8, pin_memory=True)
@@ -332,8 +360,14 @@ def gpu_arm(args):
         for i in range(args.warmup + args.steps):
             barrier()
             t0 = time.perf_counter()
-            g.run_streamed(seq_h, x.offsets, words)  # copies overlapped with phases 1 and 4
-            exchange_ms(g)
+            if xchg:  # page-locked records DMA'd in, the shard's words copied back
+                g.reset_input()
+                g.add_records(seq_h, x.offsets)
+                sharded.run_exchange(be, device="cuda", assemble=False)
+                g.states(words[: (g.total_kmers() + 11) // 12])
+            else:
+                g.run_streamed(seq_h, x.offsets, words)  # copies overlapped with phases 1 and 4
+                exchange_ms(g)
             dt = time.perf_counter() - t0
             if i >= args.warmup:
                 times.append(dt)
@@ -380,7 +414,8 @@ def gpu_arm(args):
         "vs_baseline": None, "dtype": "u64" if k <= 32 else "u128", "data": "synthetic (seeded generator)",
         "config": {"workload": wl["name"], "k": k, "num_bins": bins, "scale": args.scale, "form": head_name,
                    "bases": int(s["n_bases"]), "records": int(s["n_records"]), "distinct_kmers": int(n_dist),
-                   "kmer_occurrences": int(n_occ), "parallelism": f"bin shards x{world}" if world > 1 else "1 GPU",
+                   "kmer_occurrences": int(n_occ),
+                   "parallelism": f"bin shards x{world} ({args.shard_mode})" if world > 1 else "1 GPU",
                    "l2": "input 3.1 GB > 126 MB L2 (no flush needed)"},
         "bp_per_s": s["n_bases"] / (head["ms_per_step"] / 1e3),
         "roofline": roofline,

@@ -73,7 +73,7 @@ EXPORTED = [
     "cf1gpu_total_kmers", "cf1gpu_bin_distinct_counts", "cf1gpu_copy_states", "cf1gpu_query", "cf1gpu_dump_states", "cf1gpu_verify_bijection",
     "cf1gpu_short_seq_count", "cf1gpu_short_seq", "cf1gpu_export_mphf", "cf1gpu_export_bin", "cf1gpu_mphf_host_query",
     "cf1gpu_learned_stats", "cf1gpu_learned_grad", "cf1gpu_last_error", "cf1gpu_destroy", "cf1gpu_version",
-    "cf1gpu_distinct_kmers_noalloc",
+    "cf1gpu_distinct_kmers_noalloc", "cf1gpu_xshard_scan", "cf1gpu_xshard_route", "cf1gpu_xshard_finish",
 ]
 
 
@@ -118,6 +118,9 @@ def lib():
     L.cf1gpu_destroy.restype = None
     L.cf1gpu_version.restype = C.c_char_p
     L.cf1gpu_distinct_kmers_noalloc.argtypes = [C.c_int, C.c_uint32, vp, C.c_size_t, vp, C.c_size_t, vp, vp]
+    L.cf1gpu_xshard_scan.argtypes = [vp, vp, u64p]
+    L.cf1gpu_xshard_route.argtypes = [vp, vp, vp, C.c_size_t, vp]
+    L.cf1gpu_xshard_finish.argtypes = [vp, vp, C.c_size_t]
     _lib = L
     return L
 
@@ -133,6 +136,11 @@ def distinct_kmers_noalloc(d_seq: int, length: int, k: int, d_keys_out: int, out
 
 def _p(a, t):
     return a.ctypes.data_as(t)
+
+
+def _addr(a) -> int:
+    """Address of a numpy array (host) or a torch tensor (host or device)."""
+    return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
 
 
 def learned_grad(params: np.ndarray, x: np.ndarray, t: np.ndarray, device: int = 0):
@@ -191,6 +199,7 @@ class Cf1Gpu:
         self.h = h
         self.k = k
         self.num_bins = num_bins
+        self.shard_index, self.shard_count = shard_index, max(shard_count, 1)
         self.kw = 1 if k <= 32 else 2
 
     def _check(self, st):
@@ -262,6 +271,32 @@ class Cf1Gpu:
         out = np.empty(self.num_bins, np.uint64)
         self._check(lib().cf1gpu_bin_distinct_counts(self.h, _p(out, u64p), self.num_bins))
         return out
+
+    # ---- exchange-based sharding (cf1gpu_xshard_*): buffers are numpy
+    # arrays or torch tensors on the host or on this context's device
+    def xshard_scan(self, hist=None):
+        """Phase 1 over this shard's share of the input: (the share's 65,536
+        bucket histogram, its number of super k-mer records)."""
+        if hist is None:
+            hist = np.zeros(65536, np.uint32)
+        n = C.c_uint64(0)
+        self._check(lib().cf1gpu_xshard_scan(self.h, _addr(hist), C.byref(n)))
+        return hist, n.value
+
+    def xshard_route(self, hist, n_records: int, records=None, counts=None):
+        """The share's records grouped by owner shard, from the summed
+        histogram: (records [n_records] u64, counts [shard_count] u64)."""
+        if records is None:
+            records = np.empty(max(n_records, 1), np.uint64)
+        if counts is None:
+            counts = np.zeros(max(self.shard_count, 1), np.uint64)
+        self._check(lib().cf1gpu_xshard_route(self.h, _addr(hist), _addr(records), n_records, _addr(counts)))
+        return records[:n_records], counts
+
+    def xshard_finish(self, records, n: int | None = None):
+        """Phases 2-4 on the records this shard received."""
+        n = len(records) if n is None else n
+        self._check(lib().cf1gpu_xshard_finish(self.h, _addr(records) if n else None, n))
 
     def run_streamed(self, seq: np.ndarray, offsets: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
         """Input in, state words out, copies overlapped with phases 1 and 4

@@ -144,6 +144,7 @@ int cf1gpu_reset_input(cf1gpu_ctx *c) {
   c->short_seqs.clear();
   c->uploaded = false;
   c->ran = false;
+  c->x_step = 0;
   return CF1GPU_OK;
 }
 
@@ -213,6 +214,21 @@ int cf1gpu_bin_distinct_counts(const cf1gpu_ctx *c, uint64_t *counts, size_t nbi
     CF1_CUDA(cudaStreamSynchronize(c->stream));
     for (size_t b = 0; b < nbins; b++) counts[b] = off[b + 1] - off[b];
   });
+}
+
+int cf1gpu_xshard_scan(cf1gpu_ctx *c, uint32_t *hist, uint64_t *n_records) {
+  if (!c || !hist || !n_records) return CF1GPU_ERR_INVALID_ARG;
+  return guard(c, [&] { cf1::xshard_scan(c, hist, n_records); });
+}
+
+int cf1gpu_xshard_route(cf1gpu_ctx *c, const uint32_t *hist, uint64_t *records, size_t records_cap, uint64_t *counts) {
+  if (!c || !hist || !counts || (records_cap && !records)) return CF1GPU_ERR_INVALID_ARG;
+  return guard(c, [&] { cf1::xshard_route(c, hist, records, records_cap, counts); });
+}
+
+int cf1gpu_xshard_finish(cf1gpu_ctx *c, const uint64_t *records, size_t n) {
+  if (!c || (n && !records)) return CF1GPU_ERR_INVALID_ARG;
+  return guard(c, [&] { cf1::xshard_finish(c, records, n); });
 }
 
 int cf1gpu_copy_states(cf1gpu_ctx *c, uint64_t *dst, size_t n_words) {

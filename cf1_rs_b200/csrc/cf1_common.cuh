@@ -349,6 +349,7 @@ enum DeviceError : uint32_t {
   DEV_OVERFLOW = 1u << 2,      // a buffer or queue bound was hit
   DEV_BIJECTION = 1u << 3,     // slot seen twice or never
   DEV_WAIT_LIMIT = 1u << 4,    // a bounded spin wait gave up
+  DEV_FOREIGN = 1u << 5,       // a received record is not this shard's to process
 };
 
 }  // namespace cf1

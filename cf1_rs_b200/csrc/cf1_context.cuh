@@ -75,6 +75,14 @@ struct cf1gpu_ctx {
   cf1::DevBuf d_l0, d_l0surv, d_binfile, d_binimg, d_raw, d_intake, d_shard, d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
       d_keys, d_dist, d_dist_off, d_states, d_scan, d_seen, d_qin, d_qout, d_queue;
   uint64_t rec_cap_hint = 0;  // phase-1 record list size of the last run
+  // exchange-based sharding: the scanned slice's records wait in d_keys for
+  // routing; d_xsend holds them grouped by owner shard, d_xcnt the counts
+  cf1::DevBuf d_xsend, d_xcnt;
+  int x_step = 0;              // 0 nothing pending, 1 slice scanned, 2 slice routed
+  uint64_t x_local = 0;        // records of the scanned slice
+  uint64_t x_rec_cap = 0;      // capacity of their list in d_keys
+  double x_ms_scan = 0;        // device time of the slice's scan and routing
+  uint64_t x_launches0 = 0;    // kernel launch count when the scan began
   // autotuner: cache file ("" = off), the key the current tuning is for
   std::string tuner_path;
   cf1::TuneKey tuned_key;

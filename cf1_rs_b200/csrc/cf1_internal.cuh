@@ -139,7 +139,8 @@ struct SuperkmerArgs {
 };
 // Phase 1: minimizer histogram + unordered super k-mer list.
 void launch_superkmer_scan(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s);
-// Phase 2: route the list into per-bin ranges rec_off[0..num_bins] of records.
+// Phase 2: route the list into per-bin ranges rec_off[0..num_bins] of records
+// (rec_bucket nullptr: the records already carry their bin).
 void launch_bin_scatter(const uint64_t *rec_tmp, const uint16_t *rec_bucket, uint64_t n, const uint16_t *lut,
                         uint32_t num_bins, const uint64_t *rec_off, uint32_t *cursor, uint64_t *records, uint32_t *err,
                         cudaStream_t s);

@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(BS_BLOCK) bin_scatter_kernel(const uint64_t *r
     uint64_t r = r0 + (uint64_t)i * BS_BLOCK + tid;
     bin[i] = 0xFFFFFFFFu;
     if (r < n) {
-      bin[i] = lut[rec_bucket[r]];
+      bin[i] = rec_bucket ? lut[rec_bucket[r]] : rec_bin(rec_tmp[r]);  // no buckets: the records carry their bin
       li[i] = atomicAdd(&s_cnt[bin[i]], 1u);
     }
   }

@@ -65,6 +65,82 @@ __global__ void shard_copy_kernel(const uint64_t *in, const uint64_t *rec_off, c
   for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += blockDim.x) out[i + delta] = in[i];
 }
 
+// Exchange-based sharding.  Route: the scanned slice's records, tagged with
+// their bins, grouped by owner shard (bin % shards); a CTA counts its records
+// per owner in shared memory and reserves each owner's places with one atomic.
+constexpr int XR_BLOCK = 256, XR_ITEMS = 8;
+__global__ void __launch_bounds__(XR_BLOCK) xroute_count_kernel(const uint16_t *bucket, uint64_t n, const uint16_t *lut,
+                                                                uint32_t shards, unsigned long long *cnt) {
+  extern __shared__ uint32_t xr_cnt[];  // [shards]
+  for (uint32_t i = threadIdx.x; i < shards; i += XR_BLOCK) xr_cnt[i] = 0;
+  __syncthreads();
+  for (uint64_t r = (uint64_t)blockIdx.x * XR_BLOCK + threadIdx.x; r < n; r += (uint64_t)gridDim.x * XR_BLOCK)
+    atomicAdd(&xr_cnt[lut[bucket[r]] % shards], 1u);
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < shards; i += XR_BLOCK)
+    if (xr_cnt[i]) atomicAdd(&cnt[i], (unsigned long long)xr_cnt[i]);
+}
+
+__global__ void __launch_bounds__(XR_BLOCK) xroute_scatter_kernel(const uint64_t *rec, const uint16_t *bucket, uint64_t n,
+                                                                  const uint16_t *lut, uint32_t shards,
+                                                                  const uint64_t *off, unsigned long long *cursor,
+                                                                  uint64_t *out, uint32_t *err) {
+  extern __shared__ uint64_t xr_base[];  // [shards], then the counts
+  uint32_t *s_cnt = reinterpret_cast<uint32_t *>(xr_base + shards);
+  for (uint32_t i = threadIdx.x; i < shards; i += XR_BLOCK) s_cnt[i] = 0;
+  __syncthreads();
+  const uint64_t r0 = (uint64_t)blockIdx.x * XR_BLOCK * XR_ITEMS;
+  uint32_t bin[XR_ITEMS], li[XR_ITEMS];
+#pragma unroll
+  for (int i = 0; i < XR_ITEMS; i++) {
+    const uint64_t r = r0 + (uint64_t)i * XR_BLOCK + threadIdx.x;
+    bin[i] = 0xFFFFFFFFu;
+    if (r < n) {
+      bin[i] = lut[bucket[r]];
+      li[i] = atomicAdd(&s_cnt[bin[i] % shards], 1u);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < XR_ITEMS; i++) {
+    if (bin[i] == 0xFFFFFFFFu || li[i]) continue;
+    const uint32_t d = bin[i] % shards;
+    xr_base[d] = off[d] + atomicAdd(&cursor[d], (unsigned long long)s_cnt[d]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < XR_ITEMS; i++) {
+    if (bin[i] == 0xFFFFFFFFu) continue;
+    const uint32_t d = bin[i] % shards;
+    const uint64_t r = r0 + (uint64_t)i * XR_BLOCK + threadIdx.x, t = rec[r], idx = xr_base[d] + li[i];
+    if (idx < off[d + 1]) out[idx] = rec_pack(rec_pos(t), rec_n(t), bin[i]);
+    else atomicOr(err, (uint32_t)DEV_OVERFLOW);
+  }
+}
+
+// Finish: records per bin of the records this shard received; a record of
+// another shard's bin, or one reaching past the input, is refused.
+__global__ void __launch_bounds__(XR_BLOCK) xrecv_count_kernel(const uint64_t *rec, uint64_t n, uint32_t nbins,
+                                                               uint32_t idx, uint32_t shards, uint64_t L, int k,
+                                                               unsigned long long *cnt, uint32_t *err) {
+  extern __shared__ uint32_t xr_cnt[];  // [nbins]
+  for (uint32_t b = threadIdx.x; b < nbins; b += XR_BLOCK) xr_cnt[b] = 0;
+  __syncthreads();
+  for (uint64_t r = (uint64_t)blockIdx.x * XR_BLOCK + threadIdx.x; r < n; r += (uint64_t)gridDim.x * XR_BLOCK) {
+    const uint64_t x = rec[r];
+    const uint32_t b = rec_bin(x);
+    if (b >= nbins || b % shards != idx || rec_pos(x) + rec_n(x) + (uint64_t)k - 1 > L) atomicOr(err, (uint32_t)DEV_FOREIGN);
+    else atomicAdd(&xr_cnt[b], 1u);
+  }
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < nbins; b += XR_BLOCK)
+    if (xr_cnt[b]) atomicAdd(&cnt[b], (unsigned long long)xr_cnt[b]);
+}
+
+unsigned stride_grid(uint64_t n, int num_sms) {
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(n, XR_BLOCK), (uint64_t)num_sms * 8));
+}
+
 template <class KeyT>
 Backend<KeyT> &backend(cf1gpu_ctx *c) {
   return ctx_backend<KeyT>(c);
@@ -82,6 +158,8 @@ void check_device_errors(uint32_t err) {
   if (err & DEV_OVERFLOW) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "a device buffer bound was hit");
   if (err & DEV_MPHF_MISS) throw Error(CF1GPU_ERR_BIJECTION, "phase 4: a k-mer was not found by the MPHF");
   if (err & DEV_BIJECTION) throw Error(CF1GPU_ERR_BIJECTION, "MPHF is not a bijection onto [0, n)");
+  if (err & DEV_FOREIGN)
+    throw Error(CF1GPU_ERR_INVALID_ARG, "a received record is not this shard's (bin, position or length out of range)");
 }
 
 template <class KeyT>
@@ -129,16 +207,28 @@ struct StreamIO {
 };
 constexpr int STREAM_STAGES = 8;
 
+// One run of phases 1-4 (FULL), or one of the two device steps of an
+// exchange-sharded run: XSCAN is phase 1 over this shard's slice of the
+// minimizer tiles (the histogram goes to the caller, the records wait for
+// routing); XFINISH runs phases 2-4 on the records the shards routed here.
+enum class Step { FULL, XSCAN, XFINISH };
+struct XShard {
+  uint32_t *hist_out = nullptr;    // XSCAN: the slice's histogram (host or device memory)
+  const uint64_t *recv = nullptr;  // XFINISH: received records (host or device memory)
+  uint64_t n_recv = 0;
+};
+
 template <class KeyT>
-void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
+void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, const XShard *xs = nullptr) {
   cudaStream_t s = c->stream;
   Backend<KeyT> &be = backend<KeyT>(c);
   const uint64_t L = c->L;
   const int k = c->k;
   const uint32_t B = c->opts.num_bins;
   const bool batched = c->opts.batched != 0;
+  const uint32_t shards = c->opts.shard_count > 1 ? c->opts.shard_count : 1;
   c->nbins = B;
-  const uint64_t launches0 = g_launches.load();
+  const uint64_t launches0 = step == Step::XFINISH ? c->x_launches0 : g_launches.load();
   // The learned index needs each bin's keys sorted; BBHash needs them
   // distinct (128-bit keys always take the sorted path).
   const bool sorted = c->opts.mphf_mode == CF1GPU_MPHF_LEARNED || c->opts.sort_mode == 1 || KOps<KeyT>::WORDS == 2;
@@ -163,7 +253,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
       c->tuned_key = key;
       c->tune_valid = true;
       c->tuner_state = 1;
-    } else if (!io) {
+    } else if (!io && step == Step::FULL) {
       c->tuned_key = key;
       c->tune_valid = false;
       tune_now = true;
@@ -179,7 +269,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
   uint64_t *NM = c->d_NM.get<uint64_t>(n_nm + 2);
   CF1_CUDA(cudaMemsetAsync(W + 2 * n_nm, 0, 4 * sizeof(uint64_t), s));
   CF1_CUDA(cudaMemsetAsync(NM + n_nm, 0xFF, 2 * sizeof(uint64_t), s));
-  if (!io) launch_pack(c->d_ascii.as<uint8_t>(), L, W, NM, s);
+  if (!io && step != Step::XFINISH) launch_pack(c->d_ascii.as<uint8_t>(), L, W, NM, s);
   uint32_t *hist = c->d_hist.get<uint32_t>(NUM_BUCKETS);
   SuperkmerArgs a{};
   a.W = W;
@@ -203,9 +293,16 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
   // The list lives in the key buffer, which phase 3 only fills after phase 2
   // has routed the list.
   Small hs;
+  const bool xscan = step == Step::XSCAN;
   auto phase1 = [&](uint32_t tile) {
     a.tile = tile;
     a.n_tiles = L >= (uint64_t)k ? ceil_div(L - k + 1, a.tile) : 0;
+    if (xscan) {  // this shard's slice of the tiles, in plain launches
+      const uint64_t nt = a.n_tiles;
+      a.tile_begin = nt * c->opts.shard_index / shards;
+      a.n_tiles = nt * (c->opts.shard_index + 1) / shards;
+      a.tile_counter = nullptr;
+    }
     for (int attempt = 0;; attempt++) {
       a.rec_cap = std::max<uint64_t>(c->rec_cap_hint, L / 4 + 1024);
       uint8_t *rbuf = static_cast<uint8_t *>(c->d_keys.reserve(a.rec_cap * (sizeof(uint64_t) + sizeof(uint16_t))));
@@ -213,19 +310,21 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
       a.rec_bucket = reinterpret_cast<uint16_t *>(rbuf + a.rec_cap * sizeof(uint64_t));
       CF1_CUDA(cudaMemsetAsync(hist, 0, NUM_BUCKETS * sizeof(uint32_t), s));
       CF1_CUDA(cudaMemsetAsync(sm, 0, sizeof(Small), s));
-      launch_superkmer_scan(a, pctas, s);
-      launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
+      launch_superkmer_scan(a, xscan ? 0 : pctas, s);
+      if (!xscan) launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
       CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
-      CF1_CUDA(cudaMemcpyAsync(&c->n_super, rec_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+      if (!xscan) CF1_CUDA(cudaMemcpyAsync(&c->n_super, rec_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
       CF1_CUDA(cudaStreamSynchronize(s));
-      if (hs.rec_count != c->n_super)
+      if (!xscan && hs.rec_count != c->n_super)
         throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record count != histogram total");
       if (hs.rec_count <= a.rec_cap) break;
       if (attempt) throw Error(CF1GPU_ERR_QUEUE_OVERRUN, "phase 1: record list overflowed twice");
       c->rec_cap_hint = hs.rec_count;
     }
   };
-  if (io) {
+  if (step == Step::XFINISH) {
+    // phase 1 ran in the scan step; the records arrive below
+  } else if (io) {
     // Streamed intake: as chunk c of the record bytes lands, place the intake
     // tiles it completes, pack the W/NM words wholly inside the placed
     // prefix, and scan the minimizer tiles whose bases are all packed.  The
@@ -302,19 +401,50 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
   } else {
     phase1(c->tune.sk_tile);
   }
-  c->n_occ = hs.n_kmers;
-  c->n_bins_eff = hs.n_bins_eff;
   CF1_CUDA(cudaEventRecord(c->ev[1], s));
+  if (xscan) {  // the slice's histogram to the caller; its records wait for routing
+    check_device_errors(hs.err);
+    CF1_CUDA(cudaMemcpyAsync(xs->hist_out, hist, NUM_BUCKETS * sizeof(uint32_t), cudaMemcpyDefault, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+    c->x_local = hs.rec_count;
+    c->x_rec_cap = a.rec_cap;
+    c->x_ms_scan = elapsed(c->ev[0], c->ev[1]);
+    return;
+  }
+  if (step != Step::XFINISH) {
+    c->n_occ = hs.n_kmers;
+    c->n_bins_eff = hs.n_bins_eff;
+  }
 
   // ---- phase 2: route super k-mers into bins
+  if (step == Step::XFINISH) {
+    // The received records carry their bins: count them per bin for the
+    // ranges, after checking that every one is this shard's.
+    const uint64_t n = xs->n_recv;
+    uint64_t *rin = static_cast<uint64_t *>(c->d_keys.reserve((n + 1) * sizeof(uint64_t)));
+    if (n) CF1_CUDA(cudaMemcpyAsync(rin, xs->recv, n * sizeof(uint64_t), cudaMemcpyDefault, s));
+    uint64_t *cnt = c->d_xcnt.get<uint64_t>(B + 1);
+    CF1_CUDA(cudaMemsetAsync(cnt, 0, B * sizeof(uint64_t), s));
+    if (n) {
+      xrecv_count_kernel<<<stride_grid(n, c->num_sms), XR_BLOCK, B * sizeof(uint32_t), s>>>(
+          rin, n, B, c->opts.shard_index, shards, L, k, reinterpret_cast<unsigned long long *>(cnt), &sm->err);
+      CF1_LAUNCH_CHECK();
+    }
+    exclusive_scan_u64(cnt, rec_off, B, c->d_scan, s);
+    CF1_CUDA(cudaMemcpyAsync(&hs.err, &sm->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    CF1_CUDA(cudaStreamSynchronize(s));
+    check_device_errors(hs.err);
+    a.rec_tmp = rin;
+    a.rec_bucket = nullptr;
+    c->n_super = n;
+  }
   uint64_t NS = c->n_super;
   uint64_t *records = c->d_records.get<uint64_t>(NS + 1);
   CF1_CUDA(cudaMemsetAsync(records, 0, (NS + 1) * sizeof(uint64_t), s));
   uint32_t *cursor = c->d_cursor.get<uint32_t>(B);
   CF1_CUDA(cudaMemsetAsync(cursor, 0, B * sizeof(uint32_t), s));
   launch_bin_scatter(a.rec_tmp, a.rec_bucket, NS, lut, B, rec_off, cursor, records, &sm->err, s);
-  const uint32_t shards = c->opts.shard_count > 1 ? c->opts.shard_count : 1;
-  if (shards > 1) {
+  if (shards > 1 && step == Step::FULL) {
     // Keep this shard's bins: their records, moved to the front through the
     // free key buffer (the phase-1 list in it has been routed); the other
     // bins keep empty ranges, so they get no keys, slots or states.
@@ -336,7 +466,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
   }
   uint64_t *kpre = c->d_kpre.get<uint64_t>(NS + 1);
   record_kmer_prefix(records, NS, kpre, c->d_lens, c->d_scan, s);
-  if (shards > 1) {  // the k-mer windows of this shard's records
+  if (shards > 1 || step == Step::XFINISH) {  // the k-mer windows of this shard's records
     CF1_CUDA(cudaMemcpyAsync(&c->n_occ, kpre + NS, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     CF1_CUDA(cudaStreamSynchronize(s));
   }
@@ -553,13 +683,15 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr) {
   st.sort_msd_bits = c->msd_bits >= 0 ? (uint64_t)c->msd_bits : ~0ull;
   st.tuner_state = (uint64_t)c->tuner_state;
   st.sk_tile = c->tune.sk_tile;
-  st.ms_phase1 = elapsed(c->ev[0], c->ev[1]);
+  // an exchange-sharded run's phase 1 is the slice's scan and routing
+  const double p1_before = step == Step::XFINISH ? c->x_ms_scan : 0.0;
+  st.ms_phase1 = elapsed(c->ev[0], c->ev[1]) + p1_before;
   st.ms_phase2 = elapsed(c->ev[1], c->ev[2]);
   st.ms_phase3_sort = elapsed(c->ev[2], c->ev[3]);
   st.ms_phase3_mphf = elapsed(c->ev[3], c->ev[4]);
   st.ms_phase4 = elapsed(c->ev[4], c->ev[7]);
   st.ms_classify_kernel = elapsed(c->ev[5], c->ev[6]);
-  st.ms_total = elapsed(c->ev[0], c->ev[7]);
+  st.ms_total = elapsed(c->ev[0], c->ev[7]) + p1_before;
 }
 
 template <class KeyT>
@@ -660,6 +792,7 @@ std::string first_token(const char *name, size_t n) {
 // ---- entry points used by the C ABI (and by the C++ host mirror) ----
 void run_resident(cf1gpu_ctx *c) {
   if (!c->uploaded) throw Error(CF1GPU_ERR_STATE, "no input on the device: call cf1gpu_upload first");
+  c->x_step = 0;
   if (c->wide) run_impl<Key2>(c);
   else run_impl<uint64_t>(c);
   c->ran = true;
@@ -675,6 +808,7 @@ size_t run_streamed(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, siz
   c->short_seqs.clear();
   c->uploaded = false;
   c->ran = false;
+  c->x_step = 0;
   std::vector<uint64_t> dst(n + 1);
   uint64_t pos = 0;
   for (size_t i = 0; i < n; i++) {
@@ -744,6 +878,78 @@ size_t run_streamed(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, siz
     CF1_CUDA(cudaStreamSynchronize(s));
   }
   return nw;
+}
+
+void xshard_scan(cf1gpu_ctx *c, uint32_t *hist, uint64_t *n_local) {
+  upload(c);
+  c->ran = false;
+  c->x_step = 0;
+  c->x_launches0 = g_launches.load();
+  XShard xs;
+  xs.hist_out = hist;
+  if (c->wide) run_impl<Key2>(c, nullptr, Step::XSCAN, &xs);
+  else run_impl<uint64_t>(c, nullptr, Step::XSCAN, &xs);
+  c->x_step = 1;
+  *n_local = c->x_local;
+}
+
+void xshard_route(cf1gpu_ctx *c, const uint32_t *hist_in, uint64_t *send, size_t cap, uint64_t *counts) {
+  if (c->x_step != 1) throw Error(CF1GPU_ERR_STATE, "no scanned slice to route: call cf1gpu_xshard_scan first");
+  const uint64_t n = c->x_local;
+  if (cap < n) throw Error(CF1GPU_ERR_INVALID_ARG, "record buffer too small: need " + std::to_string(n));
+  cudaStream_t s = c->stream;
+  const uint32_t B = c->opts.num_bins;
+  const uint32_t N = c->opts.shard_count > 1 ? c->opts.shard_count : 1;
+  CF1_CUDA(cudaEventRecord(c->ev[10], s));
+  // the partition of the summed histogram: the same on every shard
+  uint32_t *hist = c->d_hist.get<uint32_t>(NUM_BUCKETS);
+  CF1_CUDA(cudaMemcpyAsync(hist, hist_in, NUM_BUCKETS * sizeof(uint32_t), cudaMemcpyDefault, s));
+  uint16_t *lut = c->d_lut.get<uint16_t>(NUM_BUCKETS);
+  uint64_t *rec_off = c->d_rec_off.get<uint64_t>(B + 1);
+  Small *sm = c->d_small.get<Small>(1);
+  CF1_CUDA(cudaMemsetAsync(sm, 0, sizeof(Small), s));
+  launch_partition(hist, B, lut, rec_off, &sm->n_bins_eff, s);
+  // the slice's records, grouped by owner shard
+  const uint8_t *rbuf = c->d_keys.as<const uint8_t>();
+  const uint64_t *rec = reinterpret_cast<const uint64_t *>(rbuf);
+  const uint16_t *bucket = reinterpret_cast<const uint16_t *>(rbuf + c->x_rec_cap * sizeof(uint64_t));
+  uint64_t *cnt = c->d_xcnt.get<uint64_t>(3 * (size_t)(N + 1));
+  uint64_t *off = cnt + (N + 1), *cur = off + (N + 1);
+  CF1_CUDA(cudaMemsetAsync(cnt, 0, 3 * (size_t)(N + 1) * sizeof(uint64_t), s));
+  uint64_t *out = c->d_xsend.get<uint64_t>(n + 1);
+  if (n) {
+    xroute_count_kernel<<<stride_grid(n, c->num_sms), XR_BLOCK, N * sizeof(uint32_t), s>>>(
+        bucket, n, lut, N, reinterpret_cast<unsigned long long *>(cnt));
+    CF1_LAUNCH_CHECK();
+  }
+  exclusive_scan_u64(cnt, off, N, c->d_scan, s);
+  if (n) {
+    xroute_scatter_kernel<<<(unsigned)ceil_div(n, (uint64_t)XR_BLOCK * XR_ITEMS), XR_BLOCK,
+                            N * (sizeof(uint64_t) + sizeof(uint32_t)), s>>>(
+        rec, bucket, n, lut, N, off, reinterpret_cast<unsigned long long *>(cur), out, &sm->err);
+    CF1_LAUNCH_CHECK();
+    CF1_CUDA(cudaMemcpyAsync(send, out, n * sizeof(uint64_t), cudaMemcpyDefault, s));
+  }
+  CF1_CUDA(cudaMemcpyAsync(counts, cnt, N * sizeof(uint64_t), cudaMemcpyDefault, s));
+  CF1_CUDA(cudaEventRecord(c->ev[11], s));
+  Small hs;
+  CF1_CUDA(cudaMemcpyAsync(&hs, sm, sizeof(Small), cudaMemcpyDeviceToHost, s));
+  CF1_CUDA(cudaStreamSynchronize(s));
+  check_device_errors(hs.err);
+  c->n_bins_eff = hs.n_bins_eff;
+  c->x_ms_scan += elapsed(c->ev[10], c->ev[11]);
+  c->x_step = 2;
+}
+
+void xshard_finish(cf1gpu_ctx *c, const uint64_t *recv, size_t n) {
+  if (c->x_step != 2) throw Error(CF1GPU_ERR_STATE, "the slice is not routed: call cf1gpu_xshard_route first");
+  XShard xs;
+  xs.recv = recv;
+  xs.n_recv = n;
+  c->x_step = 0;
+  if (c->wide) run_impl<Key2>(c, nullptr, Step::XFINISH, &xs);
+  else run_impl<uint64_t>(c, nullptr, Step::XFINISH, &xs);
+  c->ran = true;
 }
 
 void upload(cf1gpu_ctx *c) {

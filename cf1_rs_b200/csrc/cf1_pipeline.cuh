@@ -12,6 +12,9 @@ void add_fasta(cf1gpu_ctx *c, const char *path);
 void upload(cf1gpu_ctx *c);
 void run_resident(cf1gpu_ctx *c);
 size_t run_streamed(cf1gpu_ctx *c, const uint8_t *seqs, const uint64_t *off, size_t n, uint64_t *words, size_t cap);
+void xshard_scan(cf1gpu_ctx *c, uint32_t *hist, uint64_t *n_local);
+void xshard_route(cf1gpu_ctx *c, const uint32_t *hist, uint64_t *send, size_t cap, uint64_t *counts);
+void xshard_finish(cf1gpu_ctx *c, const uint64_t *recv, size_t n);
 void dump_states(cf1gpu_ctx *c, uint64_t *keys, uint8_t *states);
 void verify_bijection(cf1gpu_ctx *c);
 void query(cf1gpu_ctx *c, const uint64_t *keys, size_t n, uint64_t *slots);

@@ -10,10 +10,18 @@ is an all-gather of the per-bin distinct counts: bin b's global slots start
 at the sum of the counts of the bins before it, and the global state vector
 is the owners' per-bin state runs laid end to end in bin order.
 
+Exchange-based sharding (:func:`run_exchange`) splits phases 1-2 as well:
+every rank scans only its share of the input's minimizer tiles, the ranks
+sum their minimizer histograms (all-reduce; every rank then derives the same
+partition), route their records to the bins' owners (one all-to-all of
+8-byte records: the input itself is resident on every rank), and each owner
+runs phases 2-4 on what it received.
+
 The device part sits behind a small backend interface (``run`` returning the
-per-bin counts and the local 5-bit states), so the collective plumbing and
-the assembly below are the same code whether the states come from the GPUs
-(:class:`GpuShardBackend`) or from a stand-in in a CPU test.
+per-bin counts and the local 5-bit states; ``scan``/``route``/``finish`` for
+the exchange), so the collective plumbing and the assembly below are the
+same code whether the states come from the GPUs (:class:`GpuShardBackend`,
+:class:`GpuExchangeBackend`) or from a stand-in in a CPU test.
 """
 from __future__ import annotations
 
@@ -149,4 +157,94 @@ def run_sharded(backend, seq: np.ndarray, offsets: np.ndarray, device=None, asse
     if not assemble:
         return goff, None
     codes_all = gather_codes(codes, device)
+    return goff, pack_states(assemble_states(codes_all, counts_all))
+
+
+# ------------------------------------------------ exchange-based sharding ----
+def exchange_records(send, counts):
+    """All-to-all of routed records: `send` (int64 tensor) holds counts[r]
+    records for rank r, in rank order; returns the records sent to this rank
+    by every rank (int64 tensor on send's device)."""
+    import torch
+    import torch.distributed as dist
+
+    recv_counts = torch.empty_like(counts)
+    dist.all_to_all_single(recv_counts, counts)
+    in_splits = [int(x) for x in counts.tolist()]
+    out_splits = [int(x) for x in recv_counts.tolist()]
+    recv = torch.empty(sum(out_splits), dtype=torch.int64, device=send.device)
+    dist.all_to_all_single(recv, send, out_splits, in_splits)
+    return recv
+
+
+class GpuExchangeBackend:
+    """This rank's share of an exchange-sharded run on its GPU (the
+    cf1gpu_xshard_* entry points).  Buffers are torch tensors on the GPU, so
+    the all-reduce and the all-to-all run on them in place (NCCL)."""
+
+    def __init__(self, k: int, num_bins: int, rank: int, world: int, device: int = 0, **opts):
+        import torch
+
+        from cf1_rs_b200 import Cf1Gpu
+
+        self.dev = torch.device("cuda", device)
+        self.world = world
+        self.ctx = Cf1Gpu(k=k, num_bins=num_bins, device=device, shard_index=rank, shard_count=world, **opts)
+
+    def _settle(self):
+        # torch's stream (its allocations and collectives) before the library's
+        import torch
+
+        torch.cuda.current_stream(self.dev).synchronize()
+
+    def load(self, seq: np.ndarray, offsets: np.ndarray):
+        self.ctx.reset_input()
+        self.ctx.add_records(seq, offsets)
+
+    def scan(self):
+        import torch
+
+        hist = torch.zeros(65536, dtype=torch.int32, device=self.dev)  # u32 counts (sums wrap alike)
+        self._settle()
+        _, n = self.ctx.xshard_scan(hist)
+        return hist, n
+
+    def route(self, hist, n_local: int):
+        import torch
+
+        records = torch.empty(max(n_local, 1), dtype=torch.int64, device=self.dev)
+        counts = torch.zeros(self.world, dtype=torch.int64, device=self.dev)
+        self._settle()
+        self.ctx.xshard_route(hist, n_local, records, counts)
+        return records[:n_local], counts
+
+    def finish(self, recv):
+        self._settle()
+        self.ctx.xshard_finish(recv, recv.numel())
+        return self.ctx.bin_distinct_counts()
+
+    def codes(self):
+        g = self.ctx
+        return unpack_states(g.states(), g.total_kmers())
+
+    def close(self):
+        self.ctx.close()
+
+
+def run_exchange(backend, device=None, assemble: bool = True):
+    """Runs this rank's share of an exchange-sharded run (the backend holds
+    the input already).  Returns (global slot offsets, global packed state
+    words or None); every rank must call it (it holds collectives)."""
+    import torch.distributed as dist
+
+    hist, n_local = backend.scan()
+    dist.all_reduce(hist)  # the input's minimizer histogram, on every rank
+    send, counts = backend.route(hist, n_local)
+    recv = exchange_records(send, counts)
+    bin_counts = backend.finish(recv)
+    counts_all = allgather_counts(bin_counts, device)
+    goff = global_offsets(counts_all)
+    if not assemble:
+        return goff, None
+    codes_all = gather_codes(backend.codes(), device)
     return goff, pack_states(assemble_states(codes_all, counts_all))

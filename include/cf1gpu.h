@@ -173,6 +173,33 @@ uint64_t cf1gpu_total_kmers(const cf1gpu_ctx *ctx);
  * on one host). */
 int cf1gpu_bin_distinct_counts(const cf1gpu_ctx *ctx, uint64_t *counts, size_t nbins);
 
+/* Exchange-based bin sharding: the alternative to cf1gpu_run_phases_1_4 for
+ * shard_count contexts (one per device) that all hold the whole input.  Each
+ * scans only its slice of the input, and the shards swap their super k-mer
+ * records once:
+ *   1. cf1gpu_xshard_scan: phase 1 over this shard's share of the minimizer
+ *      tiles; hist receives the share's 65,536-bucket histogram,
+ *      *n_records the share's super k-mer records.
+ *   2. caller: sum hist over the shards (an all-reduce).
+ *   3. cf1gpu_xshard_route: the partition of the summed histogram (the same on
+ *      every shard), then the share's records, each tagged with its bin, into
+ *      records[0 .. *n_records) grouped by owner shard (bin % shard_count):
+ *      counts[r] records for shard r, r < shard_count.
+ *   4. caller: send group r to shard r (an all-to-all).
+ *   5. cf1gpu_xshard_finish: phases 2-4 on the n records this shard received,
+ *      in any order.  Records of another shard's bin, or reaching past the
+ *      input, are refused (CF1GPU_ERR_INVALID_ARG).
+ * Afterwards the context holds its bins' results exactly as after a
+ * replicated-routing run (cf1gpu_bin_distinct_counts, cf1gpu_copy_states).
+ * The reference routes on one host (src/superkmer.rs:21-210); this split of
+ * its phase 1-2 work over devices has no counterpart there.  Buffers may be
+ * host memory or device memory of the context's device (cudaMemcpyDefault),
+ * so an NCCL all-reduce and all-to-all can run on them in place. */
+int cf1gpu_xshard_scan(cf1gpu_ctx *ctx, uint32_t *hist, uint64_t *n_records);
+int cf1gpu_xshard_route(cf1gpu_ctx *ctx, const uint32_t *hist, uint64_t *records, size_t records_cap,
+                        uint64_t *counts);
+int cf1gpu_xshard_finish(cf1gpu_ctx *ctx, const uint64_t *records, size_t n);
+
 /* The state vector words (src/state_vector.rs:7-71 layout); n_words must be
  * ceil(total_kmers / 12). */
 int cf1gpu_copy_states(cf1gpu_ctx *ctx, uint64_t *dst, size_t n_words);
