@@ -34,13 +34,16 @@ __global__ void bb_init_counts_kernel(const uint64_t *seg_off, const uint32_t *s
   if (b < nbins) cnt[b] = (sel == nullptr || sel[b]) ? seg_off[b + 1] - seg_off[b] : 0;
 }
 
-// Bits per key of a level: 8 at level 0, 2 after (gamma 2 as in ph::fmph,
-// src/mphf.rs:155-160).  The wide first level places ~88% of the keys
-// instead of ~61%, so a query -- and a warp of queries, which waits for its
-// deepest lane -- walks fewer levels, and the build marks fewer keys.  At
-// 2.5e9 keys it costs ~5.7 GB of HBM; 4 bits ran phases 1-4 3% slower, 16
-// bits 1% slower (its first level's passes outweigh the shorter probes).
-constexpr uint32_t BB_GAMMA0 = 8, BB_GAMMA = 2;
+// Bits per key of a level: 8 at every level (ph::fmph uses gamma 2,
+// src/mphf.rs:155-160).  A wide level places ~88% of its keys instead of
+// ~61%, so a query -- and a warp of queries, which waits for its deepest
+// lane -- walks fewer levels, and the build runs fewer.  At 2.7e9 keys the
+// first level costs ~6.1 GB of HBM and the rest ~0.8 GB.  Measured at 3.1
+// Gbp: 4 bits at level 0 ran phases 1-4 3% slower, 16 bits 1% slower (its
+// first level's passes outweigh the shorter probes); 8 bits after level 0
+// instead of 2 took the classification kernel from 50.9 to 46.3 ms and the
+// build from 21.8 to 18.1 ms (16 levels down to 10).
+constexpr uint32_t BB_GAMMA0 = 8, BB_GAMMA = 8;
 
 // Words of each bin's block at this level (gamma bits per key, at least one
 // word for a non-empty bin) and the level's totals {keys, words}.

@@ -2,10 +2,9 @@
 //
 // The key set is split into bins (phase 2); bin b owns slots
 // [dist_off[b], dist_off[b+1]).  Inside a bin a key's local slot comes from
-//   * BBHash (per bin): levels of bit arrays 8x (first level) then 2x the
-//     keys still unplaced (gamma 2 is ph::fmph's relative_level_size 200,
-//     src/mphf.rs:155-160); the first level where the key's bit is set gives
-//     the level rank; or
+//   * BBHash (per bin): levels of bit arrays 8x the keys still unplaced
+//     (ph::fmph's relative_level_size 200 would be 2x, src/mphf.rs:155-160);
+//     the first level where the key's bit is set gives the level rank; or
 //   * the learned index: a small MLP root picks a leaf, the leaf's linear
 //     model predicts the rank, and a search in [pred - err, pred + err] of the
 //     bin's sorted keys finds the exact rank, which is the local slot.
