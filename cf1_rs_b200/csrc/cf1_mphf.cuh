@@ -61,10 +61,10 @@ CF1_HD uint64_t bb_pos(uint64_t H, uint32_t l, uint32_t nwords) {
   return ((uint64_t)t * nwords) >> 26;
 }
 
-template <class KeyT>
-CF1_HD uint64_t bb_local_slot(const BBView &v, uint32_t bin, const KeyT &key) {
-  const uint64_t H = bb_key_hash(key);
-  for (uint32_t l = 0; l < v.levels; l++) {
+// Levels [l0, l1) of a key's walk (hash H): the first level whose bit is set
+// gives the local slot.
+CF1_HD uint64_t bb_walk(const BBView &v, uint32_t bin, uint64_t H, uint32_t l0, uint32_t l1) {
+  for (uint32_t l = l0; l < l1; l++) {
     const BBMeta mt = v.meta[(uint64_t)l * v.nbins + bin];
     if (mt.nwords == 0) return SLOT_NONE;
     const uint64_t pos = bb_pos(H, l, mt.nwords);
@@ -73,6 +73,11 @@ CF1_HD uint64_t bb_local_slot(const BBView &v, uint32_t bin, const KeyT &key) {
     if ((e.x >> bit) & 1) return (uint32_t)(mt.rank_adj + (uint32_t)e.y + (uint32_t)popc64(e.x & ((1ull << bit) - 1)));
   }
   return SLOT_NONE;
+}
+
+template <class KeyT>
+CF1_HD uint64_t bb_local_slot(const BBView &v, uint32_t bin, const KeyT &key) {
+  return bb_walk(v, bin, bb_key_hash(key), 0, v.levels);
 }
 
 // ---- learned index ----

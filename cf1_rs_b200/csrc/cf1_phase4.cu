@@ -46,13 +46,39 @@ CF1_D void state_join_cas(unsigned long long *states, uint64_t slot, uint32_t c,
   atomicOr(err, (uint32_t)DEV_CAS_LIMIT);
 }
 
+// BBHash probes past level 0, deferred: a warp's lanes whose key is not placed
+// at level 0 (~12%) park {hash, bin | contribution << 16} in the warp's queue,
+// and once 32 wait, 32 lanes walk the deeper levels together.  Walking them
+// in place would hold every lane of nearly every warp through level 1 (a
+// warp waits for its deepest lane) for a few lanes' sake.
+constexpr int CL_QCAP = 64;  // < 32 waiting + up to 32 parked by one step
+
 template <class KeyT, bool SIDESET>
 __global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a) {
+  __shared__ ulonglong2 deferred[CL_BLOCK / 32][CL_QCAP];
   const unsigned lane = lane_id();
   const uint64_t n_chunks = (a.n_rec + 31) / 32;
   uint64_t chunk = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   uint32_t retries = 0;
   const int k = a.k;
+  const bool defer = !a.mphf.learned;
+  ulonglong2 *dq = deferred[threadIdx.x >> 5];
+  uint32_t qn = 0;  // parked probes (the same in every lane)
+  auto apply = [&](uint64_t slot, uint32_t c) {
+    if (slot == SLOT_NONE) atomicOr(a.err, (uint32_t)DEV_MPHF_MISS);
+    else if (SIDESET) atomicOr(a.sides + (slot >> 2), sideset_lookup(c) << (8 * (uint32_t)(slot & 3)));
+    else state_join_cas(a.states, slot, c, a.err, retries);
+  };
+  auto drain = [&](uint32_t cnt) {  // lanes < cnt walk the last cnt parked probes
+    if (lane < cnt) {
+      const ulonglong2 e = dq[qn - cnt + lane];
+      const uint32_t bin = (uint32_t)e.y & 0xFFFFu;
+      const uint64_t local = bb_walk(a.mphf.bb, bin, e.x, 1, a.mphf.bb.levels);
+      apply(local == SLOT_NONE ? SLOT_NONE : a.mphf.dist_off[bin] + local, (uint32_t)(e.y >> 16));
+    }
+    qn -= cnt;
+    __syncwarp();
+  };
   for (;;) {
     if (a.queue) {
       uint32_t c = 0;
@@ -79,6 +105,8 @@ __global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a
       uint32_t oex = __shfl_sync(FULL, excl, lo);
       const uint32_t q = j - oex;  // k-mer q of the super k-mer
       uint64_t p = rec_pos(orec) + q;
+      bool park = false;  // level 0 did not place the key: defer its probe
+      uint64_t H = 0, pbin = 0;
       if (j < total && p + k > a.L) {
         atomicOr(a.err, (uint32_t)DEV_OVERFLOW);
       } else if (j < total) {
@@ -92,14 +120,27 @@ __global__ void __launch_bounds__(CL_BLOCK) classify_kernel(ClassifyArgs<KeyT> a
         uint32_t pb = hp ? base_at(a.W, p - 1) : 0;
         uint32_t nb = hn ? base_at(a.W, p + k) : 0;
         uint32_t c = contribution(fw, rc, hp, pb, hn, nb, k);
-        uint64_t slot = mphf_slot<KeyT, true>(a.mphf, bin, kmin(fw, rc));
-        if (slot == SLOT_NONE) atomicOr(a.err, (uint32_t)DEV_MPHF_MISS);
-        else if (SIDESET) atomicOr(a.sides + (slot >> 2), sideset_lookup(c) << (8 * (uint32_t)(slot & 3)));
-        else state_join_cas(a.states, slot, c, a.err, retries);
+        const KeyT key = kmin(fw, rc);
+        if (defer) {
+          H = bb_key_hash(key);
+          const uint64_t local = bb_walk(a.mphf.bb, bin, H, 0, 1);
+          if (local != SLOT_NONE) apply(a.mphf.dist_off[bin] + local, c);
+          else park = true, pbin = bin | c << 16;
+        } else {
+          apply(mphf_slot<KeyT, true>(a.mphf, bin, key), c);
+        }
+      }
+      if (defer) {
+        const uint32_t m = __ballot_sync(FULL, park);
+        if (park) dq[qn + __popc(m & lanemask_lt())] = make_ulonglong2(H, pbin);
+        qn += __popc(m);
+        __syncwarp();
+        if (qn >= 32) drain(32);
       }
     }
     if (!a.queue) break;
   }
+  if (qn) drain(qn);
   retries = warp_sum(retries);
   if (lane == 0 && retries) atomicAdd(a.cas_retries, (unsigned long long)retries);
 }
