@@ -93,6 +93,11 @@ struct cf1gpu_ctx {
 
   // results of the last run
   uint64_t n_super = 0, n_occ = 0, n_distinct = 0, n_bins_eff = 0, cas_retries = 0;
+  // BBHash form: the distinct keys wait in their sub-buckets (dist_kept, one
+  // of the sort buffers) until d_dist is asked for
+  bool dist_pending = false;
+  void *dist_kept = nullptr;
+  uint64_t dist_nsub = 0;
   int msd_bits = 0;        // top bits split on by the MSD sort (-1: LSD path ran)
   bool force_lsd = false;  // opts.sort_mode == 1
   uint32_t nbins = 0;

@@ -643,6 +643,14 @@ void subbuckets_bits(int bits, const uint64_t *seg_off, const uint32_t *tile_off
 }  // namespace
 
 template <class KeyT>
+void msd_compact(const KeyT *kept, uint64_t nsub, KeyT *dist, MsdScratch &sc, cudaStream_t s) {
+  if (!nsub) return;
+  cs_compact_kernel<KeyT><<<(unsigned)ceil_div(nsub * 32, 256), 256, 0, s>>>(
+      kept, sc.sb_off.as<const uint64_t>(), sc.cnt.as<const uint32_t>(), sc.out_off.as<const uint64_t>(), nsub, dist);
+  CF1_LAUNCH_CHECK();
+}
+
+template <class KeyT>
 int msd_prefix_bits(uint64_t max_bin_keys, bool sorted) {
   // Split on the key's own top bits (sorted), sub-buckets of the average bin
   // size run several times over it (the first bases of canonical k-mers are
@@ -658,7 +666,7 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted) {
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
                      KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted,
-                     const Level0Out *l0) {
+                     const Level0Out *l0, KeyT **kept) {
   // passes on the top P bits: P1 then P2 (P2 may be 0) -- of the key, or of
   // its hash when only distinct keys are wanted (64-bit keys)
   const bool hashed = !sorted && KOps<KeyT>::WORDS == 1;
@@ -720,10 +728,8 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
   if (h_over) return false;
   uint64_t *out_off = sc.out_off.get<uint64_t>(nsub + 1);
   exclusive_scan_u32(cnt, out_off, nsub, sc.scan_tmp, s);
-  if (nsub) {
-    cs_compact_kernel<KeyT><<<(unsigned)ceil_div(nsub * 32, 256), 256, 0, s>>>(T, sb_off, cnt, out_off, nsub, dist);
-    CF1_LAUNCH_CHECK();
-  }
+  if (kept) *kept = T;
+  if (dist) msd_compact<KeyT>(T, nsub, dist, sc, s);
   cs_bin_off_kernel<<<(unsigned)ceil_div(nbins + 1, 256), 256, 0, s>>>(out_off, nbins, 1ull << P, dist_off);
   CF1_LAUNCH_CHECK();
   return true;
@@ -732,7 +738,8 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
 #define CF1_INST(KT)                                                                                              \
   template int msd_prefix_bits<KT>(uint64_t, bool);                                                                     \
   template bool msd_sort_unique<KT>(KT *, KT *, uint64_t, const uint64_t *, uint32_t, int, int, KT *, uint64_t *, \
-                                    MsdScratch &, cudaStream_t, bool, const Level0Out *);
+                                    MsdScratch &, cudaStream_t, bool, const Level0Out *, KT **);              \
+  template void msd_compact<KT>(const KT *, uint64_t, KT *, MsdScratch &, cudaStream_t);
 CF1_INST(uint64_t)
 CF1_INST(Key2)
 #undef CF1_INST

@@ -36,9 +36,17 @@ struct Level0Out {
   uint32_t *err = nullptr;                 // set when a slice or a bin's room is too small
 };
 
+// With dist = nullptr the distinct keys stay where the dedup left them, at
+// the start of each sub-bucket's range of *kept (keys or alt), and
+// msd_compact writes dist later; dist_off is written either way.
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
                      KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted = true,
-                     const Level0Out *l0 = nullptr);
+                     const Level0Out *l0 = nullptr, KeyT **kept = nullptr);
+
+// The deferred copy: distinct keys of the last msd_sort_unique (nsub
+// sub-buckets, left in `kept`) to dist, bins in order.
+template <class KeyT>
+void msd_compact(const KeyT *kept, uint64_t nsub, KeyT *dist, MsdScratch &sc, cudaStream_t s);
 
 }  // namespace cf1

@@ -228,6 +228,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   const bool batched = c->opts.batched != 0;
   const uint32_t shards = c->opts.shard_count > 1 ? c->opts.shard_count : 1;
   c->nbins = B;
+  c->dist_pending = false;  // the sort buffers are about to be reused
   const uint64_t launches0 = step == Step::XFINISH ? c->x_launches0 : g_launches.load();
   // The learned index needs each bin's keys sorted; BBHash needs them
   // distinct (128-bit keys always take the sorted path).
@@ -479,7 +480,8 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   uint64_t *seg = c->d_seg.get<uint64_t>(B + 1);
   seg_gather_kernel<<<(unsigned)ceil_div(B + 1, 256), 256, 0, s>>>(kpre, rec_off, B, seg);
   CF1_LAUNCH_CHECK();
-  KeyT *dist = c->d_dist.get<KeyT>(NO + 1);
+  // the dense distinct-key array, allocated when a step writes it
+  auto dist_buf = [&]() { return c->d_dist.get<KeyT>(NO + 1); };
   uint64_t *dist_off = c->d_dist_off.get<uint64_t>(B + 1);
   std::vector<uint64_t> hseg(B + 1);
   CF1_CUDA(cudaMemcpyAsync(hseg.data(), seg, (B + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
@@ -501,7 +503,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
       if (tried != -2) expand_again();  // the previous try consumed the keys
       if (batched) CF1_CUDA(cudaMemsetAsync(&sm->queues[4], 0, sizeof(uint32_t), s));
       CF1_CUDA(cudaEventRecord(c->ev[10], s));
-      const bool ok = msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist, dist_off, be.msd, s, sorted);
+      const bool ok = msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist_buf(), dist_off, be.msd, s, sorted);
       CF1_CUDA(cudaEventRecord(c->ev[11], s));
       CF1_CUDA(cudaEventSynchronize(c->ev[11]));
       const double ms = elapsed(c->ev[10], c->ev[11]);
@@ -548,8 +550,12 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     l0.surv_cnt = scnt;
     l0.err = &sm->l0_err;
   }
-  bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist, dist_off, be.msd, s, sorted,
-                                              l0_fuse ? &l0 : nullptr);
+  // The BBHash form leaves the distinct keys in their sub-buckets (kept):
+  // nothing on the path reads them, so the dense copy waits until a
+  // verification or dump asks for it.
+  KeyT *kept = nullptr;
+  bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, l0_fuse ? nullptr : dist_buf(), dist_off,
+                                              be.msd, s, sorted, l0_fuse ? &l0 : nullptr, &kept);
   c->msd_bits = done ? P : -1;
   if (tune_now) {
     tuned.sk_tile = c->tune.sk_tile;
@@ -564,36 +570,49 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
       launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[5] : nullptr, &sm->err, pctas, s);
     }
     segmented_sort<KeyT>(keys, NO, seg, B, 2 * k, be.sort, s);
-    segmented_unique<KeyT>(keys, NO, seg, B, dist, dist_off, be.sort, s);
+    segmented_unique<KeyT>(keys, NO, seg, B, dist_buf(), dist_off, be.sort, s);
   }
+  KeyT *dist = c->d_dist.as<KeyT>();
   CF1_CUDA(cudaMemcpyAsync(&c->n_distinct, dist_off + B, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
   uint32_t l0_err = 1;
   if (l0_fuse) CF1_CUDA(cudaMemcpyAsync(&l0_err, &sm->l0_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaStreamSynchronize(s));
   const bool l0_ready = l0_fuse && done && l0_err == 0;
+  const uint64_t nsub = done && P >= 0 ? (uint64_t)B << P : 0;
+  if (l0_fuse && done && !l0_ready) {  // level 0 did not fit: the plain build reads the dense keys
+    dist = dist_buf();
+    msd_compact<KeyT>(kept, nsub, dist, be.msd, s);
+  }
+  c->dist_pending = l0_ready;
+  c->dist_kept = kept;
+  c->dist_nsub = nsub;
   CF1_CUDA(cudaEventRecord(c->ev[3], s));
 
   // ---- phase 3b: MPHF
-  // the sort's buffers (NO keys each) are free now: BBHash levels use them
+  // the sort's buffers (NO keys each) are free now: BBHash levels use them,
+  // except the one holding the kept keys, whose twin they share
   KeyT *ws1 = be.sort.alt.template as<KeyT>();
+  KeyT *twin = kept == keys ? ws1 : keys;
+  const uint64_t half = (NO + 1) / 2;
   if (c->opts.mphf_mode == CF1GPU_MPHF_LEARNED) {
     be.li.build(dist, dist_off, B, k, c->learned, s);
     be.bb.build(dist, dist_off, B, be.li.fallback_sel(), s, keys, ws1, NO + 1);
   } else if (l0_ready) {
     be.bb.build_from_level0(B, l0.woff, l0_words, reinterpret_cast<const KeyT *>(l0.surv), l0.surv_off,
-                            reinterpret_cast<const uint64_t *>(l0.surv_cnt), l0_room, s, keys, ws1, NO + 1);
+                            reinterpret_cast<const uint64_t *>(l0.surv_cnt), l0_room, s, twin, twin + half, half);
   } else {
     be.bb.build(dist, dist_off, B, nullptr, s, keys, ws1, NO + 1);
   }
   CF1_CUDA(cudaEventRecord(c->ev[4], s));
 
   // ---- phase 4: classification
-  // Side-set mode keeps one byte per vertex in the key buffer, which is free
-  // once the MPHF is built (12 * nwords <= n_distinct + 11 <= 8 * (NO + 1)).
+  // Side-set mode keeps one byte per vertex in a sort buffer, which is free
+  // once the MPHF is built (12 * nwords <= n_distinct + 11 <= 8 * (NO + 1)):
+  // the key buffer, or the twin of the kept keys.
   const uint64_t nwords = ceil_div(c->n_distinct, 12);
   const bool sideset = c->opts.state_update == 0;
   unsigned long long *states = c->d_states.get<unsigned long long>(nwords + 1);
-  uint32_t *sides = sideset ? reinterpret_cast<uint32_t *>(keys) : nullptr;
+  uint32_t *sides = sideset ? reinterpret_cast<uint32_t *>(c->dist_pending ? twin : keys) : nullptr;
   if (sideset) {
     CF1_CUDA(cudaMemsetAsync(sides, 0, nwords * 12, s));
     CF1_CUDA(cudaMemsetAsync(states + nwords, 0, sizeof(unsigned long long), s));
@@ -694,8 +713,18 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   st.ms_total = elapsed(c->ev[0], c->ev[7]) + p1_before;
 }
 
+// The dense distinct-key array of a run that left it for later.
+template <class KeyT>
+void ensure_dist(cf1gpu_ctx *c) {
+  if (!c->dist_pending) return;
+  msd_compact<KeyT>(static_cast<const KeyT *>(c->dist_kept), c->dist_nsub, c->d_dist.get<KeyT>(c->n_distinct + 1),
+                    backend<KeyT>(c).msd, c->stream);
+  c->dist_pending = false;
+}
+
 template <class KeyT>
 void dump_impl(cf1gpu_ctx *c, uint64_t *keys, uint8_t *states) {
+  ensure_dist<KeyT>(c);
   cudaStream_t s = c->stream;
   uint64_t n = c->n_distinct;
   uint64_t *dk = c->d_qout.get<uint64_t>(n * cf1::KOps<KeyT>::WORDS + 1);
@@ -708,6 +737,7 @@ void dump_impl(cf1gpu_ctx *c, uint64_t *keys, uint8_t *states) {
 
 template <class KeyT>
 void verify_impl(cf1gpu_ctx *c) {
+  ensure_dist<KeyT>(c);
   cudaStream_t s = c->stream;
   uint64_t n = c->n_distinct;
   Small *sm = c->d_small.get<Small>(1);
