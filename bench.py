@@ -392,7 +392,7 @@ def gpu_arm(args):
     # and one written per occurrence (state word RMW); MPHF probes excluded
     b4 = 0.25 * L + 64.0 * n_occ
     ach = b4 / (head["ms_classify_kernel"] / 1e3) / 1e9
-    roofline = {"kernel": "classify_kernel", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
+    roofline = {"kernel": "classify_defer_kernel" if head_name == "bbhash" else "classify_kernel", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "peak_kind": peak_kind,
                 "traffic": committed_traffic(args.workload, args.scale, head_name),
                 "algorithmic_bytes": b4}
