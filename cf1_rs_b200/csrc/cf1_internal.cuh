@@ -137,6 +137,12 @@ struct SuperkmerArgs {
   uint64_t rec_cap;
   uint32_t *err;
 };
+// The default k (31, with m = 15 and w = 17 by src/params.rs:221-228) gets a
+// minimizer scan with k, m and w as compile-time constants (phase 1 27.3 ->
+// 24.4 ms at 3.1 Gbp); other k run the same code with them read at run
+// time.  (The same for the classification and expansion kernels measured
+// slower or no faster: their register allocation changed.)
+constexpr int K_FIXED = 31, M_FIXED = 15, W_FIXED = 17;
 // Phase 1: minimizer histogram + unordered super k-mer list.
 void launch_superkmer_scan(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s);
 // Phase 2: route the list into per-bin ranges rec_off[0..num_bins] of records

@@ -84,7 +84,7 @@ __global__ void pack_kernel(const uint8_t *ascii, uint64_t L, uint64_t *W, uint6
 //      its slots with one atomic add).
 constexpr uint32_t SK_INVALID = 0xFFFFFFFFu;
 
-template <int BLOCK, int ITEMS>
+template <int BLOCK, int ITEMS, int KC>
 __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
   constexpr uint32_t T = BLOCK * ITEMS;
   extern __shared__ uint32_t dyn32[];
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_base;
   __shared__ uint32_t sm[BLOCK / 32];
-  const int k = a.k, m = a.m, w = a.w;
+  const int k = KC ? KC : a.k, m = KC ? M_FIXED : a.m, w = KC ? W_FIXED : a.w;
   const unsigned tid = threadIdx.x;
   const uint64_t NK = a.L - (uint64_t)k + 1;
   uint64_t tile = a.tile_begin + blockIdx.x;
@@ -233,10 +233,11 @@ __global__ void __launch_bounds__(BS_BLOCK) bin_scatter_kernel(const uint64_t *r
 void launch_sk(const SuperkmerArgs &a, int persistent_ctas, cudaStream_t s) {
   if (a.n_tiles <= a.tile_begin) return;
   size_t smem = 2 * (a.tile + 64) * sizeof(uint32_t);
+  const bool fixed = a.k == K_FIXED && a.m == M_FIXED && a.w == W_FIXED;
   switch (a.tile) {
 #define CF1_SK_CASE(IT)                                                                              \
   case SK_BLOCK * IT: {                                                                            \
-    auto kern = superkmer_kernel<SK_BLOCK, IT>;                                                    \
+    auto kern = fixed ? superkmer_kernel<SK_BLOCK, IT, K_FIXED> : superkmer_kernel<SK_BLOCK, IT, 0>; \
     CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
     unsigned grid = persistent_ctas ? persistent_grid(kern, SK_BLOCK, smem, persistent_ctas, a.n_tiles) \
                                     : (unsigned)(a.n_tiles - a.tile_begin);                        \
