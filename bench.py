@@ -78,6 +78,9 @@ def parse():
                    help="N > 1: scan 1/N of the input per rank and swap records, or route it all on every rank")
     p.add_argument("--tuner-cache", default=os.path.join(tempfile.gettempdir(), "cf1_tuner_cache.txt"),
                    help="autotuner cache file (first warm-up run of an input class measures; '' = off)")
+    p.add_argument("--verify", choices=["auto", "on", "off"], default="auto",
+                   help="after the timed steps, check every form's per-k-mer states on the whole workload against "
+                        "the CPU oracle (auto: on with 1 GPU)")
     return p.parse_args()
 
 
@@ -189,6 +192,39 @@ def run_cpu_baseline(x, k: int, sample_bp: int, threads: int):
     return len(r.states) / dt, dt, len(seq), len(r.states)
 
 
+def mem_available() -> int:
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    return int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    return 16 << 30
+
+
+def verify_forms(x, k: int, dumps: dict) -> dict:
+    """Every form's (canonical k-mer, state) dump of the whole workload
+    against the CPU oracle's classify.rs restatement, one hash partition of
+    the k-mers at a time (as many partitions as host memory needs).  Runs
+    after the timed region; the time it takes is reported, not timed."""
+    from oracle import oracle as o
+
+    threads = os.cpu_count() or 1
+    w = 8 if k <= 32 else 16
+    n_occ = max(1, len(x.seq))
+    need = 3 * w * n_occ  # collected keys, their sort buffer and the per-block lists of one partition
+    nparts = max(2, min(64, -(-need // max(1, int(0.4 * mem_available())))))
+    log = lambda m: print(f"[verify] {m}", file=sys.stderr, flush=True)
+    r = o.check_lists(k, x.seq, x.offsets, dumps, nparts=nparts, nthreads=threads, log=log)
+    forms = r.pop("lists")
+    r["oracle"] = "CPU restatement of src/classify.rs (method 0), keyed by canonical k-mer"
+    r["forms"] = forms
+    r["mismatches"] = sum(v["mismatches"] for v in forms.values())
+    r["n_listed"] = {f: v["n_listed"] for f, v in forms.items()}
+    return r
+
+
 def reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -281,6 +317,9 @@ def gpu_arm(args):
 
     wl = WORKLOADS[args.workload]
     k, bins = wl["k"], wl["bins"]
+    verify = args.verify == "on" or (args.verify == "auto" and world == 1)
+    if verify and world > 1:
+        verify = False  # each rank holds its own bins only; the check runs on one GPU
     # strong scaling over bin shards: rank r keeps the bins b with
     # b % world == r (cf1_rs_b200.sharded)
     x = cg.SynthInput(args.workload, scale=args.scale, seed=0)
@@ -321,13 +360,26 @@ def gpu_arm(args):
         barrier()
         if clock_info is None:
             clock_info = clocks.stop()
+        # after the timed steps (untimed): the form's (key, state) list for the
+        # oracle check, if host memory holds it beside the check's own needs
+        dump = None
+        if verify:
+            w_key = 8 if k <= 32 else 16
+            n_d = int(s["n_distinct"])
+            held = sum(v["dump"][0].nbytes + v["dump"][1].nbytes for v in forms.values() if v.get("dump"))
+            need = n_d * (w_key + 2) + len(x.seq) + 3 * w_key * len(x.seq) // 16 + (8 << 30)
+            if mem_available() > need:
+                dump = g.dump_states()
+            else:
+                print(f"[verify] {form}: not checked, host memory ({mem_available() >> 30} GiB free, "
+                      f"{held >> 30} GiB held) is short of {need >> 30} GiB", file=sys.stderr, flush=True)
         total_ms = maxall(sum(ms))
         distinct = sumall(s["n_distinct"])
         forms[form] = dict(
             value=distinct * args.steps / (total_ms / 1e3), ms_per_step=total_ms / args.steps,
             ms_classify_kernel=maxall(statistics.mean(ms_cls)), launches=launches, stats=s,
             phases_ms={k2: round(v, 3) for k2, v in phase.items()},
-            learned=g.learned_stats() if form == "learned" else None, ctx=g, be=be)
+            learned=g.learned_stats() if form == "learned" else None, ctx=g, be=be, dump=dump)
         if form != args.forms.split(",")[-1]:
             g.close()
             forms[form]["ctx"] = None
@@ -403,6 +455,11 @@ def gpu_arm(args):
     b14 = 0.25 * L + 2 * s_bins + 2 * w * n_occ + 2 * w * n_dist + b4
     pipe = {"achieved": b14 / (head["ms_per_step"] / 1e3) / 1e9, "unit": "GB/s", "algorithmic_bytes": b14,
             "frac": b14 / (head["ms_per_step"] / 1e3) / 1e9 / peaks["hbm_gbs"]}
+    parity = None
+    if verify:
+        dumps = {f: v.pop("dump") for f, v in forms.items() if v.get("dump") is not None}
+        parity = verify_forms(x, k, dumps) if dumps else {"checked": False, "why": "host memory"}
+        del dumps
     cpu = None
     if not args.no_cpu_baseline:
         rate, dt, nb, nd = run_cpu_baseline(x, k, int(args.cpu_sample_mbp * 1e6), os.cpu_count() or 1)
@@ -423,6 +480,7 @@ def gpu_arm(args):
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clock_info,
+        "parity": parity if parity is not None else {"checked": False},
         "gpu_launches": int(head["launches"]),
         "forms": {f: {"value": v["value"], "ms_per_step": v["ms_per_step"],
                       "ms_classify_kernel": v["ms_classify_kernel"], "phases_ms": v["phases_ms"],

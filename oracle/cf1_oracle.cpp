@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -298,13 +299,65 @@ struct AtomicStateVector {
 // distinct canonical k-mers onto [0, n) -- here the rank in sorted order.
 // Absent keys map to 0, like `unwrap_or(0)`.
 struct ExactMap {
-  std::vector<u128> keys;  // sorted, distinct
-  uint64_t hash(u128 key) const {
-    auto it = std::lower_bound(keys.begin(), keys.end(), key);
-    if (it == keys.end() || *it != key) return 0;
+  std::vector<u128> keys;        // sorted, distinct
+  std::vector<uint64_t> keys64;  // the same as 64-bit words (k <= 32, partitioned runs)
+  bool narrow = false;           // keys64 holds the keys
+  // Optional directory over the top bits of the keys: dir[b] = first key
+  // whose top bits are >= b, so a lookup searches one small stretch.
+  std::vector<uint64_t> dir;
+  int dir_shift = 0;
+  uint64_t size() const { return narrow ? keys64.size() : keys.size(); }
+  void build_dir(int key_bits) {
+    const int D = std::min(24, key_bits);
+    dir_shift = key_bits - D;
+    dir.assign(((size_t)1 << D) + 1, 0);
+    const uint64_t n = size();
+    uint64_t i = 0;
+    for (uint64_t b = 0; b < ((uint64_t)1 << D); b++) {
+      while (i < n && (uint64_t)((narrow ? (u128)keys64[i] : keys[i]) >> dir_shift) < b) i++;
+      dir[b] = i;
+    }
+    dir[(size_t)1 << D] = n;
+  }
+  // Rank of key in the sorted keys, ~0 when absent.
+  uint64_t rank(u128 key) const {
+    uint64_t lo = 0, hi = size();
+    if (!dir.empty()) {
+      const uint64_t b = (uint64_t)(key >> dir_shift);
+      if (b + 1 >= dir.size()) return ~0ull;
+      lo = dir[b];
+      hi = dir[b + 1];
+    }
+    if (narrow) {
+      auto it = std::lower_bound(keys64.begin() + lo, keys64.begin() + hi, (uint64_t)key);
+      if (it == keys64.begin() + hi || *it != (uint64_t)key) return ~0ull;
+      return (uint64_t)(it - keys64.begin());
+    }
+    auto it = std::lower_bound(keys.begin() + lo, keys.begin() + hi, key);
+    if (it == keys.begin() + hi || *it != key) return ~0ull;
     return (uint64_t)(it - keys.begin());
   }
+  uint64_t hash(u128 key) const {  // absent keys map to 0, like `unwrap_or(0)`
+    const uint64_t r = rank(key);
+    return r == ~0ull ? 0 : r;
+  }
 };
+
+// Partition of a canonical k-mer for checks too large to hold at once: a
+// 64-bit mix of its words scaled to [0, nparts).  The classifier's updates of
+// a k-mer touch only that k-mer's own slot (src/classify.rs:147-518 read and
+// CAS `mphf.hash(km.can)` and nothing else), so running it with every other
+// partition's k-mers skipped gives this partition's states exactly.
+inline uint64_t mix64(uint64_t x) {  // SplitMix64's finalizer
+  x ^= x >> 30; x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27; x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return x;
+}
+inline uint32_t part_of(u128 can, uint32_t nparts) {
+  const uint64_t h = mix64((uint64_t)can ^ mix64((uint64_t)(can >> 64) + 0x9E3779B97F4A7C15ull));
+  return (uint32_t)(((u128)h * nparts) >> 64);
+}
 
 // -------------------------------------------------------------- classify.rs ----
 struct DirectedKmer {  // src/directed_kmer.rs:12-64
@@ -325,7 +378,9 @@ struct Classifier {  // src/classify.rs:17-519
   const ExactMap &mphf;
   AtomicStateVector &states;
   int K;
+  uint32_t part = 0, nparts = 1;  // k-mers of other partitions are skipped
   Classifier(const KSpec &s, const ExactMap &m, AtomicStateVector &v) : ks(s), mphf(m), states(v), K(s.k) {}
+  bool skip(const DirectedKmer &km) const { return nparts > 1 && part_of(km.can, nparts) != part; }
 
   void process_substring(const uint8_t *seq, uint64_t seq_len, uint64_t left_end, uint64_t right_end) {  // 34-43
     uint64_t kmer_idx = left_end;
@@ -385,7 +440,30 @@ struct Classifier {  // src/classify.rs:17-519
     }
     return kmer_idx + K;
   }
+  // The step process_contiguous_subseq (65-141) takes for the valid window at
+  // kmer_idx: a run's first window by its two neighbours (isolated,
+  // rightmost, leftmost or internal), every later one internal while a next
+  // base exists (also across a chunk's right end, 111-122) and rightmost
+  // where the run ends.  All four cases follow from the window's own
+  // neighbours, so one window can be stepped on its own.
+  // fw: the window's k-mer, rc: its reverse complement.
+  void process_at(const uint8_t *seq, uint64_t seq_len, uint64_t kmer_idx, u128 fw, u128 rc) {
+    DirectedKmer curr;
+    curr.kmer = fw;
+    curr.rc = rc;
+    curr.can = canonical_with_rc(fw, rc);
+    curr.fwd = curr.kmer == curr.can;
+    const bool no_left = kmer_idx == 0 || T.placeholder[seq[kmer_idx - 1]];
+    const bool no_right = kmer_idx + K == seq_len || T.placeholder[seq[kmer_idx + K]];
+    if (no_left && no_right) { while (!process_isolated_kmer(curr)) {} return; }
+    if (no_right) { while (!process_rightmost_kmer(curr, seq[kmer_idx - 1])) {} return; }
+    DirectedKmer next = curr;
+    next.roll(ks, seq[kmer_idx + K]);
+    if (no_left) { while (!process_leftmost_kmer(curr, next, seq[kmer_idx + K])) {} return; }
+    while (!process_internal_kmer(curr, next, seq[kmer_idx - 1], seq[kmer_idx + K])) {}
+  }
   bool process_isolated_kmer(const DirectedKmer &km) {  // 147-158
+    if (skip(km)) return true;
     uint64_t idx = mphf.hash(km.can);
     uint8_t state = states.get(idx);
     if (is_dead_end(state)) return true;
@@ -400,6 +478,7 @@ struct Classifier {  // src/classify.rs:17-519
     return process_rightmost_kmer(km, prev_char);
   }
   bool process_leftmost_kmer(const DirectedKmer &km, const DirectedKmer &next, uint8_t next_char) {  // 179-285
+    if (skip(km)) return true;
     uint64_t idx = mphf.hash(km.can);
     uint8_t state = states.get(idx);
     if (is_dead_end(state)) return true;
@@ -428,6 +507,7 @@ struct Classifier {  // src/classify.rs:17-519
     return states.compare_and_swap(idx, old_state, ns);
   }
   bool process_rightmost_kmer(const DirectedKmer &km, uint8_t prev_char) {  // 287-383
+    if (skip(km)) return true;
     uint64_t idx = mphf.hash(km.can);
     uint8_t state = states.get(idx);
     if (is_dead_end(state)) return true;
@@ -455,6 +535,7 @@ struct Classifier {  // src/classify.rs:17-519
     return states.compare_and_swap(idx, old_state, ns);
   }
   bool process_internal_kmer(const DirectedKmer &km, const DirectedKmer &next, uint8_t prev_char, uint8_t next_char) {  // 385-518
+    if (skip(km)) return true;
     uint64_t idx = mphf.hash(km.can);
     uint8_t state = states.get(idx);
     if (is_dead_end(state)) return true;
@@ -629,7 +710,7 @@ void classify_direct(const KSpec &ks, const Input &in, int nthreads, Result &r) 
   double t0 = now_s();
   ExactMap map;
   map.keys.swap(r.keys);
-  AtomicStateVector states(map.keys.size());
+  AtomicStateVector states(map.size());
   Classifier cls(ks, map, states);
   uint64_t K = ks.k;
   struct Task { uint64_t rec, left, right; };
@@ -714,6 +795,298 @@ void classify_join(const KSpec &ks, const Input &in, int nthreads, Result &r) {
   r.state_words.assign((r.keys.size() + 11) / 12, 0);
   for (size_t i = 0; i < r.keys.size(); i++) r.state_words[i / 12] |= (uint64_t)r.states[i] << (5 * (i % 12));
   r.t_classify = now_s() - t0;
+}
+
+// ------------------------------------------ partitioned full-size run ----
+// The whole-run oracle holds every distinct k-mer at once; a 3.1 Gbp genome
+// has ~2.7e9 of them.  The partitioned run restates the same classify.rs
+// steps for the k-mers of one hash partition (part_of) at a time: it collects
+// the partition's distinct canonical k-mers (src/mphf.rs:323-363 semantics),
+// then applies the Classifier's step to every window of the partition.  The
+// union over all partitions is the whole run's (key, state) set.
+//
+// A PartIndex holds, for every base position of the input, the partition of
+// the canonical k-mer of the window starting there (NO_PART when the window
+// holds a placeholder or runs past its record), so that each partition's
+// pass reads one byte per position instead of rolling every k-mer again.
+const uint8_t NO_PART = 0xFF;
+
+// Work units: records in input order, records of CHUNK_KMERS bases or more cut
+// into CHUNK_KMERS-k-mer chunks (src/classify.rs:565-594).
+struct Task { uint64_t rec, left, right; };
+std::vector<Task> make_tasks(const Input &in, uint64_t K) {
+  std::vector<Task> tasks;
+  for (uint64_t i = 0; i < in.n_rec; i++) {
+    uint64_t len = in.off[i + 1] - in.off[i];
+    if (len < K) continue;
+    uint64_t right_end = len - K;
+    if (len < CHUNK_KMERS) tasks.push_back({i, 0, right_end});
+    else for (uint64_t left = 0; left <= right_end; left += CHUNK_KMERS)
+      tasks.push_back({i, left, std::min(left + CHUNK_KMERS - 1, right_end)});
+  }
+  return tasks;
+}
+
+// Sorts v and drops repeated keys: one split on the top 12 of key_bits bits,
+// then every bucket sorted on its own thread.
+template <class KW>
+void par_sort_unique(std::vector<KW> &v, int key_bits, int nthreads) {
+  const int BB = 12;
+  const uint32_t NB = 1u << BB;
+  const int sh = key_bits > BB ? key_bits - BB : 0;
+  auto bucket = [&](const KW &x) { return (uint32_t)((u128)x >> sh) & (NB - 1); };
+  const size_t n = v.size();
+  const int nt = std::max(1, nthreads);
+  const size_t chunk = (n + nt - 1) / nt;
+  std::vector<std::vector<uint64_t>> hist(nt, std::vector<uint64_t>(NB, 0));
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++) th.emplace_back([&, t] {
+    size_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+    for (size_t i = a; i < b; i++) hist[t][bucket(v[i])]++;
+  });
+  for (auto &x : th) x.join();
+  th.clear();
+  std::vector<uint64_t> bstart(NB + 1, 0);
+  uint64_t off = 0;
+  for (uint32_t d = 0; d < NB; d++) {
+    bstart[d] = off;
+    for (int t = 0; t < nt; t++) { uint64_t c = hist[t][d]; hist[t][d] = off; off += c; }
+  }
+  bstart[NB] = off;
+  std::vector<KW> tmp(n);
+  for (int t = 0; t < nt; t++) th.emplace_back([&, t] {
+    size_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+    auto &h = hist[t];
+    for (size_t i = a; i < b; i++) tmp[h[bucket(v[i])]++] = v[i];
+  });
+  for (auto &x : th) x.join();
+  std::vector<uint64_t> ucnt(NB + 1, 0);
+  parallel_for(NB, nt, [&](uint64_t d) {
+    KW *a = tmp.data() + bstart[d], *b = tmp.data() + bstart[d + 1];
+    std::sort(a, b);
+    ucnt[d] = (uint64_t)(std::unique(a, b) - a);
+  });
+  std::vector<uint64_t> uoff(NB + 1, 0);
+  for (uint32_t d = 0; d < NB; d++) uoff[d + 1] = uoff[d] + ucnt[d];
+  parallel_for(NB, nt, [&](uint64_t d) {
+    std::memcpy(v.data() + uoff[d], tmp.data() + bstart[d], ucnt[d] * sizeof(KW));
+  });
+  v.resize(uoff[NB]);
+}
+
+struct PartIndex {
+  int k;
+  uint32_t nparts;
+  Input in;
+  std::vector<uint8_t> id;  // per base position of in.seq
+  uint64_t n_occ = 0;       // valid windows
+  double t_build = 0;
+};
+
+PartIndex *build_part_index(int k, const Input &in, uint32_t nparts, int nthreads) {
+  KSpec ks(k);
+  const uint64_t K = k;
+  PartIndex *x = new PartIndex();
+  x->k = k;
+  x->nparts = nparts;
+  x->in = in;
+  double t0 = now_s();
+  const uint64_t total = in.off[in.n_rec] - in.off[0];
+  x->id.assign(in.off[in.n_rec], NO_PART);
+  (void)total;
+  const std::vector<Task> tasks = make_tasks(in, K);
+  std::atomic<uint64_t> occ(0);
+  parallel_for(tasks.size(), nthreads, [&](uint64_t t) {
+    const Task &tk = tasks[t];
+    const uint64_t base = in.off[tk.rec];
+    const uint8_t *s = in.seq + base;
+    uint64_t run = 0, c = 0;
+    u128 fw = 0, rc = 0;
+    const uint64_t end = tk.right + K;  // one past the last base of the last window
+    for (uint64_t p = tk.left; p < end; p++) {
+      if (T.placeholder[s[p]]) { run = 0; continue; }
+      run++;
+      if (run == K) { fw = from_ascii(ks, s, p + 1 - K); rc = reverse_complement(ks, fw); }
+      else if (run > K) roll_to_next_kmer(ks, fw, T.mapped[s[p]], rc);
+      if (run >= K) {
+        x->id[base + p + 1 - K] = (uint8_t)part_of(canonical_with_rc(fw, rc), nparts);
+        c++;
+      }
+    }
+    occ += c;
+  });
+  x->n_occ = occ.load();
+  x->t_build = now_s() - t0;
+  return x;
+}
+
+// A partition pass over the position blocks of the input: every valid window
+// gets its k-mer by rolling from the window before it (src/kmer.rs:240-262)
+// or, at the start of a run, by from_ascii; f(block, record, offset in the
+// record, k-mer, its reverse complement) is called for the partition's
+// windows.
+const uint64_t PBLK = 1u << 20;
+template <class F>
+void for_part_windows(const PartIndex &x, uint32_t part, int nthreads, F f) {
+  const Input &in = x.in;
+  const KSpec ks(x.k);
+  const uint64_t K = x.k;
+  const uint64_t n = in.off[in.n_rec];
+  parallel_for((n + PBLK - 1) / PBLK, nthreads, [&](uint64_t b) {
+    const uint64_t a = b * PBLK, e = std::min(n, a + PBLK);
+    uint64_t rec = (uint64_t)(std::upper_bound(in.off, in.off + in.n_rec + 1, a) - in.off) - 1;
+    const uint8_t *id = x.id.data();
+    bool have = false;  // the window before this one is valid and in the same record
+    u128 fw = 0, rc = 0;
+    for (uint64_t i = a; i < e; i++) {
+      const uint8_t pid = id[i];
+      if (pid == NO_PART) { have = false; continue; }
+      if (in.off[rec + 1] <= i) {
+        while (in.off[rec + 1] <= i) rec++;
+        have = false;
+      }
+      const uint8_t *s = in.seq + in.off[rec];
+      const uint64_t p = i - in.off[rec];
+      if (have) roll_to_next_kmer(ks, fw, T.mapped[s[p + K - 1]], rc);
+      else { fw = from_ascii(ks, s, p); rc = reverse_complement(ks, fw); }
+      have = true;
+      if (pid == part) f(b, rec, p, fw, rc);
+    }
+  });
+}
+
+struct PartResult {
+  int k;
+  uint32_t part, nparts;
+  ExactMap map;                 // the partition's sorted distinct canonical k-mers
+  std::vector<uint8_t> states;  // per key
+  uint64_t n_occ = 0;           // the partition's k-mer occurrences
+  double t_collect = 0, t_sort = 0, t_classify = 0;
+};
+
+template <class KW>
+void collect_part(const KSpec &ks, const PartIndex &x, uint32_t part, int nthreads, std::vector<KW> &all,
+                  uint64_t &n_occ) {
+  const uint64_t n = x.in.off[x.in.n_rec];
+  const uint64_t nb = (n + PBLK - 1) / PBLK;
+  std::vector<std::vector<KW>> per(nb);
+  (void)ks;
+  for_part_windows(x, part, nthreads, [&](uint64_t b, uint64_t, uint64_t, u128 fw, u128 rc) {
+    per[b].push_back((KW)canonical_with_rc(fw, rc));
+  });
+  std::vector<uint64_t> off(nb + 1, 0);
+  for (uint64_t b = 0; b < nb; b++) off[b + 1] = off[b] + per[b].size();
+  n_occ = off[nb];
+  all.resize(n_occ);
+  parallel_for(nb, nthreads, [&](uint64_t b) {
+    std::memcpy(all.data() + off[b], per[b].data(), per[b].size() * sizeof(KW));
+    std::vector<KW>().swap(per[b]);
+  });
+}
+
+PartResult *run_part(const PartIndex &x, uint32_t part, int nthreads) {
+  const int k = x.k;
+  KSpec ks(k);
+  PartResult *r = new PartResult();
+  r->k = k;
+  r->part = part;
+  r->nparts = x.nparts;
+  double t0 = now_s();
+  if (k <= 32) {
+    r->map.narrow = true;
+    collect_part<uint64_t>(ks, x, part, nthreads, r->map.keys64, r->n_occ);
+    double t1 = now_s();
+    r->t_collect = t1 - t0;
+    par_sort_unique(r->map.keys64, 2 * k, nthreads);
+    r->t_sort = now_s() - t1;
+  } else {
+    collect_part<u128>(ks, x, part, nthreads, r->map.keys, r->n_occ);
+    double t1 = now_s();
+    r->t_collect = t1 - t0;
+    par_sort_unique(r->map.keys, 2 * k, nthreads);
+    r->t_sort = now_s() - t1;
+  }
+  double t2 = now_s();
+  r->map.build_dir(2 * k);
+  AtomicStateVector states(r->map.size());
+  Classifier cls(ks, r->map, states);
+  cls.part = part;
+  cls.nparts = x.nparts;
+  for_part_windows(x, part, nthreads, [&](uint64_t, uint64_t rec, uint64_t p, u128 fw, u128 rc) {
+    cls.process_at(x.in.seq + x.in.off[rec], x.in.off[rec + 1] - x.in.off[rec], p, fw, rc);
+  });
+  r->states.resize(r->map.size());
+  parallel_for((r->map.size() + 4095) / 4096, nthreads, [&](uint64_t b) {
+    const uint64_t a = b * 4096, e = std::min<uint64_t>(r->map.size(), a + 4096);
+    for (uint64_t i = a; i < e; i++) r->states[i] = states.get(i);
+  });
+  r->t_classify = now_s() - t2;
+  return r;
+}
+
+// Partition of every key of a (key, state) list.
+void list_parts(const uint64_t *keys, uint64_t n, bool narrow, uint32_t nparts, int nthreads, uint8_t *ids) {
+  const uint64_t BLK = 1u << 16;
+  parallel_for((n + BLK - 1) / BLK, nthreads, [&](uint64_t b) {
+    const uint64_t a = b * BLK, e = std::min(n, a + BLK);
+    for (uint64_t i = a; i < e; i++) {
+      const u128 key = narrow ? (u128)keys[i] : (((u128)keys[2 * i + 1] << 64) | keys[2 * i]);
+      ids[i] = (uint8_t)part_of(key, nparts);
+    }
+  });
+}
+
+// Compares a (key, state) list -- the GPU path's dump, in any order, with the
+// partition of each key from list_parts -- with a partition's oracle result:
+// the list's keys of this partition are looked up in the oracle's sorted
+// keys.  out[0..9]: list keys in the partition, equal states, different
+// states, keys the oracle lacks, keys listed twice, oracle keys the list
+// lacks, then the first differing entry (key lo, key hi, list state, oracle
+// state; ~0 when there is none).
+void compare_part(const PartResult &r, const uint64_t *keys, const uint8_t *states, const uint8_t *ids, uint64_t n,
+                  int nthreads, uint64_t out[10]) {
+  const bool narrow = r.map.narrow;
+  const uint64_t m = r.map.size();
+  std::vector<std::atomic<uint8_t>> seen(m);
+  for (auto &x : seen) x.store(0, std::memory_order_relaxed);
+  std::atomic<uint64_t> in_part(0), equal(0), diff(0), extra(0), dup(0);
+  std::atomic<uint64_t> first_bad(~0ull);
+  const uint64_t BLK = 1u << 16;
+  parallel_for((n + BLK - 1) / BLK, nthreads, [&](uint64_t b) {
+    uint64_t c_in = 0, c_eq = 0, c_diff = 0, c_extra = 0, c_dup = 0, bad = ~0ull;
+    const uint64_t a = b * BLK, e = std::min(n, a + BLK);
+    for (uint64_t i = a; i < e; i++) {
+      if (ids[i] != r.part) continue;
+      const u128 key = narrow ? (u128)keys[i] : (((u128)keys[2 * i + 1] << 64) | keys[2 * i]);
+      c_in++;
+      const uint64_t idx = r.map.rank(key);
+      if (idx == ~0ull) { c_extra++; bad = std::min(bad, i); continue; }
+      if (seen[idx].exchange(1)) { c_dup++; bad = std::min(bad, i); }
+      if (states[i] == r.states[idx]) c_eq++;
+      else { c_diff++; bad = std::min(bad, i); }
+    }
+    in_part += c_in; equal += c_eq; diff += c_diff; extra += c_extra; dup += c_dup;
+    uint64_t cur = first_bad.load();
+    while (bad < cur && !first_bad.compare_exchange_weak(cur, bad)) {}
+  });
+  std::atomic<uint64_t> missing(0);
+  parallel_for((m + BLK - 1) / BLK, nthreads, [&](uint64_t b) {
+    uint64_t c = 0;
+    const uint64_t a = b * BLK, e = std::min(m, a + BLK);
+    for (uint64_t i = a; i < e; i++) c += seen[i].load(std::memory_order_relaxed) == 0;
+    missing += c;
+  });
+  out[0] = in_part; out[1] = equal; out[2] = diff; out[3] = extra; out[4] = dup; out[5] = missing;
+  out[6] = out[7] = out[8] = out[9] = ~0ull;
+  const uint64_t i = first_bad.load();
+  if (i != ~0ull) {
+    const u128 key = narrow ? (u128)keys[i] : (((u128)keys[2 * i + 1] << 64) | keys[2 * i]);
+    out[6] = (uint64_t)key;
+    out[7] = (uint64_t)(key >> 64);
+    out[8] = states[i];
+    const uint64_t idx = r.map.rank(key);
+    out[9] = idx == ~0ull ? ~0ull : r.states[idx];
+  }
 }
 
 // ------------------------------------------------------- binning spec ----
@@ -888,6 +1261,44 @@ void cfo_copy_short(void *h, uint64_t *idx, uint64_t *len) {
 }
 void cfo_times(void *h, double out3[3]) { Result *r = (Result *)h; out3[0] = r->t_keys; out3[1] = r->t_sort; out3[2] = r->t_classify; }
 
+// --- partitioned run (checks of inputs too large for cfo_run) ---
+void *cfo_part_index_new(int k, const uint8_t *seq, const uint64_t *rec_off, uint64_t n_rec, uint32_t nparts,
+                         int nthreads) {
+  if (k < 1 || k > 63 || (k % 2) == 0 || nparts == 0 || nparts >= NO_PART) return nullptr;
+  Input in{seq, rec_off, n_rec};
+  return build_part_index(k, in, nparts, nthreads);
+}
+void cfo_part_index_free(void *h) { delete (PartIndex *)h; }
+uint64_t cfo_part_index_n_occ(void *h) { return ((PartIndex *)h)->n_occ; }
+double cfo_part_index_seconds(void *h) { return ((PartIndex *)h)->t_build; }
+void *cfo_part_run(void *index, uint32_t part, int nthreads) {
+  PartIndex *x = (PartIndex *)index;
+  if (!x || part >= x->nparts) return nullptr;
+  return run_part(*x, part, nthreads);
+}
+void cfo_part_free(void *h) { delete (PartResult *)h; }
+uint64_t cfo_part_n_distinct(void *h) { return ((PartResult *)h)->map.size(); }
+uint64_t cfo_part_n_occ(void *h) { return ((PartResult *)h)->n_occ; }
+void cfo_part_times(void *h, double out3[3]) {
+  PartResult *r = (PartResult *)h;
+  out3[0] = r->t_collect; out3[1] = r->t_sort; out3[2] = r->t_classify;
+}
+void cfo_part_copy(void *h, uint64_t *keys, uint8_t *states) {  // keys as in cfo_copy_keys
+  PartResult *r = (PartResult *)h;
+  const uint64_t n = r->map.size();
+  if (r->map.narrow) std::memcpy(keys, r->map.keys64.data(), n * 8);
+  else for (uint64_t i = 0; i < n; i++) { keys[2 * i] = (uint64_t)r->map.keys[i]; keys[2 * i + 1] = (uint64_t)(r->map.keys[i] >> 64); }
+  std::memcpy(states, r->states.data(), n);
+}
+void cfo_list_parts(const uint64_t *keys, uint64_t n, int k, uint32_t nparts, int nthreads, uint8_t *ids) {
+  list_parts(keys, n, k <= 32, nparts, nthreads, ids);
+}
+void cfo_part_compare(void *h, const uint64_t *keys, const uint8_t *states, const uint8_t *ids, uint64_t n,
+                      int nthreads, uint64_t out[10]) {
+  compare_part(*(PartResult *)h, keys, states, ids, n, nthreads, out);
+}
+uint32_t cfo_part_of(const uint64_t key[2], uint32_t nparts) { return part_of(((u128)key[1] << 64) | key[0], nparts); }
+
 // --- binning spec ---
 int cfo_minimizer_len(int k) {  // src/params.rs:221-228
   int m = std::min(k / 2, 15);
@@ -935,6 +1346,64 @@ void cfo_mlp_grad(const float *params, const float *x, const float *t, uint64_t 
     }
   }
   *loss = l;
+}
+
+// The trained parameterisation of the learned-index root, in double
+// precision: q = knot logits theta[H], output weights w2[H], output bias b2.
+// Widths d = softmax(theta), knots t_j = sum_{i<j} d_i; unit j is
+// clamp((x - t_j) / d_j, 0, 1); y = b2 + sum_j w2_j unit_j; the loss is the
+// mean of (y - target)^2.  The gradient is taken with respect to d and t
+// directly (inside its ramp, d unit/d t_j = -1/d_j and d unit/d d_j =
+// -z/d_j with z = (x - t_j)/d_j), then carried through the knot sums and
+// the softmax Jacobian d_m (D_m - sum_j d_j D_j).
+double learned_loss_q(const double *q, const float *x, const float *tg, uint64_t n, double *grad) {
+  const int H = 16;
+  double mx = q[0];
+  for (int j = 1; j < H; j++) mx = std::max(mx, q[j]);
+  double d[H], t[H], s = 0;
+  for (int j = 0; j < H; j++) { d[j] = std::exp(q[j] - mx); s += d[j]; }
+  double acc = 0;
+  for (int j = 0; j < H; j++) { d[j] /= s; t[j] = acc; acc += d[j]; }
+  double dLdd[H] = {0}, dLdt[H] = {0}, dLdw2[H] = {0}, dLdb2 = 0, loss = 0;
+  for (uint64_t i = 0; i < n; i++) {
+    double z[H], u[H], y = q[2 * H];
+    for (int j = 0; j < H; j++) {
+      z[j] = ((double)x[i] - t[j]) / d[j];
+      u[j] = z[j] <= 0 ? 0 : (z[j] >= 1 ? 1 : z[j]);
+      y += q[H + j] * u[j];
+    }
+    const double e = y - (double)tg[i];
+    loss += e * e / (double)n;
+    const double dy = 2 * e / (double)n;
+    dLdb2 += dy;
+    for (int j = 0; j < H; j++) {
+      dLdw2[j] += dy * u[j];
+      if (z[j] > 0 && z[j] < 1) {
+        dLdt[j] += dy * q[H + j] * (-1.0 / d[j]);
+        dLdd[j] += dy * q[H + j] * (-z[j] / d[j]);
+      }
+    }
+  }
+  if (grad) {
+    double D[H];
+    for (int m = 0; m < H; m++) {
+      D[m] = dLdd[m];
+      for (int j = m + 1; j < H; j++) D[m] += dLdt[j];  // t_j = sum_{i<j} d_i
+    }
+    double dot = 0;
+    for (int j = 0; j < H; j++) dot += d[j] * D[j];
+    for (int m = 0; m < H; m++) grad[m] = d[m] * (D[m] - dot);
+    for (int j = 0; j < H; j++) grad[H + j] = dLdw2[j];
+    grad[2 * H] = dLdb2;
+  }
+  return loss;
+}
+
+void cfo_learned_grad_q(const double *q, const float *x, const float *t, uint64_t n, double *grad, double *loss) {
+  *loss = learned_loss_q(q, x, t, n, grad);
+}
+double cfo_learned_loss_q(const double *q, const float *x, const float *t, uint64_t n) {
+  return learned_loss_q(q, x, t, n, nullptr);
 }
 
 }  // extern "C"

@@ -91,6 +91,28 @@ def lib():
         f32p = C.POINTER(C.c_float)
         f64p = C.POINTER(C.c_double)
         L.cfo_mlp_grad.argtypes = [f32p, f32p, f32p, C.c_uint64, f64p, f64p]
+        L.cfo_learned_grad_q.argtypes = [f64p, f32p, f32p, C.c_uint64, f64p, f64p]
+        L.cfo_learned_loss_q.restype = C.c_double
+        L.cfo_learned_loss_q.argtypes = [f64p, f32p, f32p, C.c_uint64]
+        L.cfo_part_index_new.restype = C.c_void_p
+        L.cfo_part_index_new.argtypes = [C.c_int, u8p, u64p, C.c_uint64, C.c_uint32, C.c_int]
+        L.cfo_part_index_free.argtypes = [C.c_void_p]
+        L.cfo_part_index_n_occ.restype = C.c_uint64
+        L.cfo_part_index_n_occ.argtypes = [C.c_void_p]
+        L.cfo_part_index_seconds.restype = C.c_double
+        L.cfo_part_index_seconds.argtypes = [C.c_void_p]
+        L.cfo_part_run.restype = C.c_void_p
+        L.cfo_part_run.argtypes = [C.c_void_p, C.c_uint32, C.c_int]
+        L.cfo_part_free.argtypes = [C.c_void_p]
+        for name in ("cfo_part_n_distinct", "cfo_part_n_occ"):
+            getattr(L, name).restype = C.c_uint64
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.cfo_part_times.argtypes = [C.c_void_p, f64p]
+        L.cfo_part_copy.argtypes = [C.c_void_p, u64p, u8p]
+        L.cfo_list_parts.argtypes = [u64p, C.c_uint64, C.c_int, C.c_uint32, C.c_int, u8p]
+        L.cfo_part_compare.argtypes = [C.c_void_p, u64p, u8p, u8p, C.c_uint64, C.c_int, u64p]
+        L.cfo_part_of.restype = C.c_uint32
+        L.cfo_part_of.argtypes = [u64p, C.c_uint32]
         _lib = L
     return _lib
 
@@ -240,6 +262,164 @@ def run(k: int, seq: np.ndarray, rec_off: np.ndarray, nthreads: int = 1, method:
         L.cfo_free(h)
 
 
+# ---------------------------------------------------------------- partitioned run
+class PartIndex:
+    """Partition (part_of) of the canonical k-mer of every window of an input,
+    for classify.rs restatements that run one hash partition at a time
+    (cfo_part_index_new): inputs whose distinct k-mers do not fit in memory
+    at once.  Keeps references to the input arrays while it lives."""
+
+    def __init__(self, k: int, seq: np.ndarray, rec_off: np.ndarray, nparts: int, nthreads: int = 1):
+        self.k, self.nparts = k, nparts
+        self._seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        self._off = np.ascontiguousarray(rec_off, dtype=np.uint64)
+        self.h = lib().cfo_part_index_new(k, _p(self._seq, u8p), _p(self._off, u64p), len(self._off) - 1, nparts,
+                                          nthreads)
+        if not self.h:
+            raise ValueError(f"bad k ({k}) or partition count ({nparts})")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cfo_part_index_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    @property
+    def n_occ(self) -> int:
+        return lib().cfo_part_index_n_occ(self.h)
+
+    @property
+    def seconds(self) -> float:
+        return lib().cfo_part_index_seconds(self.h)
+
+
+class PartResult:
+    """Per-k-mer states of one hash partition (cfo_part_run): the classify.rs
+    step applied to every window whose canonical k-mer is in the partition.
+    The union over all partitions equals run(method=0)."""
+
+    def __init__(self, index: PartIndex, part: int, nthreads: int = 1):
+        self.k, self.part, self.nparts = index.k, part, index.nparts
+        self.h = lib().cfo_part_run(index.h, part, nthreads)
+        if not self.h:
+            raise ValueError(f"bad partition {part} of {index.nparts}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cfo_part_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    @property
+    def n_distinct(self) -> int:
+        return lib().cfo_part_n_distinct(self.h)
+
+    @property
+    def n_occ(self) -> int:
+        return lib().cfo_part_n_occ(self.h)
+
+    @property
+    def times(self):
+        t = (C.c_double * 3)()
+        lib().cfo_part_times(self.h, t)
+        return tuple(t)
+
+    def keys_states(self):
+        n = self.n_distinct
+        kw = 1 if self.k <= 32 else 2
+        keys = np.empty(n * kw, dtype=np.uint64)
+        st = np.empty(n, dtype=np.uint8)
+        lib().cfo_part_copy(self.h, _p(keys, u64p), _p(st, u8p))
+        return (keys if kw == 1 else keys.reshape(n, 2)), st
+
+    def compare(self, keys: np.ndarray, states: np.ndarray, ids: np.ndarray, nthreads: int = 1) -> dict:
+        """Lines a (key, state) list (any order; ids = list_parts of its keys)
+        up with this partition."""
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        states = np.ascontiguousarray(states, dtype=np.uint8)
+        ids = np.ascontiguousarray(ids, dtype=np.uint8)
+        out = np.zeros(10, dtype=np.uint64)
+        lib().cfo_part_compare(self.h, _p(keys, u64p), _p(states, u8p), _p(ids, u8p), len(states), nthreads,
+                               _p(out, u64p))
+        none = 2**64 - 1
+        first = None
+        if int(out[6]) != none or int(out[7]) != none:
+            first = {"key": int(out[6]) | (int(out[7]) << 64), "state": int(out[8]),
+                     "oracle_state": None if int(out[9]) == none else int(out[9])}
+        return {"in_part": int(out[0]), "equal": int(out[1]), "state_diff": int(out[2]), "extra": int(out[3]),
+                "dup": int(out[4]), "missing": int(out[5]), "first": first}
+
+
+def list_parts(keys: np.ndarray, k: int, nparts: int, nthreads: int = 1) -> np.ndarray:
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    n = keys.shape[0]
+    ids = np.empty(n, dtype=np.uint8)
+    lib().cfo_list_parts(_p(keys, u64p), n, k, nparts, nthreads, _p(ids, u8p))
+    return ids
+
+
+def part_of(key: int, nparts: int) -> int:
+    arr = (C.c_uint64 * 2)(key & (2**64 - 1), key >> 64)
+    return lib().cfo_part_of(arr, nparts)
+
+
+def check_lists(k: int, seq: np.ndarray, rec_off: np.ndarray, lists: dict, nparts: int = 8, nthreads: int = 1,
+                log=None) -> dict:
+    """Full check of (canonical k-mer, state) lists -- {name: (keys, states)},
+    each in any order -- against the classify.rs restatement, run one hash
+    partition at a time.  Per list, mismatches counts differing states,
+    listed keys the oracle lacks, keys listed twice and oracle keys the list
+    lacks."""
+    import time
+    t0 = time.perf_counter()
+    names = list(lists)
+    tot = {n: {"in_part": 0, "equal": 0, "state_diff": 0, "extra": 0, "dup": 0, "missing": 0} for n in names}
+    first = {n: None for n in names}
+    ids = {n: list_parts(lists[n][0], k, nparts, nthreads) for n in names}
+    n_dist = n_occ = 0
+    index = PartIndex(k, seq, rec_off, nparts, nthreads)
+    try:
+        for p in range(nparts):
+            r = PartResult(index, p, nthreads)
+            try:
+                n_dist += r.n_distinct
+                n_occ += r.n_occ
+                for n in names:
+                    c = r.compare(lists[n][0], lists[n][1], ids[n], nthreads)
+                    for key in tot[n]:
+                        tot[n][key] += c[key]
+                    if first[n] is None and c["first"] is not None:
+                        first[n] = c["first"]
+                if log:
+                    log(f"partition {p + 1}/{nparts}: {r.n_distinct} distinct, "
+                        f"collect/sort/classify {[round(t, 1) for t in r.times]} s")
+            finally:
+                r.close()
+    finally:
+        index.close()
+    out = {"checked": True, "method": "classify.rs restatement, hash-partitioned", "nparts": nparts,
+           "n_distinct": n_dist, "n_occ": n_occ, "seconds": round(time.perf_counter() - t0, 1),
+           "threads": nthreads, "lists": {}}
+    for n in names:
+        t = tot[n]
+        out["lists"][n] = {"n_listed": int(len(lists[n][1])),
+                           "mismatches": t["state_diff"] + t["extra"] + t["dup"] + t["missing"],
+                           **{key: t[key] for key in ("state_diff", "extra", "dup", "missing")},
+                           "first_mismatch": first[n]}
+    return out
+
+
+def check_states(k: int, seq: np.ndarray, rec_off: np.ndarray, keys: np.ndarray, states: np.ndarray,
+                 nparts: int = 8, nthreads: int = 1, log=None) -> dict:
+    """check_lists for one list: the result's counts at the top level."""
+    r = check_lists(k, seq, rec_off, {"list": (keys, states)}, nparts, nthreads, log)
+    one = r.pop("lists")["list"]
+    r.update(one)
+    return r
+
+
 # ---------------------------------------------------------------- binning spec
 def minimizer_len(k: int) -> int:
     return lib().cfo_minimizer_len(k)
@@ -275,6 +455,28 @@ def mlp_grad(params: np.ndarray, x: np.ndarray, t: np.ndarray):
     lib().cfo_mlp_grad(_p(params, C.POINTER(C.c_float)), _p(x, C.POINTER(C.c_float)), _p(t, C.POINTER(C.c_float)),
                        len(x), _p(g, C.POINTER(C.c_double)), C.byref(loss))
     return loss.value, g
+
+
+def learned_grad_q(q: np.ndarray, x: np.ndarray, t: np.ndarray):
+    """(loss, dL/dq) of the learned-index root in its trained
+    parameterisation (knot logits, output weights, output bias), in double
+    precision."""
+    q = np.ascontiguousarray(q, np.float64)
+    x = np.ascontiguousarray(x, np.float32)
+    t = np.ascontiguousarray(t, np.float32)
+    g = np.zeros(len(q), np.float64)
+    loss = C.c_double()
+    lib().cfo_learned_grad_q(_p(q, C.POINTER(C.c_double)), _p(x, C.POINTER(C.c_float)), _p(t, C.POINTER(C.c_float)),
+                             len(x), _p(g, C.POINTER(C.c_double)), C.byref(loss))
+    return loss.value, g
+
+
+def learned_loss_q(q: np.ndarray, x: np.ndarray, t: np.ndarray) -> float:
+    q = np.ascontiguousarray(q, np.float64)
+    x = np.ascontiguousarray(x, np.float32)
+    t = np.ascontiguousarray(t, np.float32)
+    return lib().cfo_learned_loss_q(_p(q, C.POINTER(C.c_double)), _p(x, C.POINTER(C.c_float)),
+                                    _p(t, C.POINTER(C.c_float)), len(x))
 
 
 def concat_records(records, sep: bytes = b"N"):
