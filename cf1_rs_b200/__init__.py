@@ -72,7 +72,7 @@ EXPORTED = [
     "cf1gpu_get_stats",
     "cf1gpu_total_kmers", "cf1gpu_bin_distinct_counts", "cf1gpu_copy_states", "cf1gpu_query", "cf1gpu_dump_states", "cf1gpu_verify_bijection",
     "cf1gpu_short_seq_count", "cf1gpu_short_seq", "cf1gpu_export_mphf", "cf1gpu_export_bin", "cf1gpu_mphf_host_query",
-    "cf1gpu_learned_stats", "cf1gpu_learned_grad", "cf1gpu_last_error", "cf1gpu_destroy", "cf1gpu_version",
+    "cf1gpu_learned_stats", "cf1gpu_learned_grad", "cf1gpu_learned_grad_q", "cf1gpu_last_error", "cf1gpu_destroy", "cf1gpu_version",
     "cf1gpu_distinct_kmers_noalloc", "cf1gpu_xshard_scan", "cf1gpu_xshard_route", "cf1gpu_xshard_finish",
 ]
 
@@ -112,6 +112,7 @@ def lib():
     L.cf1gpu_export_bin.argtypes = [vp, C.c_uint32, u8p, C.POINTER(C.c_size_t)]
     L.cf1gpu_learned_stats.argtypes = [vp, C.POINTER(C.c_double)]
     L.cf1gpu_learned_grad.argtypes = [C.c_int, f32p, f32p, f32p, C.c_size_t, f32p, f32p]
+    L.cf1gpu_learned_grad_q.argtypes = [C.c_int, f32p, f32p, f32p, C.c_size_t, f32p, f32p]
     L.cf1gpu_last_error.argtypes = [vp]
     L.cf1gpu_last_error.restype = C.c_char_p
     L.cf1gpu_destroy.argtypes = [vp]
@@ -152,6 +153,21 @@ def learned_grad(params: np.ndarray, x: np.ndarray, t: np.ndarray, device: int =
     loss = C.c_float()
     st = lib().cf1gpu_learned_grad(device, _p(params, f32p), _p(x, f32p), _p(t, f32p), len(x), _p(g, f32p),
                                    C.byref(loss))
+    if st != OK:
+        raise Cf1Error(st, lib().cf1gpu_last_error(None).decode())
+    return float(loss.value), g
+
+
+def learned_grad_q(q: np.ndarray, x: np.ndarray, t: np.ndarray, device: int = 0):
+    """(loss, dL/dq) of one learned-index training step on the GPU: q = knot
+    logits[16], output weights[16], output bias (cf1gpu_learned_grad_q)."""
+    q = np.ascontiguousarray(q, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    t = np.ascontiguousarray(t, np.float32)
+    g = np.zeros(len(q), np.float32)
+    loss = C.c_float()
+    st = lib().cf1gpu_learned_grad_q(device, _p(q, f32p), _p(x, f32p), _p(t, f32p), len(x), _p(g, f32p),
+                                     C.byref(loss))
     if st != OK:
         raise Cf1Error(st, lib().cf1gpu_last_error(None).decode())
     return float(loss.value), g

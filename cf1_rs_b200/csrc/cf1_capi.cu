@@ -326,6 +326,19 @@ int cf1gpu_learned_stats(const cf1gpu_ctx *c, double out5[5]) {
   return CF1GPU_OK;
 }
 
+int cf1gpu_learned_grad_q(int device, const float *q, const float *x, const float *t, size_t n, float *grad_q,
+                          float *loss) {
+  if (!q || !grad_q || !loss || (n && (!x || !t))) return CF1GPU_ERR_INVALID_ARG;
+  try {
+    CF1_CUDA(cudaSetDevice(device));
+    cf1::learned_grad_q_host(q, x, t, n, grad_q, loss);
+    return CF1GPU_OK;
+  } catch (const cf1::Error &e) {
+    g_create_error = e.what();
+    return e.status;
+  }
+}
+
 int cf1gpu_learned_grad(int device, const float *params, const float *x, const float *t, size_t n, float *grad,
                         float *loss) {
   if (!params || !grad || !loss || (n && (!x || !t))) return CF1GPU_ERR_INVALID_ARG;

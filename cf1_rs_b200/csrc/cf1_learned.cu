@@ -429,6 +429,42 @@ __global__ void __launch_bounds__(LT_BLOCK) li_grad_kernel(const float *params, 
   }
 }
 
+// One training step's gradient with respect to the trained parameters Q:
+// the same derive_params, mlp_accumulate, reduce_grads and grad_q calls
+// li_train_kernel makes before its Adam update, over n given samples.
+__global__ void __launch_bounds__(LT_BLOCK) li_grad_q_kernel(const float *q, const float *x, const float *t,
+                                                            uint32_t n, float *gq_out, float *loss_out) {
+  __shared__ float P[LI_NPARAM], Q[LI_NQ], GQ[LI_NQ], sd[H], stk[H];
+  __shared__ float red[LT_NW][LI_NPARAM + 1];
+  const unsigned tid = threadIdx.x;
+  if (tid < LI_NQ) Q[tid] = q[tid];
+  __syncthreads();
+  if (tid == 0) derive_params(Q, P, sd, stk);
+  __syncthreads();
+  float g[LI_NPARAM];
+#pragma unroll
+  for (int p = 0; p < LI_NPARAM; p++) g[p] = 0.f;
+  float loss = 0.f;
+  const float scale = n ? 1.f / (float)n : 0.f;
+  for (uint32_t i = tid; i < n; i += LT_BLOCK) mlp_accumulate(P, x[i], t[i], scale, g, loss);
+  reduce_grads(g, loss, red);
+  __syncthreads();
+  if (tid == 0) {
+    float G[LI_NPARAM];
+    for (int p = 0; p < LI_NPARAM; p++) {
+      float v = 0.f;
+      for (int w = 0; w < LT_NW; w++) v += red[w][p];
+      G[p] = v;
+    }
+    grad_q(G, sd, stk, GQ);
+    float l = 0.f;
+    for (int w = 0; w < LT_NW; w++) l += red[w][LI_NPARAM];
+    *loss_out = l;
+  }
+  __syncthreads();
+  if (tid < LI_NQ) gq_out[tid] = GQ[tid];
+}
+
 }  // namespace
 
 template <class KeyT>
@@ -564,6 +600,25 @@ void learned_grad_host(const float *params, const float *x, const float *t, size
   CF1_CUDA(cudaMemcpy(out, g, (LI_NPARAM + 1) * 4, cudaMemcpyDeviceToHost));
   std::memcpy(grad, out, LI_NPARAM * 4);
   *loss = out[LI_NPARAM];
+}
+
+void learned_grad_q_host(const float *q, const float *x, const float *t, size_t n, float *grad_q, float *loss) {
+  DevBuf dq, dx, dt, dg;
+  float *qq = dq.get<float>(LI_NQ + 1);
+  float *xx = dx.get<float>(n + 1);
+  float *tt = dt.get<float>(n + 1);
+  float *g = dg.get<float>(LI_NQ + 1);
+  CF1_CUDA(cudaMemcpy(qq, q, LI_NQ * 4, cudaMemcpyHostToDevice));
+  if (n) {
+    CF1_CUDA(cudaMemcpy(xx, x, n * 4, cudaMemcpyHostToDevice));
+    CF1_CUDA(cudaMemcpy(tt, t, n * 4, cudaMemcpyHostToDevice));
+  }
+  li_grad_q_kernel<<<1, LT_BLOCK>>>(qq, xx, tt, (uint32_t)n, g, g + LI_NQ);
+  CF1_LAUNCH_CHECK();
+  float out[LI_NQ + 1];
+  CF1_CUDA(cudaMemcpy(out, g, (LI_NQ + 1) * 4, cudaMemcpyDeviceToHost));
+  std::memcpy(grad_q, out, LI_NQ * 4);
+  *loss = out[LI_NQ];
 }
 
 }  // namespace cf1

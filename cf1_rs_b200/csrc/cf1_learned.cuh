@@ -46,5 +46,7 @@ struct LearnedBuild {
 // Full-batch MSE loss and gradient of the root MLP on the device (the same
 // code the training kernel runs).  params: LI_NPARAM floats.  Host pointers.
 void learned_grad_host(const float *params, const float *x, const float *t, size_t n, float *grad, float *loss);
+// dL/dQ of one training step (Q = knot logits[16], w2[16], b2), on the current device.
+void learned_grad_q_host(const float *q, const float *x, const float *t, size_t n, float *grad_q, float *loss);
 
 }  // namespace cf1

@@ -252,6 +252,17 @@ int cf1gpu_learned_stats(const cf1gpu_ctx *ctx, double out5[5]);
 int cf1gpu_learned_grad(int device, const float *params, const float *x, const float *t, size_t n, float *grad,
                         float *loss);
 
+/* Gradient the learned-index trainer applies: dL/dq of one training step for
+ * the trained parameters q = knot logits theta[16], output weights w2[16],
+ * output bias b2 (33 floats).  The first layer is derived from the knots --
+ * widths d = softmax(theta), knots t_j = d_0 + ... + d_{j-1}, w1_j = 1/d_j,
+ * b1_j = -t_j/d_j -- so grad_q carries the chain rule through the softmax and
+ * the knot sums on top of cf1gpu_learned_grad's dL/dP.  Same loss (mean
+ * squared error over the n samples (x_i, t_i)).  Diagnostic: no counterpart in
+ * the reference (its MPHF has no trained part, src/mphf.rs:155-160). */
+int cf1gpu_learned_grad_q(int device, const float *q, const float *x, const float *t, size_t n, float *grad_q,
+                          float *loss);
+
 /* Distinct canonical k-mers of one record, for callers that must not
  * allocate device memory.  No counterpart in the reference (it has no
  * device memory at all): this exists for host applications that own the
@@ -266,8 +277,10 @@ int cf1gpu_learned_grad(int device, const float *params, const float *x, const f
  * len - k + 1; receives the distinct canonical k-mers of the record's
  * placeholder-free windows, ascending (the phase-3 key set of
  * src/mphf.rs:323-363 for this record).  d_n_out: device u64, their count.
- * Work is queued on `stream` (a cudaStream_t, NULL = default stream);
- * outputs are valid once the stream has run it.
+ * Work is queued on `stream` (a cudaStream_t, NULL = the default stream
+ * of `device`); a stream must belong to `device` -- the call makes `device`
+ * current before launching, and a stream of another device returns
+ * CF1GPU_ERR_INVALID_ARG.  Outputs are valid once the stream has run it.
  *
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with the device current; make that first call

@@ -358,6 +358,27 @@ def test_learned_gradients_match_cpu():
         assert np.abs(grad_g - grad_c).max() <= 1e-4 * scale
 
 
+def test_learned_grad_q_matches_cpu():
+    """The gradient the trainer applies -- through the softmax knot widths,
+    w1 = 1/d and b1 = -t/d -- against the double-precision oracle."""
+    rng = np.random.default_rng(3)
+    for trial in range(8):
+        if trial == 0:  # the trainer's starting point: the identity root
+            q = np.concatenate([np.zeros(16), np.full(16, 1 / 16), [0.0]])
+        else:
+            q = np.concatenate([rng.normal(0, 0.8, 16), np.abs(rng.normal(1 / 16, 0.05, 16)), [rng.normal(0, 0.1)]])
+        q = q.astype(np.float32)
+        n = int(rng.integers(1, 4097))
+        x = rng.random(n).astype(np.float32)
+        t = np.sort(rng.random(n)).astype(np.float32)
+        loss_g, grad_g = cg.learned_grad_q(q, x, t)
+        loss_c, grad_c = o.learned_grad_q(q.astype(np.float64), x, t)
+        scale = max(1e-6, float(np.abs(grad_c).max()))
+        assert abs(loss_g - loss_c) <= 1e-4 * max(1.0, loss_c)
+        # fp32 device arithmetic vs the fp64 oracle: 1e-4 of the gradient scale, logits included
+        assert np.abs(grad_g - grad_c).max() <= 1e-4 * scale, (trial, np.abs(grad_g - grad_c).argmax())
+
+
 def test_learned_network_gain():
     """The trained root shrinks the search windows of the index without it."""
     x = cg.SynthInput(5, scale=0.005)
