@@ -37,6 +37,8 @@ constexpr uint32_t NA_TILE = NA_BLOCK * NA_ITEMS;            // 2048 keys
 constexpr uint32_t NA_MAX_TILES = NA_MAX_BASES / NA_TILE;     // 512
 constexpr uint32_t NA_DIGITS = 256;
 constexpr int NA_NW = NA_BLOCK / 32;
+// The histogram and scatter kernels index per-digit arrays by thread.
+static_assert(NA_BLOCK == (int)NA_DIGITS, "one thread per radix digit");
 
 // Scratch layout (byte offsets).
 constexpr size_t NA_KEYS = 0;                                          // u64 [NA_MAX_BASES]
@@ -92,11 +94,12 @@ __global__ void na_extract_kernel(const uint8_t *seq, uint64_t len, int k, uint6
   if (ok) keys[base + __popc(m & lanemask_lt())] = can;
 }
 
-// Per tile digit counts, digit-major with a fixed stride of NA_MAX_TILES.
-// Launched over all NA_MAX_TILES tiles: tiles past the key count write zeros,
-// so nothing a previous call left in the array reaches the scan.
+// Per tile digit counts, digit-major (digit d of tile t at d * ntiles + t).
+// Launched over all ntiles tiles of the call's largest possible key count:
+// tiles past the actual count write zeros, so every entry the scan reads was
+// written by this call and nothing a previous call left reaches it.
 __global__ void __launch_bounds__(NA_BLOCK) na_hist_kernel(const uint64_t *keys, const uint32_t *count, int shift,
-                                                           uint32_t *H) {
+                                                           uint32_t ntiles, uint32_t *H) {
   __shared__ uint32_t h[NA_DIGITS];
   const uint32_t t = blockIdx.x, n = *count;
   h[threadIdx.x] = 0;
@@ -104,7 +107,7 @@ __global__ void __launch_bounds__(NA_BLOCK) na_hist_kernel(const uint64_t *keys,
   uint64_t start = (uint64_t)t * NA_TILE, end = start + NA_TILE < n ? start + NA_TILE : n;
   for (uint64_t i = start + threadIdx.x; i < end; i += NA_BLOCK) atomicAdd(&h[(keys[i] >> shift) & 0xFF], 1u);
   __syncthreads();
-  H[threadIdx.x * NA_MAX_TILES + t] = h[threadIdx.x];
+  H[threadIdx.x * ntiles + t] = h[threadIdx.x];
 }
 
 // One CTA: exclusive scan of n u32 values (n <= NA_DIGITS * NA_MAX_TILES).
@@ -124,7 +127,7 @@ __global__ void __launch_bounds__(1024) na_scan_kernel(const uint32_t *in, uint3
 // Stable scatter of one tile (round-major order, warp ranks by match_any,
 // per (round, warp, digit) counts turned into offsets per digit).
 __global__ void __launch_bounds__(NA_BLOCK) na_scatter_kernel(const uint64_t *in, uint64_t *out, const uint32_t *count,
-                                                              int shift, const uint32_t *Hs) {
+                                                              int shift, uint32_t ntiles, const uint32_t *Hs) {
   __shared__ uint16_t cnt[NA_ITEMS * NA_NW * NA_DIGITS];
   __shared__ uint32_t s_base[NA_DIGITS];
   const uint32_t t = blockIdx.x, n = *count;
@@ -134,7 +137,7 @@ __global__ void __launch_bounds__(NA_BLOCK) na_scatter_kernel(const uint64_t *in
   uint64_t end = start + NA_TILE < n ? start + NA_TILE : n;
   uint32_t *c32 = reinterpret_cast<uint32_t *>(cnt);
   for (uint32_t i = tid; i < NA_ITEMS * NA_NW * NA_DIGITS / 2; i += NA_BLOCK) c32[i] = 0;
-  s_base[tid] = Hs[tid * NA_MAX_TILES + t];
+  s_base[tid] = Hs[tid * ntiles + t];
   __syncthreads();
   uint64_t key[NA_ITEMS];
   uint32_t dg[NA_ITEMS], wr[NA_ITEMS];
@@ -215,6 +218,13 @@ extern "C" int cf1gpu_distinct_kmers_noalloc(int device, uint32_t k, const uint8
   uint64_t max_keys = len >= k ? len - k + 1 : 0;
   if ((len && !d_seq) || !d_keys_out || !d_n_out || out_cap < max_keys) return CF1GPU_ERR_INVALID_ARG;
   if (device < 0 || device >= 64) return CF1GPU_ERR_INVALID_ARG;
+  (void)cudaGetLastError();  // an earlier call's error is not this call's
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (s) {  // the work goes to `device`: a stream of another device is refused
+    int sdev = -1;
+    if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) return CF1GPU_ERR_INVALID_ARG;
+    if (sdev != device) return CF1GPU_ERR_INVALID_ARG;
+  }
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
   if (cudaSetDevice(device) != cudaSuccess) return CF1GPU_ERR_CUDA;
@@ -231,7 +241,6 @@ extern "C" int cf1gpu_distinct_kmers_noalloc(int device, uint32_t k, const uint8
     }
     base = g_addr[device];
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   Scratch sc = carve(static_cast<unsigned char *>(base));
   uint32_t ntiles = (uint32_t)((max_keys + NA_TILE - 1) / NA_TILE);
   cudaError_t e = cudaMemsetAsync(sc.count, 0, sizeof(uint32_t), s);
@@ -239,9 +248,9 @@ extern "C" int cf1gpu_distinct_kmers_noalloc(int device, uint32_t k, const uint8
     na_extract_kernel<<<(unsigned)((max_keys + 255) / 256), 256, 0, s>>>(d_seq, len, (int)k, sc.keys, sc.count);
     uint64_t *src = sc.keys, *dst = sc.alt;
     for (int shift = 0; shift < 2 * (int)k; shift += 8) {
-      na_hist_kernel<<<NA_MAX_TILES, NA_BLOCK, 0, s>>>(src, sc.count, shift, sc.hist);
-      na_scan_kernel<<<1, 1024, 0, s>>>(sc.hist, sc.hscan, NA_HENTRIES);
-      na_scatter_kernel<<<ntiles, NA_BLOCK, 0, s>>>(src, dst, sc.count, shift, sc.hscan);
+      na_hist_kernel<<<ntiles, NA_BLOCK, 0, s>>>(src, sc.count, shift, ntiles, sc.hist);
+      na_scan_kernel<<<1, 1024, 0, s>>>(sc.hist, sc.hscan, NA_DIGITS * ntiles);
+      na_scatter_kernel<<<ntiles, NA_BLOCK, 0, s>>>(src, dst, sc.count, shift, ntiles, sc.hscan);
       uint64_t *t = src;
       src = dst;
       dst = t;

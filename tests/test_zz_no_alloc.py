@@ -52,8 +52,10 @@ def test_noalloc_matches_regular_path_twice_in_a_row():
     # caller-owned output buffers, sized for the largest record
     out = torch.zeros(cg.NOALLOC_MAX_BASES, dtype=torch.int64, device="cuda")
     n_out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    # k = 31 and 21 take an even number of 8-bit sort passes, k = 27 and 11 an
+    # odd one (the sorted keys end in the other half of the scratch array)
     cases = [(31, _record(1, cg.NOALLOC_MAX_BASES)), (31, _record(2, 70_001)), (21, _record(3, 300_000)),
-             (31, _record(4, 40))]
+             (27, _record(5, 200_000)), (11, _record(6, 90_000)), (31, _record(4, 40))]
     for k, seq in cases:
         got = _noalloc(torch, seq, k, out, n_out)
         want = _regular(seq, k)
@@ -67,3 +69,15 @@ def test_noalloc_rejects_records_beyond_its_limit():
                                    buf.data_ptr())
     assert st == cg.ERR_TOO_LARGE
     assert cg.distinct_kmers_noalloc(buf.data_ptr(), 100, 32, buf.data_ptr(), 100, buf.data_ptr()) == cg.ERR_INVALID_ARG
+
+
+def test_noalloc_refuses_a_stream_of_another_device():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two devices")
+    buf = torch.zeros(16, dtype=torch.int64, device="cuda:0")
+    with torch.cuda.device(1):
+        other = torch.cuda.Stream()
+    st = cg.distinct_kmers_noalloc(buf.data_ptr(), 100, 31, buf.data_ptr(), 100, buf.data_ptr(),
+                                   stream=other.cuda_stream, device=0)
+    assert st == cg.ERR_INVALID_ARG
