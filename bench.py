@@ -58,6 +58,11 @@ WORKLOADS = {
     5: dict(k=31, bins=256, name="human-scale synthetic genome 3.1 Gbp, 25 chromosomes, ~50% repeats, k=31"),
 }
 METRIC = "k-mers classified/s, 1 B200: learned-index vs GPU BBHash vs CPU (bit-exact)"
+# What the CPU arm does: the oracle port's phase-3 semantics (canonical
+# k-mers, radix sort, unique) and its classify.rs restatement over an exact
+# rank map; it builds no minimizer histogram, no bins and no MPHF, so it does
+# less than the reference's phases 1-4.
+CPU_SCOPE = "oracle port: sort + unique + classify.rs restatement; no minimizer histogram, routing or MPHF"
 UNIT = "distinct k-mers/s"
 
 
@@ -96,17 +101,21 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-TRAFFIC_MD = os.path.join(ROOT, "profiles", "classify_traffic_workload5_full.md")
+def traffic_md(form: str, kernel: str) -> str:
+    if kernel == "classify":
+        return os.path.join(ROOT, "profiles", "classify_traffic_workload5_full.md")
+    return os.path.join(ROOT, "profiles", f"cs_sort_unique_{form}_traffic_workload5.md")
 
 
-def committed_traffic(workload: int, scale: float, form: str):
-    """DRAM bytes (read + write) of one classify launch, from the committed
-    ncu summary of the full 3.1 Gbp workload's BBHash form; None for any
-    other workload, scale or form."""
-    if workload != 5 or scale != 1.0 or form != "bbhash":
+def committed_traffic(workload: int, scale: float, form: str, kernel: str = "classify"):
+    """DRAM bytes (read + write) of one launch of the kernel, full size, from
+    the committed ncu summary for the 3.1 Gbp workload (the summary says
+    whether it was captured at full size or scaled from a smaller case); None
+    for any other workload or scale, or when no summary exists."""
+    if workload != 5 or scale != 1.0 or (kernel == "classify" and form != "bbhash"):
         return None
     try:
-        with open(TRAFFIC_MD) as f:
+        with open(traffic_md(form, kernel)) as f:
             m = re.search(r"^traffic_bytes_per_launch = (\d+)$", f.read(), re.M)
         return int(m.group(1)) if m else None
     except OSError:
@@ -251,7 +260,8 @@ def reference_arm(args):
         "data": "synthetic (seeded generator)",
         "config": {"workload": wl["name"], "k": wl["k"], "num_bins": wl["bins"], "scale": args.scale,
                    "parallelism": "cpu threads"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                         "scope": CPU_SCOPE},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "CPU oracle port of phases 1-4 (phase-3 sort+dedup, classify.rs restatement); "
                 "the Rust reference cannot be built here (no cargo)",
@@ -349,11 +359,12 @@ def gpu_arm(args):
         barrier()
         if clock_info is None:
             clocks.start()
-        ms, ms_cls, launches, phase = [], [], 0, {}
+        ms, ms_cls, ms_dd, launches, phase = [], [], [], 0, {}
         for _ in range(args.steps):
             ms.append(step())
             s = g.stats()
             ms_cls.append(s["ms_classify_kernel"])
+            ms_dd.append(s["ms_dedup_kernel"])
             launches += s["n_kernel_launches"]
             for key in ("ms_phase1", "ms_phase2", "ms_phase3_sort", "ms_phase3_mphf", "ms_phase4"):
                 phase[key] = phase.get(key, 0.0) + s[key] / args.steps
@@ -377,7 +388,8 @@ def gpu_arm(args):
         distinct = sumall(s["n_distinct"])
         forms[form] = dict(
             value=distinct * args.steps / (total_ms / 1e3), ms_per_step=total_ms / args.steps,
-            ms_classify_kernel=maxall(statistics.mean(ms_cls)), launches=launches, stats=s,
+            ms_classify_kernel=maxall(statistics.mean(ms_cls)), ms_dedup_kernel=maxall(statistics.mean(ms_dd)),
+            launches=launches, stats=s,
             phases_ms={k2: round(v, 3) for k2, v in phase.items()},
             learned=g.learned_stats() if form == "learned" else None, ctx=g, be=be, dump=dump)
         if form != args.forms.split(",")[-1]:
@@ -440,14 +452,28 @@ def gpu_arm(args):
     L = s["n_bases"] + s["n_records"]
     n_occ, n_dist = s["n_kmer_occurrences"], s["n_distinct"]
     w = 8 if k <= 32 else 16
-    # classification kernel: 2-bit sequence read once + one 32-B sector read
-    # and one written per occurrence (state word RMW); MPHF probes excluded
+    # classification per occurrence (state_path 1, 2): 2-bit sequence read
+    # once + one 32-B sector read and one written per occurrence (state word
+    # RMW); MPHF probes excluded
     b4 = 0.25 * L + 64.0 * n_occ
-    ach = b4 / (head["ms_classify_kernel"] / 1e3) / 1e9
-    roofline = {"kernel": "classify_defer_kernel" if head_name == "bbhash" else "classify_kernel", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "peak_kind": peak_kind,
-                "traffic": committed_traffic(args.workload, args.scale, head_name),
-                "algorithmic_bytes": b4}
+    if int(s["state_path"]) == 0:
+        # states joined in phase 3: the dominant kernel is the shared-memory
+        # dedup, which reads every occurrence's key and side-set byte and
+        # writes every distinct key and its joined byte (+ in the BBHash form
+        # BBHash level 0: 8 bits per occurrence, stored as 16-B {bits, rank}
+        # entries per 64 bits, i.e. 2 B per occurrence)
+        b_dd = (w + 1.0) * n_occ + (w + 1.0) * n_dist + (2.0 * n_occ if head_name == "bbhash" else 0.0)
+        ach = b_dd / (head["ms_dedup_kernel"] / 1e3) / 1e9
+        roofline = {"kernel": "cs_sort_unique_kernel", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
+                    "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "peak_kind": peak_kind,
+                    "traffic": committed_traffic(args.workload, args.scale, head_name, "dedup"),
+                    "algorithmic_bytes": b_dd}
+    else:
+        ach = b4 / (head["ms_classify_kernel"] / 1e3) / 1e9
+        roofline = {"kernel": "classify_defer_kernel" if head_name == "bbhash" else "classify_kernel", "bound": "hbm",
+                    "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
+                    "peak_kind": peak_kind, "traffic": committed_traffic(args.workload, args.scale, head_name),
+                    "algorithmic_bytes": b4}
     # whole phases 1-4: input read once, records written + read, keys
     # written + read by the sort, distinct keys written and read by the MPHF
     # build, plus the classification bytes above
@@ -464,7 +490,8 @@ def gpu_arm(args):
     if not args.no_cpu_baseline:
         rate, dt, nb, nd = run_cpu_baseline(x, k, int(args.cpu_sample_mbp * 1e6), os.cpu_count() or 1)
         cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
-               "sample": f"first {nb / 1e6:.1f} Mbp of the workload ({nd} distinct k-mers), {dt:.1f} s"}
+               "sample": f"first {nb / 1e6:.1f} Mbp of the workload ({nd} distinct k-mers), {dt:.1f} s",
+               "scope": CPU_SCOPE}
     line = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "strong",

@@ -48,14 +48,14 @@ class Opts(C.Structure):
 
 _STAT_U = ["n_bases", "n_records", "n_short", "n_superkmers", "n_kmer_occurrences", "n_distinct", "n_bins",
            "n_state_words", "mphf_bytes", "bbhash_levels", "learned_bins", "fallback_bins", "learned_max_err",
-           "classify_cas_retries", "n_kernel_launches", "sort_msd_bits", "tuner_state", "sk_tile"]
+           "classify_cas_retries", "n_kernel_launches", "sort_msd_bits", "tuner_state", "sk_tile", "state_path"]
 _STAT_D = ["ms_h2d", "ms_phase1", "ms_phase2", "ms_phase3_sort", "ms_phase3_mphf", "ms_phase4", "ms_total",
-           "ms_classify_kernel"]
+           "ms_classify_kernel", "ms_dedup_kernel"]
 
 
 class Stats(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in _STAT_U] + [("reserved_u", C.c_uint64 * 2)] + \
-               [(n, C.c_double) for n in _STAT_D] + [("reserved_d", C.c_double * 4)]
+    _fields_ = [(n, C.c_uint64) for n in _STAT_U] + [("reserved_u", C.c_uint64 * 1)] + \
+               [(n, C.c_double) for n in _STAT_D] + [("reserved_d", C.c_double * 3)]
 
 
 _lib = None
@@ -190,7 +190,7 @@ class Cf1Gpu:
     def __init__(self, k: int = 31, num_bins: int = 128, device: int = 0, mode: str = "bbhash",
                  batched: bool = False, track_short_seqs: bool = False, learned_max_err: int = 0,
                  learned_train_steps: int = 0, learned_leaf_size: int = 0, sk_tile: int = 0,
-                 sort_mode: str = "msd", state_update: str = "sideset", shard_index: int = 0,
+                 sort_mode: str = "msd", state_update: str = "phase3", shard_index: int = 0,
                  shard_count: int = 1, tuner_cache: str | None = None):
         L = lib()
         o = Opts()
@@ -204,7 +204,7 @@ class Cf1Gpu:
         o.learned_leaf_size = learned_leaf_size
         o.sk_tile = sk_tile
         o.sort_mode = {"msd": 0, "lsd": 1}[sort_mode]
-        o.state_update = {"sideset": 0, "cas": 1}[state_update]
+        o.state_update = {"phase3": 0, "cas": 1, "sideset": 2}[state_update]
         o.shard_index, o.shard_count = shard_index, shard_count
         self._tuner_path = tuner_cache.encode() if tuner_cache else None  # kept alive for the call
         o.tuner_cache_path = self._tuner_path

@@ -71,8 +71,8 @@ int cf1gpu_create(const cf1gpu_opts *opts, cf1gpu_ctx **out) {
     g_create_error = "sort_mode must be 0 (MSD) or 1 (LSD)";
     return CF1GPU_ERR_INVALID_ARG;
   }
-  if (opts->state_update > 1) {
-    g_create_error = "state_update must be 0 (side sets) or 1 (CAS)";
+  if (opts->state_update > 2) {
+    g_create_error = "state_update must be 0 (side sets joined in phase 3), 1 (CAS) or 2 (side-set classification)";
     return CF1GPU_ERR_INVALID_ARG;
   }
   if (opts->shard_count > cf1::MAX_BINS || (opts->shard_count > 1 && opts->shard_index >= opts->shard_count) ||

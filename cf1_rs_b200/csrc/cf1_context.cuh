@@ -74,6 +74,8 @@ struct cf1gpu_ctx {
   // device buffers
   cf1::DevBuf d_l0, d_l0surv, d_binfile, d_binimg, d_raw, d_intake, d_shard, d_ascii, d_W, d_NM, d_hist, d_lut, d_rec_off, d_small, d_cursor, d_records, d_kpre, d_lens, d_seg,
       d_keys, d_dist, d_dist_off, d_states, d_scan, d_seen, d_qin, d_qout, d_queue;
+  // state_update 0: one side-set byte per key beside the sort's two key buffers
+  cf1::DevBuf d_pay, d_pay_alt;
   uint64_t rec_cap_hint = 0;  // phase-1 record list size of the last run
   // exchange-based sharding: the scanned slice's records wait in d_keys for
   // routing; d_xsend holds them grouped by owner shard, d_xcnt the counts

@@ -169,7 +169,8 @@ void record_kmer_prefix(const uint64_t *records, uint64_t n_rec, uint64_t *kpre,
 // i.  Writes past n_keys or reads past base L are skipped and flagged in err.
 template <class KeyT>
 void launch_expand(const uint64_t *records, uint64_t n_rec, const uint64_t *kpre, const uint64_t *W, int k, KeyT *keys,
-                   uint64_t n_keys, uint64_t L, uint32_t *queue, uint32_t *err, int persistent_ctas, cudaStream_t s);
+                   uint64_t n_keys, uint64_t L, uint32_t *queue, uint32_t *err, int persistent_ctas, cudaStream_t s,
+                   const uint64_t *NM = nullptr, uint8_t *sides = nullptr);
 
 // Sorts each segment [seg_off[b], seg_off[b+1]) of keys ascending (LSD radix,
 // segmented).  The result is in `keys` on return.

@@ -261,6 +261,22 @@ CF1_D uint32_t key_leaf(const LIRoot &R, const KeyT &key, int k, uint64_t &h) {
   return li_leaf_of(R, li_root_eval(R, li_x(R, h)));
 }
 
+// Runs of equal leaves inside a warp (the lanes hold consecutive keys, and a
+// monotone root sends consecutive keys to non-decreasing leaves, so a leaf is
+// one run; the reductions below stay exact for any order): the lane of the
+// run's first key, from the ballot of run heads.
+CF1_D uint32_t run_head_lane(uint32_t leaf, unsigned lane, unsigned &heads) {
+  const uint32_t prev = __shfl_up_sync(FULL, leaf, 1);
+  heads = __ballot_sync(FULL, lane == 0 || leaf != prev);
+  return 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));
+}
+CF1_D bool run_tail(uint32_t leaf, unsigned lane) {
+  const uint32_t next = __shfl_down_sync(FULL, leaf, 1);
+  return lane == 31 || leaf != next;
+}
+
+// Per leaf: first and last local rank and key count, one atomic of each kind
+// per run of a warp.
 template <class KeyT>
 __global__ void __launch_bounds__(LT_BLOCK) li_assign_kernel(const KeyT *keys, const uint64_t *dist_off,
                                                             const uint32_t *tile_off, uint32_t nbins,
@@ -271,21 +287,22 @@ __global__ void __launch_bounds__(LT_BLOCK) li_assign_kernel(const KeyT *keys, c
   TileSpan sp = tile_span(dist_off, tile_off, nbins, t, LT_TILE);
   const LIRoot &R = roots[sp.seg];
   const uint64_t base = dist_off[sp.seg];
+  const unsigned lane = lane_id();
   for (uint64_t i0 = sp.start; i0 < sp.end; i0 += LT_BLOCK) {
     uint64_t i = i0 + threadIdx.x;
     bool act = i < sp.end;
     uint64_t h;
     uint32_t leaf = act ? key_leaf(R, keys[i], k, h) : 0xFFFFFFFFu;
     uint32_t rank = (uint32_t)(i - base);
-    unsigned peers = __match_any_sync(FULL, leaf);
+    unsigned heads;
+    const uint32_t hl = run_head_lane(leaf, lane, heads);
+    const bool tail = run_tail(leaf, lane);
     if (act) {
-      uint32_t hi_lane = 31 - __clz(peers);
-      uint32_t rmax = __shfl_sync(peers, rank, hi_lane);
-      if ((peers & lanemask_lt()) == 0) {
-        uint64_t g = R.leaf_off + leaf;
-        atomicMin(&lfirst[g], rank);
-        atomicMax(&llast[g], rmax);
-        atomicAdd(&ln[g], (uint32_t)__popc(peers));
+      const uint64_t g = R.leaf_off + leaf;
+      if (lane == hl) atomicMin(&lfirst[g], rank);
+      if (tail) {
+        atomicMax(&llast[g], rank);
+        atomicAdd(&ln[g], lane - hl + 1);
       }
     }
   }
@@ -318,6 +335,8 @@ __global__ void li_fit_kernel(const KeyT *keys, const uint64_t *dist_off, const 
   leaves[g] = L;
 }
 
+// Per leaf: the largest |prediction - rank| over its keys (a segmented max
+// over each warp's runs, one atomic per run).
 template <class KeyT>
 __global__ void __launch_bounds__(LT_BLOCK) li_err_kernel(const KeyT *keys, const uint64_t *dist_off,
                                                          const uint32_t *tile_off, uint32_t nbins,
@@ -327,6 +346,7 @@ __global__ void __launch_bounds__(LT_BLOCK) li_err_kernel(const KeyT *keys, cons
   TileSpan sp = tile_span(dist_off, tile_off, nbins, t, LT_TILE);
   const LIRoot &R = roots[sp.seg];
   const uint64_t base = dist_off[sp.seg];
+  const unsigned lane = lane_id();
   for (uint64_t i0 = sp.start; i0 < sp.end; i0 += LT_BLOCK) {
     uint64_t i = i0 + threadIdx.x;
     bool act = i < sp.end;
@@ -339,11 +359,15 @@ __global__ void __launch_bounds__(LT_BLOCK) li_err_kernel(const KeyT *keys, cons
       d = d < 0 ? -d : d;
       e = d > 0xFFFFFFF0ll ? 0xFFFFFFF0u : (uint32_t)d;
     }
-    unsigned peers = __match_any_sync(FULL, leaf);
-    if (act) {
-      uint32_t m = __reduce_max_sync(peers, e);
-      if ((peers & lanemask_lt()) == 0) atomicMax(&leaves[R.leaf_off + leaf].err, m);
+    unsigned heads;
+    const uint32_t hl = run_head_lane(leaf, lane, heads);
+    const bool tail = run_tail(leaf, lane);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(FULL, e, d);
+      if (lane >= hl + d) e = v > e ? v : e;
     }
+    if (act && tail) atomicMax(&leaves[R.leaf_off + leaf].err, e);
   }
 }
 
@@ -381,7 +405,13 @@ __global__ void __launch_bounds__(LT_BLOCK) li_decide_kernel(const uint64_t *dis
   }
 }
 
-// Verification: every key of a learned bin must come back as its own rank.
+// Verification, the bijection judge: every key of a learned bin must come
+// back as its own rank.  A query for keys[i] is the lower bound of the key in
+// its window (li_local_slot); in a bin whose keys strictly increase that is i
+// exactly when the window holds i.  So the pass checks each key's window and
+// the order of each adjacent pair -- together a proof that the learned index
+// maps the bin's keys one to one onto [0, n) -- in one streaming read of the
+// keys, with no search.
 template <class KeyT>
 __global__ void __launch_bounds__(LT_BLOCK) li_verify_kernel(const KeyT *keys, const uint64_t *dist_off,
                                                            const uint32_t *tile_off, uint32_t nbins, LIView v,
@@ -393,8 +423,11 @@ __global__ void __launch_bounds__(LT_BLOCK) li_verify_kernel(const KeyT *keys, c
   const uint64_t base = dist_off[sp.seg], n = dist_off[sp.seg + 1] - base;
   bool bad = false;
   for (uint64_t i = sp.start + threadIdx.x; i < sp.end; i += LT_BLOCK) {
-    uint64_t s = li_local_slot(v, keys + base, n, sp.seg, keys[i]);
-    bad |= (s != i - base);
+    const KeyT key = keys[i];
+    const int64_t r = (int64_t)(i - base);
+    int64_t lo, hi;
+    const bool found = li_window(v, n, sp.seg, key, lo, hi) && lo <= r && r <= hi;
+    bad |= !found || (r > 0 && !(keys[i - 1] < key));
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) miss[sp.seg] = 1;
 }

@@ -148,17 +148,28 @@ CF1_HD int64_t li_predict(const LILeaf &lf, uint64_t h) {
   return (int64_t)lf.first_rank + f_round(q);
 }
 
+// The window [lo, hi] of local ranks a query for key searches: root, leaf,
+// the leaf's line, +- its error bound, clamped to the bin.  False when the
+// root sends the key to an empty leaf.
 template <class KeyT>
-CF1_HD uint64_t li_local_slot(const LIView &v, const KeyT *bin_keys, uint64_t n_bin, uint32_t bin, const KeyT &key) {
+CF1_HD bool li_window(const LIView &v, uint64_t n_bin, uint32_t bin, const KeyT &key, int64_t &lo, int64_t &hi) {
   const LIRoot &r = v.roots[bin];
   uint64_t h = KOps<KeyT>::high64(key, v.k);
   uint32_t leaf = li_leaf_of(r, li_root_eval(r, li_x(r, h)));
   const LILeaf lf = v.leaves[r.leaf_off + leaf];
-  if (lf.n == 0) return SLOT_NONE;
+  if (lf.n == 0) return false;
   int64_t p = li_predict(lf, h);
-  int64_t lo = p - (int64_t)lf.err, hi = p + (int64_t)lf.err;
+  lo = p - (int64_t)lf.err;
+  hi = p + (int64_t)lf.err;
   if (lo < 0) lo = 0;
   if (hi > (int64_t)n_bin - 1) hi = (int64_t)n_bin - 1;
+  return true;
+}
+
+template <class KeyT>
+CF1_HD uint64_t li_local_slot(const LIView &v, const KeyT *bin_keys, uint64_t n_bin, uint32_t bin, const KeyT &key) {
+  int64_t lo, hi;
+  if (!li_window(v, n_bin, bin, key, lo, hi)) return SLOT_NONE;
   // lower_bound in [lo, hi]
   int64_t a = lo, b = hi + 1;
   while (a < b) {

@@ -88,16 +88,19 @@ __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, con
 // and each digit's run is written out with consecutive threads on
 // consecutive addresses.  Four CTAs per SM (64 registers): at 3.1 Gbp the
 // two 64-bit passes took 3.3 ms less than with three CTAs and 80 registers.
+// With pin/pout, each key's payload byte (its side-set byte) moves with it.
 template <class KeyT, int BITS>
 __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
                                                                  const uint32_t *tile_off, uint32_t nseg, int shift,
-                                                                 bool hashed, const uint64_t *Hs) {
+                                                                 bool hashed, const uint64_t *Hs, const uint8_t *pin,
+                                                                 uint8_t *pout) {
   constexpr uint32_t DIG = 1u << BITS;
   extern __shared__ __align__(16) unsigned char ms_smem[];
   KeyT *stage = reinterpret_cast<KeyT *>(ms_smem);                            // [MS_TILE]
   uint32_t *whist = reinterpret_cast<uint32_t *>(stage + MS_TILE);           // [MS_NW][DIG]
   uint32_t *lstart = whist + MS_NW * DIG;                                     // [DIG]
   uint64_t *base = reinterpret_cast<uint64_t *>(lstart + DIG);                // [DIG]
+  uint8_t *pstage = reinterpret_cast<uint8_t *>(base + DIG);                  // [MS_TILE] when pin
   __shared__ uint32_t sm[MS_BLOCK / 32];
   const uint32_t t = blockIdx.x;
   if (t >= tile_off[nseg]) return;
@@ -165,14 +168,18 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
   for (int r = 0; r < MS_ITEMS; r++) {
     if (pk[r] != 0xFFFFFFFFu) {
       uint32_t d = pk[r] & 0xFF, li = warp * (MS_ITEMS * 32) + r * 32 + lane;
-      stage[lstart[d] + wh[d] + (pk[r] >> 8)] = HOLD ? kk[HOLD ? r : 0] : in[sp.start + li];
+      const uint32_t at = lstart[d] + wh[d] + (pk[r] >> 8);
+      stage[at] = HOLD ? kk[HOLD ? r : 0] : in[sp.start + li];
+      if (pin) pstage[at] = pin[sp.start + li];
     }
   }
   __syncthreads();
   for (uint32_t i = tid; i < n; i += MS_BLOCK) {
     KeyT kk = stage[i];
     uint32_t d = ms_digit(kk, shift, DIG - 1, hashed);
-    out[base[d] + (i - lstart[d])] = kk;
+    const uint64_t o = base[d] + (i - lstart[d]);
+    out[o] = kk;
+    if (pin) pout[o] = pstage[i];
   }
 }
 
@@ -209,9 +216,13 @@ CF1_D void cs_swap_if(KeyT &a, KeyT &b, bool up) {
 // they do not fit in three quarters of the set.  Every probe sequence is
 // bounded by the set size.  Warps step through the keys together, so the
 // insert count and the give-up test are per warp; the set is emptied into T
-// a warp-sized group of slots at a time.
+// a warp-sized group of slots at a time.  With TP (payload bytes parallel to
+// T), the payloads of a key's copies are ORed into its slot's byte of SPw
+// (cap bytes of shared memory) and written beside the key: the per-side join
+// of the vertex's occurrences.  A pass that gives up leaves T and TP as they
+// were.
 CF1_D uint32_t cs_hash_dedup(uint64_t *T, uint64_t a, uint64_t n, uint64_t *S, uint32_t cap, uint32_t *s_cnt,
-                             uint32_t *sm) {
+                             uint32_t *sm, uint8_t *TP = nullptr, uint32_t *SPw = nullptr) {
   (void)sm;
   const unsigned tid = threadIdx.x, lane = lane_id();
   const uint64_t EMPTY = ~0ull;  // above every key (keys use at most 62 bits)
@@ -221,6 +232,8 @@ CF1_D uint32_t cs_hash_dedup(uint64_t *T, uint64_t a, uint64_t n, uint64_t *S, u
     tbits++;
   }
   for (uint32_t i = tid; i < tsize; i += CS_BLOCK) S[i] = EMPTY;
+  if (TP)
+    for (uint32_t i = tid; i < tsize / 4; i += CS_BLOCK) SPw[i] = 0;
   if (tid == 0) *s_cnt = 0;
   __syncthreads();
   const uint32_t limit = tsize / 4 * 3;
@@ -235,11 +248,11 @@ CF1_D uint32_t cs_hash_dedup(uint64_t *T, uint64_t a, uint64_t n, uint64_t *S, u
       uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - tbits));  // multiplicative hashing
       for (uint32_t probe = 0; probe < tsize; probe++) {
         unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long *>(S + h), EMPTY, key);
-        if (old == EMPTY) {
-          added = true;
+        if (old == EMPTY || old == key) {
+          added = old == EMPTY;
+          if (TP) atomicOr(&SPw[h >> 2], (uint32_t)TP[a + i] << (8 * (h & 3)));
           break;
         }
-        if (old == key) break;
         h = (h + 1) & (tsize - 1);
       }
     }
@@ -259,7 +272,11 @@ CF1_D uint32_t cs_hash_dedup(uint64_t *T, uint64_t a, uint64_t n, uint64_t *S, u
     uint32_t o = 0;
     if (lane == 0 && b) o = atomicAdd(s_cnt, (uint32_t)__popc(b));
     o = __shfl_sync(FULL, o, 0);
-    if (f) T[a + o + __popc(b & lanemask_lt())] = v;
+    if (f) {
+      const uint64_t at = a + o + __popc(b & lanemask_lt());
+      T[at] = v;
+      if (TP) TP[at] = (uint8_t)(SPw[(base + lane) >> 2] >> (8 * ((base + lane) & 3)));
+    }
   }
   __syncthreads();
   return d;
@@ -284,14 +301,33 @@ struct CsDigit {
 struct CsShared {
   uint32_t *hist, *cur, *sm;
   int *big;
+  uint8_t *SP = nullptr;  // payload bytes beside S (CAP), when the keys carry payloads
 };
+
+template <class KeyT>
+CF1_D void cs_swap_if(KeyT &a, KeyT &b, uint8_t *pa, uint8_t *pb, bool up) {
+  if ((b < a) == up) {
+    KeyT t = a;
+    a = b;
+    b = t;
+    if (pa) {
+      uint8_t u = *pa;
+      *pa = *pb;
+      *pb = u;
+    }
+  }
+}
 
 // Sorted distinct keys of src[0, m) (m <= CAP, keys all in [0, 1024) buckets
 // of dig) into out[0, tot); returns tot.  src is fully read into shared
-// memory before out is written, so they may overlap.  All threads call it.
+// memory before out is written, so they may overlap.  With srcP/outP (and
+// sh.SP), each key's payload byte moves with it and the payloads of a key's
+// copies are ORed.  All threads call it.
 template <class KeyT>
 CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &dig, KeyT *S, const CsShared &sh,
-                                    KeyT *out, bool distinct) {
+                                    KeyT *out, bool distinct, const uint8_t *srcP = nullptr,
+                                    uint8_t *outP = nullptr) {
+  uint8_t *SP = srcP ? sh.SP : nullptr;
   constexpr uint32_t CAP = cs_cap<KeyT>();
   const unsigned tid = threadIdx.x;
   for (uint32_t i = tid; i < CS_BUCKETS; i += CS_BLOCK) sh.hist[i] = 0;
@@ -319,7 +355,9 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
   __syncthreads();
   for (uint32_t i = tid; i < m; i += CS_BLOCK) {
     KeyT key = src[i];
-    S[atomicAdd(&sh.cur[dig(key)], 1u)] = key;
+    const uint32_t at = atomicAdd(&sh.cur[dig(key)], 1u);
+    S[at] = key;
+    if (SP) SP[at] = srcP[i];
   }
   __syncthreads();
   // insertion sort per bucket (bucket b spans [hist[b], cur[b]))
@@ -331,25 +369,32 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
     }
     for (uint32_t i = lo + 1; i < hi; i++) {
       KeyT x = S[i];
+      const uint8_t xp = SP ? SP[i] : 0;
       uint32_t q = i;
       while (q > lo && x < S[q - 1]) {
         S[q] = S[q - 1];
+        if (SP) SP[q] = SP[q - 1];
         q--;
       }
       S[q] = x;
+      if (SP) SP[q] = xp;
     }
   }
   __syncthreads();
   if (*sh.big) {  // bitonic sort of the whole range, padded to a power of two
     uint32_t P2 = 1;
     while (P2 < m) P2 <<= 1;
-    for (uint32_t i = m + tid; i < P2; i += CS_BLOCK) S[i] = KOps<KeyT>::max_key();
+    for (uint32_t i = m + tid; i < P2; i += CS_BLOCK) {
+      S[i] = KOps<KeyT>::max_key();
+      if (SP) SP[i] = 0;
+    }
     __syncthreads();
     for (uint32_t size = 2; size <= P2; size <<= 1) {
       for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
         for (uint32_t i = tid; i < P2 / 2; i += CS_BLOCK) {
           uint32_t lo = 2 * i - (i & (stride - 1));
-          cs_swap_if(S[lo], S[lo + stride], (lo & size) == 0);
+          cs_swap_if(S[lo], S[lo + stride], SP ? SP + lo : nullptr, SP ? SP + lo + stride : nullptr,
+                     (lo & size) == 0);
         }
         __syncthreads();
       }
@@ -357,13 +402,24 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
   }
   (void)CAP;
   if (distinct) {  // already one copy per key: plain copy out
-    for (uint32_t i = tid; i < m; i += CS_BLOCK) out[i] = S[i];
+    for (uint32_t i = tid; i < m; i += CS_BLOCK) {
+      out[i] = S[i];
+      if (SP) outP[i] = SP[i];
+    }
     __syncthreads();
     return m;
   }
-  // adjacent-unique
+  // adjacent-unique; a run's first key takes the OR of the run's payloads
   return block_select<CS_BLOCK>(
-      m, [&](uint32_t i) { return i == 0 || S[i] != S[i - 1]; }, [&](uint32_t i, uint32_t r) { out[r] = S[i]; },
+      m, [&](uint32_t i) { return i == 0 || S[i] != S[i - 1]; },
+      [&](uint32_t i, uint32_t r) {
+        out[r] = S[i];
+        if (SP) {
+          uint32_t p = SP[i];
+          for (uint32_t j = i + 1; j < m && S[j] == S[i]; j++) p |= SP[j];
+          outP[r] = (uint8_t)p;
+        }
+      },
       sh.sm);
 }
 
@@ -444,10 +500,19 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
 // consecutive pieces up to CAP keys are sorted one after another, and their
 // distinct keys are appended at T[a].  Only a single piece above CAP keys
 // makes the kernel report the sub-bucket as oversized.
+// With TP/UP (payload bytes parallel to T and U), every distinct key leaves
+// with the OR of its copies' payloads beside it in TP.
+// Chunks (sorted form): with clist, CTA c takes the run of consecutive
+// sub-buckets [j0, j1) of one bin that the plan packed together (coff: the
+// plan's chunks per bin, scanned), sorts the run as one range -- its bucket is
+// the sub-bucket's place in the run, then the next key bits -- and credits
+// all its distinct keys to sub-bucket j0.
 template <class KeyT, bool SORTED>
 __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kernel(KeyT *T, KeyT *U, const uint64_t *sb_off,
                                                                   uint64_t nsub, int shift, int bits, uint32_t *cnt,
-                                                                  uint32_t *oversize, int P, Level0Out l0) {
+                                                                  uint32_t *oversize, int P, Level0Out l0,
+                                                                  uint8_t *TP, uint8_t *UP, const uint2 *clist,
+                                                                  const uint64_t *coff, uint32_t nbins) {
   constexpr uint32_t CAP = cs_cap<KeyT, SORTED>();
   constexpr bool L0 = !SORTED && KOps<KeyT>::WORDS == 1;
   __shared__ unsigned long long s_l0base;
@@ -457,31 +522,49 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
   uint32_t *cur = hist + CS_BUCKETS;                              // [CS_BUCKETS]
   uint32_t *pstart = cur + CS_BUCKETS;                            // [CS_BUCKETS + 1]
   uint16_t *cb = reinterpret_cast<uint16_t *>(pstart + CS_BUCKETS + 1);  // [CS_BUCKETS + 1]
+  uint32_t *SPw = reinterpret_cast<uint32_t *>(cb + CS_BUCKETS + 2);     // [CAP / 4] payloads, when TP
   __shared__ uint32_t sm[CS_BLOCK / 32];
   __shared__ int s_big, s_nchunks, s_bad;
   __shared__ uint32_t s_cnt;
-  const uint64_t j = blockIdx.x;
+  uint64_t j = blockIdx.x, jend = j + 1;
+  if (clist) {
+    const uint32_t bin = upper_segment(coff, nbins, (uint64_t)blockIdx.x);
+    const uint2 r = clist[((uint64_t)bin << P) + (blockIdx.x - coff[bin])];
+    j = ((uint64_t)bin << P) + r.x;
+    jend = ((uint64_t)bin << P) + r.y;
+  }
   if (j >= nsub) return;
-  const uint64_t a = sb_off[j], n = sb_off[j + 1] - a;
+  const uint64_t a = sb_off[j], n = sb_off[jend] - a;
   const unsigned tid = threadIdx.x;
   // the sub-bucket's distinct keys end at T[a, a + result); ~0u: oversized
   auto body = [&]() -> uint32_t {
     if (n == 0) return 0;
-    CsShared sh{hist, cur, sm, &s_big};
+    CsShared sh{hist, cur, sm, &s_big, TP ? reinterpret_cast<uint8_t *>(SPw) : nullptr};
     CsDigit plain{shift, bits, 0, 0, 0u};
+    if (jend - j > 1) {  // a packed run: bucket = place of the sub-bucket in the run, then the next bits
+      const uint32_t span = (uint32_t)(jend - j);
+      int g = 0;
+      while ((1u << g) < span) g++;
+      const int rest = shift + bits;  // the sub-bucket prefix sits at bits [rest, rest + P)
+      const int b2 = 10 - g < rest ? 10 - g : rest;
+      plain = CsDigit{rest, P, rest - b2, b2, (uint32_t)(j & ((1ull << P) - 1))};
+    }
     uint32_t m = (uint32_t)n;
     bool distinct = false;
     // 64-bit keys: one copy of each key first.  Repeats put hundreds of
     // copies of a k-mer in one bucket, where sorting copies would dominate.
     if ((!SORTED || n > CS_DEDUP_MIN) && KOps<KeyT>::WORDS == 1) {
-      uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(T), a, n, reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
+      uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(T), a, n, reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm,
+                                 TP, SPw);
       if (d != ~0u) {
         m = d;
         distinct = true;
         if (!SORTED) return d;  // distinct keys are all that is needed
       }
     }
-    if (m <= CAP) return cs_sort_unique_range<KeyT>(T + a, m, plain, S, sh, T + a, distinct);
+    if (m <= CAP)
+      return cs_sort_unique_range<KeyT>(T + a, m, plain, S, sh, T + a, distinct, TP ? TP + a : nullptr,
+                                        TP ? TP + a : nullptr);
     // local split on the next `bits` bits into U[a, a+n)
     const uint32_t npieces = 1u << bits, pmask = npieces - 1;
     for (uint32_t i = tid; i <= CS_BUCKETS; i += CS_BLOCK) pstart[i] = 0;
@@ -526,7 +609,9 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
     __syncthreads();
     for (uint64_t i = tid; i < n; i += CS_BLOCK) {
       KeyT key = T[a + i];
-      U[a + atomicAdd(&cur[KOps<KeyT>::digit(key, shift, pmask)], 1u)] = key;
+      const uint32_t at = atomicAdd(&cur[KOps<KeyT>::digit(key, shift, pmask)], 1u);
+      U[a + at] = key;
+      if (TP) UP[a + at] = TP[a + i];
     }
     __syncthreads();
     uint32_t outc = 0;
@@ -542,14 +627,15 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
       bool dd = false;
       if (len > CS_DEDUP_MIN && KOps<KeyT>::WORDS == 1) {
         uint32_t d = cs_hash_dedup(reinterpret_cast<uint64_t *>(U), a + pstart[p0], len,
-                                   reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm);
+                                   reinterpret_cast<uint64_t *>(S), CAP, &s_cnt, sm, TP ? UP : nullptr, SPw);
         if (d != ~0u) {  // (a failed pass leaves U untouched)
           len = d;
           dd = true;
         }
         if (len > CAP) return ~0u;
       }
-      outc += cs_sort_unique_range<KeyT>(U + a + pstart[p0], len, dig, S, sh, T + a + outc, dd);
+      outc += cs_sort_unique_range<KeyT>(U + a + pstart[p0], len, dig, S, sh, T + a + outc, dd,
+                                         TP ? UP + a + pstart[p0] : nullptr, TP ? TP + a + outc : nullptr);
     }
     return outc;
   };
@@ -558,6 +644,7 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
     cnt[j] = res == ~0u ? 0 : res;
     if (res == ~0u) atomicOr(oversize, 1u);
   }
+  for (uint64_t q = j + 1 + tid; q < jend; q += CS_BLOCK) cnt[q] = 0;
   if constexpr (L0) {
     if (l0.AR && res != ~0u) {
       __syncthreads();
@@ -566,6 +653,32 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
                reinterpret_cast<uint16_t *>(S), CAP * sizeof(KeyT) / 2, sm, &s_l0base);
     }
   }
+}
+
+// Chunk plan of the sorted form: per bin (one thread), runs of consecutive
+// sub-buckets packed greedily up to cap keys (a sub-bucket above cap is a run
+// of its own), written as (first, end) sub-bucket indices within the bin to
+// clist[bin << P ...]; ccount[bin] = the bin's runs.
+__global__ void cs_plan_kernel(const uint64_t *sb_off, uint32_t nbins, int P, uint32_t cap, uint2 *clist,
+                               uint32_t *ccount) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbins) return;
+  const uint32_t per = 1u << P;
+  const uint64_t *o = sb_off + ((uint64_t)b << P);
+  uint2 *out = clist + ((uint64_t)b << P);
+  uint32_t nc = 0, start = 0;
+  uint64_t acc = 0;
+  for (uint32_t q = 0; q < per; q++) {
+    const uint64_t sz = o[q + 1] - o[q];
+    if (acc > 0 && acc + sz > cap) {
+      out[nc++] = make_uint2(start, q);
+      start = q;
+      acc = 0;
+    }
+    acc += sz;
+  }
+  out[nc++] = make_uint2(start, per);
+  ccount[b] = nc;
 }
 
 // One warp per sub-bucket: copy its distinct keys to the dense array.
@@ -586,7 +699,7 @@ __global__ void cs_bin_off_kernel(const uint64_t *out_off, uint32_t nbins, uint6
 
 template <class KeyT, int BITS>
 void ms_pass(const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift, bool hashed,
-             MsdScratch &sc, cudaStream_t s) {
+             MsdScratch &sc, cudaStream_t s, const uint8_t *pin, uint8_t *pout) {
   constexpr uint32_t DIG = 1u << BITS;
   uint32_t ub = (uint32_t)(ceil_div(n, MS_TILE) + nseg);
   uint32_t *tile_off = sc.tile_off.get<uint32_t>(nseg + 1);
@@ -596,24 +709,26 @@ void ms_pass(const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uin
   ms_hist_kernel<KeyT, BITS><<<ub, MS_BLOCK, 0, s>>>(in, seg_off, tile_off, nseg, shift, hashed, H);
   CF1_LAUNCH_CHECK();
   exclusive_scan_u32(H, Hs, (uint64_t)ub * DIG, sc.scan_tmp, s);
-  size_t smem = MS_TILE * sizeof(KeyT) + (MS_NW + 1) * DIG * sizeof(uint32_t) + DIG * sizeof(uint64_t);
+  size_t smem = MS_TILE * sizeof(KeyT) + (MS_NW + 1) * DIG * sizeof(uint32_t) + DIG * sizeof(uint64_t) +
+                (pin ? MS_TILE : 0);
   CF1_CUDA(cudaFuncSetAttribute(ms_scatter_kernel<KeyT, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  ms_scatter_kernel<KeyT, BITS><<<ub, MS_BLOCK, smem, s>>>(in, out, seg_off, tile_off, nseg, shift, hashed, Hs);
+  ms_scatter_kernel<KeyT, BITS><<<ub, MS_BLOCK, smem, s>>>(in, out, seg_off, tile_off, nseg, shift, hashed, Hs, pin,
+                                                           pout);
   CF1_LAUNCH_CHECK();
 }
 
 template <class KeyT>
 void ms_pass_bits(int bits, const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift,
-                  bool hashed, MsdScratch &sc, cudaStream_t s) {
+                  bool hashed, MsdScratch &sc, cudaStream_t s, const uint8_t *pin, uint8_t *pout) {
   switch (bits) {
-    case 1: ms_pass<KeyT, 1>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
-    case 2: ms_pass<KeyT, 2>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
-    case 3: ms_pass<KeyT, 3>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
-    case 4: ms_pass<KeyT, 4>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
-    case 5: ms_pass<KeyT, 5>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
-    case 6: ms_pass<KeyT, 6>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
-    case 7: ms_pass<KeyT, 7>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
-    case 8: ms_pass<KeyT, 8>(in, out, n, seg_off, nseg, shift, hashed, sc, s); break;
+    case 1: ms_pass<KeyT, 1>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
+    case 2: ms_pass<KeyT, 2>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
+    case 3: ms_pass<KeyT, 3>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
+    case 4: ms_pass<KeyT, 4>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
+    case 5: ms_pass<KeyT, 5>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
+    case 6: ms_pass<KeyT, 6>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
+    case 7: ms_pass<KeyT, 7>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
+    case 8: ms_pass<KeyT, 8>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
     default: throw Error(-1, "MSD pass width must be 1..8 bits");
   }
 }
@@ -667,7 +782,8 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted) {
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
                      KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted,
-                     const Level0Out *l0, KeyT **kept) {
+                     const Level0Out *l0, KeyT **kept, uint8_t *pkeys, uint8_t *palt, uint8_t **kept_pay) {
+  uint8_t *PT = pkeys;  // payloads beside T (nullptr: keys carry none)
   // passes on the top P bits: P1 then P2 (P2 may be 0) -- of the key, or of
   // its hash when only distinct keys are wanted (64-bit keys)
   const bool hashed = !sorted && KOps<KeyT>::WORDS == 1;
@@ -679,7 +795,7 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
   if (P == 0) {
     CF1_CUDA(cudaMemcpyAsync(sb_off, seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
   } else if (n) {
-    ms_pass_bits<KeyT>(P1, keys, alt, n, seg_off, nbins, key_bits - P1, hashed, sc, s);
+    ms_pass_bits<KeyT>(P1, keys, alt, n, seg_off, nbins, key_bits - P1, hashed, sc, s, pkeys, palt);
     const uint64_t *seg2 = seg_off;
     uint32_t nseg2 = nbins;
     if (P2) {
@@ -688,10 +804,12 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
       subbuckets_bits(P1, seg_off, sc.tile_off.as<uint32_t>(), nbins, sc.hscan.as<uint64_t>(), sb1, s);
       nseg2 = (uint32_t)((uint64_t)nbins << P1);
       seg2 = sb1;
-      ms_pass_bits<KeyT>(P2, alt, keys, n, seg2, nseg2, key_bits - P1 - P2, hashed, sc, s);
+      ms_pass_bits<KeyT>(P2, alt, keys, n, seg2, nseg2, key_bits - P1 - P2, hashed, sc, s, palt, pkeys);
       T = keys;
+      PT = pkeys;
     } else {
       T = alt;
+      PT = palt;
     }
     subbuckets_bits(P2 ? P2 : P1, seg2, sc.tile_off.as<uint32_t>(), nseg2, sc.hscan.as<uint64_t>(), sb_off, s);
   } else {
@@ -712,24 +830,52 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
     shift = 0;
   }
   // S, hist, cur, pstart (u32) and the chunk bounds (u16)
-  size_t smem = cs_cap_for(KOps<KeyT>::WORDS == 2, sorted) * sizeof(KeyT) + (3 * CS_BUCKETS + 1) * sizeof(uint32_t) +
-                (CS_BUCKETS + 1) * sizeof(uint16_t);
+  const uint32_t cap = cs_cap_for(KOps<KeyT>::WORDS == 2, sorted);
+  size_t smem = cap * sizeof(KeyT) + (3 * CS_BUCKETS + 1) * sizeof(uint32_t) + (CS_BUCKETS + 2) * sizeof(uint16_t) +
+                (pkeys ? cap : 0);
   auto kern = sorted ? cs_sort_unique_kernel<KeyT, true> : cs_sort_unique_kernel<KeyT, false>;
   CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   KeyT *U = T == keys ? alt : keys;
+  uint8_t *PU = pkeys ? (PT == pkeys ? palt : pkeys) : nullptr;
   if (nsub) {
     Level0Out lo;
     if (l0 && hashed) lo = *l0;
-    kern<<<(unsigned)nsub, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over, P, lo);
+    for (auto &e : sc.ev)
+      if (!e) CF1_CUDA(cudaEventCreate(&e));
+    // sorted form: consecutive small sub-buckets of a bin are packed into
+    // one CTA's run (the top bits of canonical k-mers are skewed, so most
+    // sub-buckets are far below the capacity the largest ones need)
+    const uint2 *clist = nullptr;
+    const uint64_t *coff = nullptr;
+    uint64_t grid = nsub;
+    if (sorted && P > 0) {
+      uint2 *cl = sc.clist.get<uint2>(nsub);
+      uint32_t *cc = sc.ccount.get<uint32_t>(nbins + 1);
+      uint64_t *co = sc.coff.get<uint64_t>(nbins + 1);
+      cs_plan_kernel<<<(unsigned)ceil_div(nbins, 128), 128, 0, s>>>(sb_off, nbins, P, cap, cl, cc);
+      CF1_LAUNCH_CHECK();
+      exclusive_scan_u32(cc, co, nbins, sc.scan_tmp, s);
+      CF1_CUDA(cudaMemcpyAsync(&grid, co + nbins, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+      CF1_CUDA(cudaStreamSynchronize(s));
+      clist = cl;
+      coff = co;
+    }
+    CF1_CUDA(cudaEventRecord(sc.ev[0], s));
+    kern<<<(unsigned)grid, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over, P, lo, PT,
+                                                PU, clist, coff, nbins);
     CF1_LAUNCH_CHECK();
+    CF1_CUDA(cudaEventRecord(sc.ev[1], s));
   }
   uint32_t h_over = 0;
   CF1_CUDA(cudaMemcpyAsync(&h_over, over, 4, cudaMemcpyDeviceToHost, s));
   CF1_CUDA(cudaStreamSynchronize(s));
+  sc.ms_dedup = 0;
+  if (nsub) CF1_CUDA(cudaEventElapsedTime(&sc.ms_dedup, sc.ev[0], sc.ev[1]));
   if (h_over) return false;
   uint64_t *out_off = sc.out_off.get<uint64_t>(nsub + 1);
   exclusive_scan_u32(cnt, out_off, nsub, sc.scan_tmp, s);
   if (kept) *kept = T;
+  if (kept_pay) *kept_pay = PT;
   if (dist) msd_compact<KeyT>(T, nsub, dist, sc, s);
   cs_bin_off_kernel<<<(unsigned)ceil_div(nbins + 1, 256), 256, 0, s>>>(out_off, nbins, 1ull << P, dist_off);
   CF1_LAUNCH_CHECK();
@@ -739,7 +885,8 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
 #define CF1_INST(KT)                                                                                              \
   template int msd_prefix_bits<KT>(uint64_t, bool);                                                                     \
   template bool msd_sort_unique<KT>(KT *, KT *, uint64_t, const uint64_t *, uint32_t, int, int, KT *, uint64_t *, \
-                                    MsdScratch &, cudaStream_t, bool, const Level0Out *, KT **);              \
+                                    MsdScratch &, cudaStream_t, bool, const Level0Out *, KT **, uint8_t *,    \
+                                    uint8_t *, uint8_t **);                                                   \
   template void msd_compact<KT>(const KT *, uint64_t, KT *, MsdScratch &, cudaStream_t);
 CF1_INST(uint64_t)
 CF1_INST(Key2)

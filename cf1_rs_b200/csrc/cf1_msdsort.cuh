@@ -6,7 +6,13 @@
 namespace cf1 {
 
 struct MsdScratch {
-  DevBuf tile_off, hist, hscan, scan_tmp, sb_off, sb_off1, cnt, out_off, flag;
+  DevBuf tile_off, hist, hscan, scan_tmp, sb_off, sb_off1, cnt, out_off, flag, clist, ccount, coff;
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // around the last dedup kernel launch
+  float ms_dedup = 0;                      // its device time
+  ~MsdScratch() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
 };
 
 // Top bits to split on so that the largest bin's sub-buckets hold about a
@@ -39,10 +45,14 @@ struct Level0Out {
 // With dist = nullptr the distinct keys stay where the dedup left them, at
 // the start of each sub-bucket's range of *kept (keys or alt), and
 // msd_compact writes dist later; dist_off is written either way.
+// With pkeys/palt (one payload byte per key, beside keys and alt), each
+// distinct key leaves with the OR of its copies' payloads at the same place
+// of *kept_pay (pkeys or palt, beside *kept).
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
                      KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted = true,
-                     const Level0Out *l0 = nullptr, KeyT **kept = nullptr);
+                     const Level0Out *l0 = nullptr, KeyT **kept = nullptr, uint8_t *pkeys = nullptr,
+                     uint8_t *palt = nullptr, uint8_t **kept_pay = nullptr);
 
 // The deferred copy: distinct keys of the last msd_sort_unique (nsub
 // sub-buckets, left in `kept`) to dist, bins in order.

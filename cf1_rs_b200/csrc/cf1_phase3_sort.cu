@@ -24,11 +24,16 @@ __global__ void record_len_kernel(const uint64_t *records, uint64_t n, uint32_t 
 
 // Warp-cooperative expansion: a warp takes 32 records, and its lanes walk the
 // records' k-mers in one flattened index space, so output stores are
-// contiguous whatever the record lengths.
+// contiguous whatever the record lengths.  With `sides` (and NM), each
+// occurrence also writes its side-set byte: the (front, back) contribution
+// its true neighbours in the sequence give the vertex (src/classify.rs:
+// 65-518 as the per-side join), so phase 3 can join a vertex's occurrences
+// while it removes their duplicate keys.
 template <class KeyT>
 __global__ void __launch_bounds__(256) expand_kernel(const uint64_t *records, uint64_t n_rec, const uint64_t *kpre,
                                                      const uint64_t *W, int k, KeyT *keys, uint64_t n_keys,
-                                                     uint64_t L, uint32_t *queue, uint32_t *err) {
+                                                     uint64_t L, uint32_t *queue, uint32_t *err, const uint64_t *NM,
+                                                     uint8_t *sides) {
   const unsigned lane = lane_id();
   const uint64_t n_chunks = ceil_div_dev(n_rec);
   uint64_t chunk = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -59,12 +64,22 @@ __global__ void __launch_bounds__(256) expand_kernel(const uint64_t *records, ui
       uint64_t opos = __shfl_sync(FULL, pos, lo);
       uint32_t oex = __shfl_sync(FULL, excl, lo);
       uint64_t ooff = __shfl_sync(FULL, off, lo);
+      const uint32_t onrec = __shfl_sync(FULL, n, lo);
       if (j < total) {
         uint32_t t = j - oex;
         if (ooff + t < n_keys && opos + t + k <= L) {
-          KeyT fw = KOps<KeyT>::extract(W, opos + t, k);
+          const uint64_t p = opos + t;
+          KeyT fw = KOps<KeyT>::extract(W, p, k);
           KeyT rc = KOps<KeyT>::rc(fw, k);
           keys[ooff + t] = kmin(fw, rc);
+          if (sides) {
+            // inside a super k-mer the windows before and after are valid, so
+            // only its first and last k-mers can lack a neighbour
+            const bool hp = t > 0 || (p > 0 && !is_n(NM, p - 1));
+            const bool hn = t + 1 < onrec || (p + k < L && !is_n(NM, p + k));
+            const uint32_t pb = hp ? base_at(W, p - 1) : 0, nb = hn ? base_at(W, p + k) : 0;
+            sides[ooff + t] = (uint8_t)sideset_lookup(contribution(fw, rc, hp, pb, hn, nb, k));
+          }
         } else {
           atomicOr(err, (uint32_t)DEV_OVERFLOW);
         }
@@ -220,13 +235,14 @@ void record_kmer_prefix(const uint64_t *records, uint64_t n_rec, uint64_t *kpre,
 
 template <class KeyT>
 void launch_expand(const uint64_t *records, uint64_t n_rec, const uint64_t *kpre, const uint64_t *W, int k, KeyT *keys,
-                   uint64_t n_keys, uint64_t L, uint32_t *queue, uint32_t *err, int persistent_ctas, cudaStream_t s) {
+                   uint64_t n_keys, uint64_t L, uint32_t *queue, uint32_t *err, int persistent_ctas, cudaStream_t s,
+                   const uint64_t *NM, uint8_t *sides) {
   if (n_rec == 0) return;
   uint64_t warps = ceil_div(n_rec, 32);
   unsigned grid = persistent_ctas ? persistent_grid(expand_kernel<KeyT>, 256, 0, persistent_ctas, ceil_div(warps, 8))
                                   : (unsigned)ceil_div(warps, 8);
   expand_kernel<KeyT><<<grid, 256, 0, s>>>(records, n_rec, kpre, W, k, keys, n_keys, L,
-                                           persistent_ctas ? queue : nullptr, err);
+                                           persistent_ctas ? queue : nullptr, err, NM, sides);
   CF1_LAUNCH_CHECK();
 }
 
@@ -279,7 +295,8 @@ void segmented_unique(const KeyT *keys, uint64_t n, const uint64_t *seg_off, uin
 
 #define CF1_INST(KT)                                                                                                 \
   template void launch_expand<KT>(const uint64_t *, uint64_t, const uint64_t *, const uint64_t *, int, KT *,        \
-                                  uint64_t, uint64_t, uint32_t *, uint32_t *, int, cudaStream_t);                   \
+                                  uint64_t, uint64_t, uint32_t *, uint32_t *, int, cudaStream_t, const uint64_t *,  \
+                                  uint8_t *);                                                                       \
   template void segmented_sort<KT>(KT *, uint64_t, const uint64_t *, uint32_t, int, SortScratch<KT> &, cudaStream_t); \
   template void segmented_unique<KT>(const KT *, uint64_t, const uint64_t *, uint32_t, KT *, uint64_t *,            \
                                      SortScratch<KT> &, cudaStream_t);

@@ -160,6 +160,35 @@ __global__ void __launch_bounds__(CL_BLOCK_DEFER) classify_defer_kernel(Classify
   classify_body<KeyT, SIDESET, true>(a);
 }
 
+// One warp per sub-bucket: each distinct key's side-set byte to its slot.
+// A learned bin's slot is the key's rank, which the dense layout already
+// gives; a BBHash bin walks the levels (one probe for most keys, in the bin's
+// block, which the neighbouring warps share).
+template <class KeyT>
+__global__ void __launch_bounds__(256) place_sides_kernel(MphfView<KeyT> m, const KeyT *kept, const KeyT *dense,
+                                                          const uint8_t *kept_pay, const uint64_t *sb_off,
+                                                          const uint32_t *cnt, const uint64_t *out_off, uint64_t j0,
+                                                          uint64_t j1, int P, uint8_t *sides, uint32_t *err) {
+  const uint64_t j = j0 + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (j >= j1) return;
+  const uint32_t c = cnt[j], bin = (uint32_t)(j >> P);
+  const uint64_t a = sb_off[j], o = out_off[j], base = m.dist_off[bin], end = m.dist_off[bin + 1];
+  const bool ranked = m.learned && m.li.roots[bin].use_learned;
+  bool miss = false;
+  for (uint32_t i = lane_id(); i < c; i += 32) {
+    uint64_t slot;
+    if (ranked) {
+      slot = o + i;
+    } else {
+      const uint64_t local = bb_local_slot(m.bb, bin, dense ? dense[o + i] : kept[a + i]);
+      slot = local == SLOT_NONE ? SLOT_NONE : base + local;
+    }
+    if (slot < end && slot >= base) sides[slot] = kept_pay[a + i];
+    else miss = true;
+  }
+  if (__any_sync(FULL, miss) && lane_id() == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
+}
+
 // Word w of the state vector from side-set bytes 12w .. 12w+11 (three u32).
 constexpr int PK_BLOCK = 256;
 __global__ void __launch_bounds__(PK_BLOCK) sideset_pack_kernel(const uint32_t *sides, uint64_t w0, uint64_t w1,
@@ -250,6 +279,16 @@ void launch_classify(const ClassifyArgs<KeyT> &a, int persistent_ctas, cudaStrea
   CF1_LAUNCH_CHECK();
 }
 
+template <class KeyT>
+void launch_place_sides(const MphfView<KeyT> &m, const KeyT *kept, const KeyT *dense, const uint8_t *kept_pay,
+                        const uint64_t *sb_off, const uint32_t *cnt, const uint64_t *out_off, uint64_t j0, uint64_t j1,
+                        int P, uint8_t *sides, uint32_t *err, cudaStream_t s) {
+  if (j1 <= j0) return;
+  place_sides_kernel<KeyT><<<(unsigned)ceil_div((j1 - j0) * 32, 256), 256, 0, s>>>(
+      m, kept, dense, kept_pay, sb_off, cnt, out_off, j0, j1, P, sides, err);
+  CF1_LAUNCH_CHECK();
+}
+
 void launch_sideset_pack(const uint32_t *sides, uint64_t w0, uint64_t w1, unsigned long long *states,
                          cudaStream_t s) {
   if (w1 <= w0) return;
@@ -285,6 +324,9 @@ void launch_query(const MphfView<KeyT> &m, const uint16_t *lut, int k, int mlen,
 
 #define CF1_INST(KT)                                                                                             \
   template void launch_classify<KT>(const ClassifyArgs<KT> &, int, cudaStream_t);                               \
+  template void launch_place_sides<KT>(const MphfView<KT> &, const KT *, const KT *, const uint8_t *,           \
+                                       const uint64_t *, const uint32_t *, const uint64_t *, uint64_t, uint64_t, \
+                                       int, uint8_t *, uint32_t *, cudaStream_t);                                \
   template void launch_dump<KT>(const MphfView<KT> &, uint32_t, uint64_t, const unsigned long long *, uint64_t *, \
                                 uint8_t *, cudaStream_t);                                                       \
   template void launch_verify<KT>(const MphfView<KT> &, uint32_t, uint64_t, uint32_t *, uint32_t *, cudaStream_t); \

@@ -23,6 +23,18 @@ struct ClassifyArgs {
 template <class KeyT>
 void launch_classify(const ClassifyArgs<KeyT> &a, int persistent_ctas, cudaStream_t s);
 
+// Phase 4 when phase 3 has joined the occurrences: the side-set byte left
+// beside each distinct key (kept[sb_off[j] + i], i < cnt[j], for the
+// sub-buckets j in [j0, j1) of 2^P per bin) goes to its vertex's slot --
+// the key's rank (out_off[j] + i) in a bin the learned index serves, its
+// BBHash slot in any other bin.  A slot outside the bin flags DEV_MPHF_MISS.
+// The keys are read from the dense array (dense[out_off[j] + i]) when it is
+// given, else from beside the bytes (kept[sb_off[j] + i]).
+template <class KeyT>
+void launch_place_sides(const MphfView<KeyT> &m, const KeyT *kept, const KeyT *dense, const uint8_t *kept_pay,
+                        const uint64_t *sb_off, const uint32_t *cnt, const uint64_t *out_off, uint64_t j0, uint64_t j1,
+                        int P, uint8_t *sides, uint32_t *err, cudaStream_t s);
+
 // Packs side-set bytes (3 u32 per state word) into state words [w0, w1).
 void launch_sideset_pack(const uint32_t *sides, uint64_t w0, uint64_t w1, unsigned long long *states,
                          cudaStream_t s);

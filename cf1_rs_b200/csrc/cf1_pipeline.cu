@@ -476,7 +476,15 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   // ---- phase 3a: expand, sort per bin, unique
   const uint64_t NO = c->n_occ;
   KeyT *keys = c->d_keys.get<KeyT>(NO + 1);
-  launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[2] : nullptr, &sm->err, pctas, s);
+  // state_update 0: every occurrence's side-set byte travels with its key
+  // through the MSD sort, whose dedup joins a vertex's occurrences, so phase
+  // 4 only places each distinct key's byte in its slot (the LSD fallback has
+  // no payloads: phase 4 then classifies the occurrences as before)
+  const bool join3 = c->opts.state_update == 0 && !c->force_lsd;
+  uint8_t *pay = join3 ? c->d_pay.get<uint8_t>(NO + 16) : nullptr;
+  uint8_t *pay_alt = join3 ? c->d_pay_alt.get<uint8_t>(NO + 16) : nullptr;
+  launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[2] : nullptr, &sm->err, pctas, s, NM,
+                      pay);
   uint64_t *seg = c->d_seg.get<uint64_t>(B + 1);
   seg_gather_kernel<<<(unsigned)ceil_div(B + 1, 256), 256, 0, s>>>(kpre, rec_off, B, seg);
   CF1_LAUNCH_CHECK();
@@ -492,7 +500,8 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   const int P0 = c->force_lsd ? -1 : msd_prefix_bits<KeyT>(max_bin, sorted);
   auto msd_width = [&](int delta) { return P0 < 0 ? -1 : std::min(16, std::max(0, P0 + delta)); };
   auto expand_again = [&]() {
-    launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[4] : nullptr, &sm->err, pctas, s);
+    launch_expand<KeyT>(records, NS, kpre, W, k, keys, NO, L, batched ? &sm->queues[4] : nullptr, &sm->err, pctas, s,
+                        NM, pay);
   };
   if (tune_now && P0 >= 0) {  // autotuner: time each MSD width, keep the fastest
     double best = 1e30;
@@ -503,7 +512,8 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
       if (tried != -2) expand_again();  // the previous try consumed the keys
       if (batched) CF1_CUDA(cudaMemsetAsync(&sm->queues[4], 0, sizeof(uint32_t), s));
       CF1_CUDA(cudaEventRecord(c->ev[10], s));
-      const bool ok = msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist_buf(), dist_off, be.msd, s, sorted);
+      const bool ok = msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, dist_buf(), dist_off, be.msd, s, sorted,
+                                            nullptr, nullptr, pay, pay_alt);
       CF1_CUDA(cudaEventRecord(c->ev[11], s));
       CF1_CUDA(cudaEventSynchronize(c->ev[11]));
       const double ms = elapsed(c->ev[10], c->ev[11]);
@@ -554,8 +564,10 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   // nothing on the path reads them, so the dense copy waits until a
   // verification or dump asks for it.
   KeyT *kept = nullptr;
+  uint8_t *kept_pay = nullptr;
   bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, l0_fuse ? nullptr : dist_buf(), dist_off,
-                                              be.msd, s, sorted, l0_fuse ? &l0 : nullptr, &kept);
+                                              be.msd, s, sorted, l0_fuse ? &l0 : nullptr, &kept, pay, pay_alt,
+                                              &kept_pay);
   c->msd_bits = done ? P : -1;
   if (tune_now) {
     tuned.sk_tile = c->tune.sk_tile;
@@ -579,6 +591,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   CF1_CUDA(cudaStreamSynchronize(s));
   const bool l0_ready = l0_fuse && done && l0_err == 0;
   const uint64_t nsub = done && P >= 0 ? (uint64_t)B << P : 0;
+  const bool joined = join3 && done && kept_pay != nullptr;  // phase 3 joined the occurrences' side sets
   if (l0_fuse && done && !l0_ready) {  // level 0 did not fit: the plain build reads the dense keys
     dist = dist_buf();
     msd_compact<KeyT>(kept, nsub, dist, be.msd, s);
@@ -610,11 +623,21 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   // once the MPHF is built (12 * nwords <= n_distinct + 11 <= 8 * (NO + 1)):
   // the key buffer, or the twin of the kept keys.
   const uint64_t nwords = ceil_div(c->n_distinct, 12);
-  const bool sideset = c->opts.state_update == 0;
+  const bool sideset = c->opts.state_update != 1;
   unsigned long long *states = c->d_states.get<unsigned long long>(nwords + 1);
-  uint32_t *sides = sideset ? reinterpret_cast<uint32_t *>(c->dist_pending ? twin : keys) : nullptr;
+  // joined: phase 3 left each distinct key's side-set byte beside it, and
+  // the other payload buffer takes the bytes in slot order
+  uint32_t *sides = !sideset ? nullptr
+                    : joined ? reinterpret_cast<uint32_t *>(kept_pay == pay ? pay_alt : pay)
+                             : reinterpret_cast<uint32_t *>(c->dist_pending ? twin : keys);
+  const KeyT *dense = c->dist_pending ? nullptr : c->d_dist.as<const KeyT>();
   if (sideset) {
-    CF1_CUDA(cudaMemsetAsync(sides, 0, nwords * 12, s));
+    if (joined) {  // every slot gets its byte; only the last word's unused tail is cleared
+      if (nwords * 12 > c->n_distinct)
+        CF1_CUDA(cudaMemsetAsync(reinterpret_cast<uint8_t *>(sides) + c->n_distinct, 0, nwords * 12 - c->n_distinct, s));
+    } else {
+      CF1_CUDA(cudaMemsetAsync(sides, 0, nwords * 12, s));
+    }
     CF1_CUDA(cudaMemsetAsync(states + nwords, 0, sizeof(unsigned long long), s));
   } else {
     CF1_CUDA(cudaMemsetAsync(states, 0, (nwords + 1) * sizeof(unsigned long long), s));
@@ -650,11 +673,17 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
         b1 = b0 + 1;
         while (b1 < B && hro[b1] < target) b1++;
       }
-      ClassifyArgs<KeyT> cs = ca;
-      cs.records = records + hro[b0];
-      cs.n_rec = hro[b1] - hro[b0];
-      if (batched) CF1_CUDA(cudaMemsetAsync(ca.queue, 0, sizeof(uint32_t), s));
-      launch_classify<KeyT>(cs, pctas, s);
+      if (joined) {
+        launch_place_sides<KeyT>(ca.mphf, kept, dense, kept_pay, be.msd.sb_off.template as<const uint64_t>(),
+                                 be.msd.cnt.template as<const uint32_t>(), be.msd.out_off.template as<const uint64_t>(),
+                                 (uint64_t)b0 << P, (uint64_t)b1 << P, P, reinterpret_cast<uint8_t *>(sides), &sm->err, s);
+      } else {
+        ClassifyArgs<KeyT> cs = ca;
+        cs.records = records + hro[b0];
+        cs.n_rec = hro[b1] - hro[b0];
+        if (batched) CF1_CUDA(cudaMemsetAsync(ca.queue, 0, sizeof(uint32_t), s));
+        launch_classify<KeyT>(cs, pctas, s);
+      }
       const uint64_t w_fin = b1 == B ? nwords : hdo[b1] / 12;
       if (w_fin > w_done) {
         if (sideset) launch_sideset_pack(sides, w_done, w_fin, states, s);
@@ -670,7 +699,12 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     CF1_CUDA(cudaStreamSynchronize(c->copy_stream));
     io->words_done = true;
   } else {
-    launch_classify<KeyT>(ca, pctas, s);
+    if (joined)
+      launch_place_sides<KeyT>(ca.mphf, kept, dense, kept_pay, be.msd.sb_off.template as<const uint64_t>(),
+                               be.msd.cnt.template as<const uint32_t>(), be.msd.out_off.template as<const uint64_t>(), 0,
+                               nsub, P, reinterpret_cast<uint8_t *>(sides), &sm->err, s);
+    else
+      launch_classify<KeyT>(ca, pctas, s);
     CF1_CUDA(cudaEventRecord(c->ev[6], s));
     if (sideset) launch_sideset_pack(sides, 0, nwords, states, s);
   }
@@ -710,6 +744,8 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   st.ms_phase3_mphf = elapsed(c->ev[3], c->ev[4]);
   st.ms_phase4 = elapsed(c->ev[4], c->ev[7]);
   st.ms_classify_kernel = elapsed(c->ev[5], c->ev[6]);
+  st.ms_dedup_kernel = done ? be.msd.ms_dedup : 0.0;
+  st.state_path = joined ? 0 : (c->opts.state_update == 1 ? 1 : 2);
   st.ms_total = elapsed(c->ev[0], c->ev[7]) + p1_before;
 }
 

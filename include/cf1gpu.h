@@ -79,9 +79,15 @@ typedef struct cf1gpu_opts {
   uint32_t sk_tile;           /* k-mer positions per minimizer tile: 1024, 2048 or 4096 (0 = tuner / default) */
   uint32_t sort_mode;         /* phase-3 sort: 0 = per-bin MSD + shared-memory sort (LSD when a sub-bucket
                                  overflows), 1 = segmented LSD radix sort only */
-  uint32_t state_update;      /* phase-4 state update: 0 = side-set bytes joined by atomic OR, then packed;
-                                 1 = atomicCAS loop on the packed words (src/state_vector.rs:47-70).
-                                 Both give the same words. */
+  uint32_t state_update;      /* how the vertex states are formed, all giving the same words:
+                                 0 = each k-mer occurrence's side-set byte travels with its key through the
+                                 phase-3 sort, whose dedup ORs a vertex's occurrences together; phase 4 then
+                                 puts each distinct key's byte in its slot and packs the words (with the LSD
+                                 sort, which carries no bytes, phase 4 falls back to mode 2);
+                                 1 = phase 4 classifies every occurrence with an atomicCAS loop on the
+                                 packed words (src/state_vector.rs:47-70);
+                                 2 = phase 4 classifies every occurrence into side-set bytes by atomic OR,
+                                 then packs them */
   uint32_t shard_index;       /* bin sharding over shard_count devices: this context keeps the bins b with
                                  b % shard_count == shard_index for phases 3-4 (phases 1-2 still route the
                                  whole input, so every shard sees the same partition); slots, states and
@@ -108,7 +114,9 @@ typedef struct cf1gpu_stats {
   uint64_t sort_msd_bits;      /* top bits the MSD sort split bins on; UINT64_MAX when the LSD path ran */
   uint64_t tuner_state;        /* 0 no autotuner, 1 parameters from the cache, 2 measured in this run */
   uint64_t sk_tile;            /* phase-1 tile this run used */
-  uint64_t reserved_u[2];
+  uint64_t state_path;         /* how the last run formed the states: 0 joined in phase 3, 1 CAS classification,
+                                  2 side-set classification (state_update, or 2 when the LSD sort ran) */
+  uint64_t reserved_u[1];
   double ms_h2d;               /* host->device copy of the input */
   double ms_phase1;            /* pack + minimizer histogram + partition */
   double ms_phase2;            /* super k-mer routing */
@@ -116,8 +124,9 @@ typedef struct cf1gpu_stats {
   double ms_phase3_mphf;       /* MPHF construction (+ bijection check) */
   double ms_phase4;            /* classification */
   double ms_total;             /* device time of phases 1-4 (excludes h2d) */
-  double ms_classify_kernel;   /* the classification kernel alone */
-  double reserved_d[4];
+  double ms_classify_kernel;   /* the phase-4 kernel alone: classification, or the placing of joined side sets */
+  double ms_dedup_kernel;      /* the phase-3 shared-memory sort / dedup kernel alone (0 when the LSD path ran) */
+  double reserved_d[3];
 } cf1gpu_stats;
 
 /* Fills defaults: k 31, 128 bins, device 0, BBHash, not batched. */

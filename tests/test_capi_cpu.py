@@ -57,6 +57,17 @@ def test_invalid_bins_rejected():
         assert L.cf1gpu_create(C.byref(o), C.byref(h)) == cg.ERR_INVALID_ARG
 
 
+def test_invalid_state_update_rejected():
+    L = cg.lib()
+    o = cg.Opts()
+    L.cf1gpu_default_opts(C.byref(o))
+    assert o.state_update == 0  # side sets joined in phase 3 by default
+    o.state_update = 3
+    h = C.c_void_p()
+    assert L.cf1gpu_create(C.byref(o), C.byref(h)) == cg.ERR_INVALID_ARG
+    assert b"state_update" in L.cf1gpu_last_error(None)
+
+
 def test_null_arguments():
     L = cg.lib()
     assert L.cf1gpu_create(None, None) == cg.ERR_INVALID_ARG

@@ -50,7 +50,8 @@ def test_phase5_reproduces_golden_output():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("k", K_VALUES)
-@pytest.mark.parametrize("mode,update", [("bbhash", "sideset"), ("learned", "sideset"), ("bbhash", "cas")])
+@pytest.mark.parametrize("mode,update", [("bbhash", "phase3"), ("learned", "phase3"), ("bbhash", "sideset"),
+                                         ("learned", "sideset"), ("bbhash", "cas")])
 def test_gpu_reproduces_golden_states(k, mode, update):
     g = load(k)
     run = gpu_run(g["seq"], g["offsets"], k, mode=mode, state_update=update, num_bins=16)

@@ -56,17 +56,34 @@ def test_sort_modes(k, sort_mode):
 @pytest.mark.parametrize("mode", ["bbhash", "learned"])
 @pytest.mark.parametrize("k", [5, 31, 33, 63])
 def test_state_update_modes(k, mode):
-    # side-set OR + pack and the CAS loop on packed words give the same words
+    # side sets joined by the phase-3 dedup, side-set OR per occurrence + pack,
+    # and the CAS loop on packed words all give the same words
     recs = random_records(900 + k, k, n_records=120, max_len=5000)
     seq, off = o.concat_records(recs)
     words = {}
-    for upd in ("sideset", "cas"):
+    for upd in ("phase3", "sideset", "cas"):
         g, _ = assert_parity(seq, off, k, mode=mode, num_bins=16, state_update=upd)
         words[upd] = g.states()
-        if upd == "sideset":
+        if upd != "cas":
             assert g.stats()["classify_cas_retries"] == 0
         g.close()
+    assert np.array_equal(words["phase3"], words["cas"])
     assert np.array_equal(words["sideset"], words["cas"])
+
+
+@pytest.mark.parametrize("mode", ["bbhash", "learned"])
+def test_phase3_join_with_lsd_fallback_and_oversized_subbuckets(mode):
+    # The LSD sort carries no side-set bytes: phase 4 then classifies the
+    # occurrences.  Long homopolymers and tandem repeats put thousands of
+    # copies of a few keys in one sub-bucket, where the dedup's joins and the
+    # sorted path's runs of equal keys do the work.
+    rng = np.random.default_rng(77)
+    recs = [b"A" * 20000, b"AT" * 9000, (b"ACGTTGCA" * 3000), bytes(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 50000)])]
+    recs.append(recs[-1][1000:9000][::-1].translate(bytes.maketrans(b"ACGT", b"TGCA")))
+    seq, off = o.concat_records(recs)
+    for sort_mode in ("msd", "lsd"):
+        g, _ = assert_parity(seq, off, 31, mode=mode, num_bins=4, sort_mode=sort_mode)
+        g.close()
 
 
 def _pinned_copy(a):
