@@ -338,10 +338,24 @@ struct ExactMap {
     return (uint64_t)(it - keys.begin());
   }
   uint64_t hash(u128 key) const {  // absent keys map to 0, like `unwrap_or(0)`
+    if (memo_map == this && memo_key == key) return memo_idx;
     const uint64_t r = rank(key);
     return r == ~0ull ? 0 : r;
   }
+  // A caller that already knows a key's rank (the partitioned run walks its
+  // occurrences in key order) leaves it here for this thread's next lookups.
+  static thread_local const ExactMap *memo_map;
+  static thread_local u128 memo_key;
+  static thread_local uint64_t memo_idx;
+  void remember(u128 key, uint64_t idx) const {
+    memo_map = this;
+    memo_key = key;
+    memo_idx = idx;
+  }
 };
+thread_local const ExactMap *ExactMap::memo_map = nullptr;
+thread_local u128 ExactMap::memo_key = 0;
+thread_local uint64_t ExactMap::memo_idx = 0;
 
 // Partition of a canonical k-mer for checks too large to hold at once: a
 // 64-bit mix of its words scaled to [0, nparts).  The classifier's updates of
@@ -964,24 +978,124 @@ struct PartResult {
   double t_collect = 0, t_sort = 0, t_classify = 0;
 };
 
+// An occurrence of the partition: its canonical k-mer and the input position
+// of its window.
 template <class KW>
-void collect_part(const KSpec &ks, const PartIndex &x, uint32_t part, int nthreads, std::vector<KW> &all,
-                  uint64_t &n_occ) {
-  const uint64_t n = x.in.off[x.in.n_rec];
+struct Occ {
+  KW key;
+  uint64_t pos;
+};
+
+// Sorts the occurrences by key (one split on the top 12 of key_bits bits,
+// then every bucket sorted on its own thread); bstart[0..4096] gets the
+// buckets' bounds.
+template <class KW>
+void par_sort_occ(std::vector<Occ<KW>> &v, int key_bits, int nthreads, std::vector<uint64_t> &bstart) {
+  const int BB = 12;
+  const uint32_t NB = 1u << BB;
+  const int sh = key_bits > BB ? key_bits - BB : 0;
+  auto bucket = [&](const Occ<KW> &x) { return (uint32_t)((u128)x.key >> sh) & (NB - 1); };
+  const size_t n = v.size();
+  const int nt = std::max(1, nthreads);
+  const size_t chunk = (n + nt - 1) / nt;
+  std::vector<std::vector<uint64_t>> hist(nt, std::vector<uint64_t>(NB, 0));
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++) th.emplace_back([&, t] {
+    size_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+    for (size_t i = a; i < b; i++) hist[t][bucket(v[i])]++;
+  });
+  for (auto &x : th) x.join();
+  th.clear();
+  bstart.assign(NB + 1, 0);
+  uint64_t off = 0;
+  for (uint32_t d = 0; d < NB; d++) {
+    bstart[d] = off;
+    for (int t = 0; t < nt; t++) { uint64_t c = hist[t][d]; hist[t][d] = off; off += c; }
+  }
+  bstart[NB] = off;
+  std::vector<Occ<KW>> tmp(n);
+  for (int t = 0; t < nt; t++) th.emplace_back([&, t] {
+    size_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+    auto &h = hist[t];
+    for (size_t i = a; i < b; i++) tmp[h[bucket(v[i])]++] = v[i];
+  });
+  for (auto &x : th) x.join();
+  parallel_for(NB, nt, [&](uint64_t d) {
+    std::sort(tmp.data() + bstart[d], tmp.data() + bstart[d + 1],
+              [](const Occ<KW> &a, const Occ<KW> &b) { return a.key < b.key; });
+  });
+  v.swap(tmp);
+}
+
+// The partition's occurrences in key order and its sorted distinct keys;
+// then the Classifier's step for every occurrence, a key's occurrences in a
+// row on one thread (the key's rank is known, so the slot lookup is served
+// from the map's memo, and the key's state word stays in cache).
+template <class KW>
+void run_part_keyed(const KSpec &ks, const PartIndex &x, uint32_t part, int nthreads, PartResult *r,
+                    std::vector<KW> &keys) {
+  const Input &in = x.in;
+  const uint64_t n = in.off[in.n_rec];
   const uint64_t nb = (n + PBLK - 1) / PBLK;
-  std::vector<std::vector<KW>> per(nb);
-  (void)ks;
-  for_part_windows(x, part, nthreads, [&](uint64_t b, uint64_t, uint64_t, u128 fw, u128 rc) {
-    per[b].push_back((KW)canonical_with_rc(fw, rc));
+  double t0 = now_s();
+  std::vector<std::vector<Occ<KW>>> per(nb);
+  for_part_windows(x, part, nthreads, [&](uint64_t b, uint64_t rec, uint64_t p, u128 fw, u128 rc) {
+    per[b].push_back(Occ<KW>{(KW)canonical_with_rc(fw, rc), in.off[rec] + p});
   });
   std::vector<uint64_t> off(nb + 1, 0);
   for (uint64_t b = 0; b < nb; b++) off[b + 1] = off[b] + per[b].size();
-  n_occ = off[nb];
-  all.resize(n_occ);
+  r->n_occ = off[nb];
+  std::vector<Occ<KW>> occ(r->n_occ);
   parallel_for(nb, nthreads, [&](uint64_t b) {
-    std::memcpy(all.data() + off[b], per[b].data(), per[b].size() * sizeof(KW));
-    std::vector<KW>().swap(per[b]);
+    std::memcpy(occ.data() + off[b], per[b].data(), per[b].size() * sizeof(Occ<KW>));
+    std::vector<Occ<KW>>().swap(per[b]);
   });
+  double t1 = now_s();
+  r->t_collect = t1 - t0;
+  std::vector<uint64_t> bstart;
+  par_sort_occ(occ, 2 * ks.k, nthreads, bstart);
+  const uint32_t NB = (uint32_t)bstart.size() - 1;
+  std::vector<uint64_t> ucnt(NB, 0), uoff(NB + 1, 0);
+  parallel_for(NB, nthreads, [&](uint64_t d) {
+    uint64_t c = 0;
+    for (uint64_t i = bstart[d]; i < bstart[d + 1]; i++) c += i == bstart[d] || occ[i].key != occ[i - 1].key;
+    ucnt[d] = c;
+  });
+  for (uint32_t d = 0; d < NB; d++) uoff[d + 1] = uoff[d] + ucnt[d];
+  keys.resize(uoff[NB]);
+  parallel_for(NB, nthreads, [&](uint64_t d) {
+    uint64_t o = uoff[d];
+    for (uint64_t i = bstart[d]; i < bstart[d + 1]; i++)
+      if (i == bstart[d] || occ[i].key != occ[i - 1].key) keys[o++] = occ[i].key;
+  });
+  r->t_sort = now_s() - t1;
+  double t2 = now_s();
+  r->map.build_dir(2 * ks.k);
+  AtomicStateVector states(r->map.size());
+  Classifier cls(ks, r->map, states);
+  cls.part = part;
+  cls.nparts = x.nparts;
+  parallel_for(NB, nthreads, [&](uint64_t d) {
+    uint64_t rank = uoff[d];
+    const uint64_t e = bstart[d + 1];
+    for (uint64_t i = bstart[d]; i < e; i++) {
+      if (i + 16 < e) __builtin_prefetch(in.seq + occ[i + 16].pos);
+      if (i > bstart[d] && occ[i].key != occ[i - 1].key) rank++;
+      const uint64_t pos = occ[i].pos;
+      const uint64_t rec = (uint64_t)(std::upper_bound(in.off, in.off + in.n_rec + 1, pos) - in.off) - 1;
+      const uint8_t *s = in.seq + in.off[rec];
+      const uint64_t p = pos - in.off[rec];
+      const u128 fw = from_ascii(ks, s, p);
+      r->map.remember(occ[i].key, rank);
+      cls.process_at(s, in.off[rec + 1] - in.off[rec], p, fw, reverse_complement(ks, fw));
+    }
+  });
+  r->states.resize(r->map.size());
+  parallel_for((r->map.size() + 4095) / 4096, nthreads, [&](uint64_t b) {
+    const uint64_t a = b * 4096, e2 = std::min<uint64_t>(r->map.size(), a + 4096);
+    for (uint64_t i = a; i < e2; i++) r->states[i] = states.get(i);
+  });
+  r->t_classify = now_s() - t2;
 }
 
 PartResult *run_part(const PartIndex &x, uint32_t part, int nthreads) {
@@ -991,36 +1105,12 @@ PartResult *run_part(const PartIndex &x, uint32_t part, int nthreads) {
   r->k = k;
   r->part = part;
   r->nparts = x.nparts;
-  double t0 = now_s();
   if (k <= 32) {
     r->map.narrow = true;
-    collect_part<uint64_t>(ks, x, part, nthreads, r->map.keys64, r->n_occ);
-    double t1 = now_s();
-    r->t_collect = t1 - t0;
-    par_sort_unique(r->map.keys64, 2 * k, nthreads);
-    r->t_sort = now_s() - t1;
+    run_part_keyed<uint64_t>(ks, x, part, nthreads, r, r->map.keys64);
   } else {
-    collect_part<u128>(ks, x, part, nthreads, r->map.keys, r->n_occ);
-    double t1 = now_s();
-    r->t_collect = t1 - t0;
-    par_sort_unique(r->map.keys, 2 * k, nthreads);
-    r->t_sort = now_s() - t1;
+    run_part_keyed<u128>(ks, x, part, nthreads, r, r->map.keys);
   }
-  double t2 = now_s();
-  r->map.build_dir(2 * k);
-  AtomicStateVector states(r->map.size());
-  Classifier cls(ks, r->map, states);
-  cls.part = part;
-  cls.nparts = x.nparts;
-  for_part_windows(x, part, nthreads, [&](uint64_t, uint64_t rec, uint64_t p, u128 fw, u128 rc) {
-    cls.process_at(x.in.seq + x.in.off[rec], x.in.off[rec + 1] - x.in.off[rec], p, fw, rc);
-  });
-  r->states.resize(r->map.size());
-  parallel_for((r->map.size() + 4095) / 4096, nthreads, [&](uint64_t b) {
-    const uint64_t a = b * 4096, e = std::min<uint64_t>(r->map.size(), a + 4096);
-    for (uint64_t i = a; i < e; i++) r->states[i] = states.get(i);
-  });
-  r->t_classify = now_s() - t2;
   return r;
 }
 
