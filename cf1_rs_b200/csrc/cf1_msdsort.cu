@@ -543,6 +543,7 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
     CsDigit plain{shift, bits, 0, 0, 0u};
     if (jend - j > 1) {  // a packed run: bucket = place of the sub-bucket in the run, then the next bits
       const uint32_t span = (uint32_t)(jend - j);
+      if (span > CS_BUCKETS) return ~0u;  // the plan never makes one; refused (LSD path) rather than mis-bucketed
       int g = 0;
       while ((1u << g) < span) g++;
       const int rest = shift + bits;  // the sub-bucket prefix sits at bits [rest, rest + P)
@@ -656,9 +657,13 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
 }
 
 // Chunk plan of the sorted form: per bin (one thread), runs of consecutive
-// sub-buckets packed greedily up to cap keys (a sub-bucket above cap is a run
-// of its own), written as (first, end) sub-bucket indices within the bin to
-// clist[bin << P ...]; ccount[bin] = the bin's runs.
+// sub-buckets packed greedily up to cap keys and at most CS_BUCKETS
+// sub-buckets (the run's counting sort buckets a key by its sub-bucket's
+// place in the run first; sparse stretches of the key space -- canonical
+// k-mers starting with TTT... -- hold thousands of near-empty sub-buckets at
+// wide splits), a sub-bucket above cap keys being a run of its own, written as
+// (first, end) sub-bucket indices within the bin to clist[bin << P ...];
+// ccount[bin] = the bin's runs.
 __global__ void cs_plan_kernel(const uint64_t *sb_off, uint32_t nbins, int P, uint32_t cap, uint2 *clist,
                                uint32_t *ccount) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -670,7 +675,7 @@ __global__ void cs_plan_kernel(const uint64_t *sb_off, uint32_t nbins, int P, ui
   uint64_t acc = 0;
   for (uint32_t q = 0; q < per; q++) {
     const uint64_t sz = o[q + 1] - o[q];
-    if (acc > 0 && acc + sz > cap) {
+    if ((acc > 0 && acc + sz > cap) || q - start == CS_BUCKETS) {
       out[nc++] = make_uint2(start, q);
       start = q;
       acc = 0;

@@ -71,6 +71,21 @@ def test_state_update_modes(k, mode):
     assert np.array_equal(words["sideset"], words["cas"])
 
 
+def test_sorted_runs_over_sparse_key_ranges(tmp_path):
+    """One bin of ~12M k-mer occurrences; the autotuner's first run tries
+    split widths up to 16 bits (65,536 sub-buckets).  Canonical k-mers are
+    rare at the top of the key space (starting TTG.., TTT..: a few keys per
+    sub-bucket), so there the sorted dedup's packed runs are limited by their
+    1,024-sub-bucket bucket range rather than by their key capacity."""
+    rng = np.random.default_rng(404)
+    s = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 12_000_000)].tobytes()
+    seq, off = o.concat_records([s[:7_000_000], s[7_000_000:]])
+    cache = str(tmp_path / "tuner.txt")
+    g, _ = assert_parity(seq, off, 31, mode="learned", num_bins=1, tuner_cache=cache)
+    assert g.stats()["tuner_state"] == 2  # this run measured the widths
+    g.close()
+
+
 @pytest.mark.parametrize("mode", ["bbhash", "learned"])
 def test_phase3_join_with_lsd_fallback_and_oversized_subbuckets(mode):
     # The LSD sort carries no side-set bytes: phase 4 then classifies the
