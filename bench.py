@@ -83,6 +83,9 @@ def parse():
                    help="N > 1: scan 1/N of the input per rank and swap records, or route it all on every rank")
     p.add_argument("--tuner-cache", default=os.path.join(tempfile.gettempdir(), "cf1_tuner_cache.txt"),
                    help="autotuner cache file (first warm-up run of an input class measures; '' = off)")
+    p.add_argument("--state-update", choices=["phase3", "sideset", "cas"], default="phase3",
+                   help="how the states are formed (library state_update): joined in the phase-3 dedup, or "
+                        "classified per occurrence in phase 4 (side-set OR / CAS loop)")
     p.add_argument("--verify", choices=["auto", "on", "off"], default="auto",
                    help="after the timed steps, check every form's per-k-mer states on the whole workload against "
                         "the CPU oracle (auto: on with 1 GPU)")
@@ -341,7 +344,7 @@ def gpu_arm(args):
     for form in args.forms.split(","):
         batched = form == "learned"
         copts = dict(mode=form, batched=batched, track_short_seqs=bool(wl.get("short")), tuner_cache=tuner_path,
-                     learned_leaf_size=args.leaf_size)
+                     learned_leaf_size=args.leaf_size, state_update=args.state_update)
         be = sharded.GpuExchangeBackend(k, bins, rank, world, device=local, **copts) if xchg else None
         g = be.ctx if xchg else cg.Cf1Gpu(k=k, num_bins=bins, device=local, shard_index=rank, shard_count=world,
                                           **copts)
@@ -391,7 +394,8 @@ def gpu_arm(args):
             ms_classify_kernel=maxall(statistics.mean(ms_cls)), ms_dedup_kernel=maxall(statistics.mean(ms_dd)),
             launches=launches, stats=s,
             phases_ms={k2: round(v, 3) for k2, v in phase.items()},
-            learned=g.learned_stats() if form == "learned" else None, ctx=g, be=be, dump=dump)
+            learned=g.learned_stats() if form == "learned" else None, ctx=g, be=be, dump=dump,
+            image_bytes=g.mphf_image_bytes())
         if form != args.forms.split(",")[-1]:
             g.close()
             forms[form]["ctx"] = None
@@ -408,7 +412,7 @@ def gpu_arm(args):
         g, be = head["ctx"], head["be"]
         if g is None:
             copts = dict(mode=head_name, batched=head_name == "learned", track_short_seqs=bool(wl.get("short")),
-                         tuner_cache=tuner_path, learned_leaf_size=args.leaf_size)
+                         tuner_cache=tuner_path, learned_leaf_size=args.leaf_size, state_update=args.state_update)
             be = sharded.GpuExchangeBackend(k, bins, rank, world, device=local, **copts) if xchg else None
             g = be.ctx if xchg else cg.Cf1Gpu(k=k, num_bins=bins, device=local, shard_index=rank,
                                               shard_count=world, **copts)
@@ -512,6 +516,8 @@ def gpu_arm(args):
         "forms": {f: {"value": v["value"], "ms_per_step": v["ms_per_step"],
                       "ms_classify_kernel": v["ms_classify_kernel"], "phases_ms": v["phases_ms"],
                       "bbhash_levels": int(v["stats"]["bbhash_levels"]), "mphf_bytes": int(v["stats"]["mphf_bytes"]),
+                      "mphf_image_bytes": int(v["image_bytes"]), "state_path": int(v["stats"]["state_path"]),
+                      "ms_dedup_kernel": v["ms_dedup_kernel"],
                       "sort": ("lsd" if v["stats"]["sort_msd_bits"] == 2**64 - 1
                                else f"msd{v['stats']['sort_msd_bits']}"),
                       "learned_bins": int(v["stats"]["learned_bins"]), "fallback_bins": int(v["stats"]["fallback_bins"]),

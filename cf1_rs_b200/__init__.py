@@ -378,6 +378,12 @@ class Cf1Gpu:
             with open(os.path.join(work_dir, f"cf1_bin_{b:05d}.bin"), "wb") as f:
                 f.write(self.export_bin(b))
 
+    def mphf_image_bytes(self) -> int:
+        """Size of the host image export_mphf would copy."""
+        need = C.c_size_t(0)
+        self._check(lib().cf1gpu_export_mphf(self.h, None, C.byref(need)))
+        return int(need.value)
+
     def export_mphf(self) -> np.ndarray:
         need = C.c_size_t(0)
         self._check(lib().cf1gpu_export_mphf(self.h, None, C.byref(need)))

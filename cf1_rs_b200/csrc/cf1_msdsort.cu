@@ -857,7 +857,10 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
       uint2 *cl = sc.clist.get<uint2>(nsub);
       uint32_t *cc = sc.ccount.get<uint32_t>(nbins + 1);
       uint64_t *co = sc.coff.get<uint64_t>(nbins + 1);
-      cs_plan_kernel<<<(unsigned)ceil_div(nbins, 128), 128, 0, s>>>(sb_off, nbins, P, cap, cl, cc);
+      // runs of up to 2/3 of the capacity: the shared-memory set of the
+      // dedup (a power of two >= 1.5 n slots, filled to 3/4 at most) then
+      // always holds the run, so it never falls back to sorting copies
+      cs_plan_kernel<<<(unsigned)ceil_div(nbins, 128), 128, 0, s>>>(sb_off, nbins, P, cap * 2 / 3, cl, cc);
       CF1_LAUNCH_CHECK();
       exclusive_scan_u32(cc, co, nbins, sc.scan_tmp, s);
       CF1_CUDA(cudaMemcpyAsync(&grid, co + nbins, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
