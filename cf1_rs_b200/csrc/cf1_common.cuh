@@ -83,6 +83,19 @@ struct KOps<uint64_t> {
     uint64_t top = s ? ((w0 << s) | (w1 >> (64 - s))) : w0;
     return top >> (64 - 2 * k);
   }
+  // The same, and from the words it reads the base after the k-mer (next,
+  // base p + k); prev (base p - 1) needs one more word only when p starts a
+  // word.  want_prev: the caller knows base p - 1 exists.
+  static CF1_HD uint64_t extract_nb(const uint64_t *W, uint64_t p, int k, bool want_prev, uint32_t &prev,
+                                    uint32_t &next) {
+    uint64_t i = p >> 5;
+    int s = (int)(p & 31) * 2;
+    uint64_t w0 = W[i], w1 = W[i + 1];
+    uint64_t top = s ? ((w0 << s) | (w1 >> (64 - s))) : w0;  // bases p .. p + 31
+    next = (uint32_t)(top >> (62 - 2 * k)) & 3;               // k <= 31
+    prev = want_prev ? (s ? (uint32_t)(w0 >> (64 - s)) & 3 : (uint32_t)W[i - 1] & 3) : 0;
+    return top >> (64 - 2 * k);
+  }
   static CF1_HD uint64_t rc(uint64_t x, int k) { return rev_bases64(~x) >> (64 - 2 * k); }
   static CF1_HD uint64_t mask(int k) { return k >= 32 ? ~0ull : ((1ull << (2 * k)) - 1); }
   static CF1_HD void roll(uint64_t &fw, uint64_t &rcv, uint32_t base, int k) {
@@ -116,6 +129,23 @@ struct KOps<Key2> {
     uint64_t w0 = W[i], w1 = W[i + 1], w2 = W[i + 2];
     uint64_t t0 = s ? ((w0 << s) | (w1 >> (64 - s))) : w0;
     uint64_t t1 = s ? ((w1 << s) | (w2 >> (64 - s))) : w1;
+    int sh = 128 - 2 * k;  // 2..62
+    Key2 r;
+    r.hi = t0 >> sh;
+    r.lo = (t1 >> sh) | (t0 << (64 - sh));
+    return r;
+  }
+  // The same, and the bases after (p + k) and before (p - 1) the k-mer, as
+  // KOps<uint64_t>::extract_nb.
+  static CF1_HD Key2 extract_nb(const uint64_t *W, uint64_t p, int k, bool want_prev, uint32_t &prev,
+                                uint32_t &next) {
+    uint64_t i = p >> 5;
+    int s = (int)(p & 31) * 2;
+    uint64_t w0 = W[i], w1 = W[i + 1], w2 = W[i + 2];
+    uint64_t t0 = s ? ((w0 << s) | (w1 >> (64 - s))) : w0;  // bases p .. p + 31
+    uint64_t t1 = s ? ((w1 << s) | (w2 >> (64 - s))) : w1;  // bases p + 32 .. p + 63
+    next = (uint32_t)(t1 >> (62 - 2 * (k - 32))) & 3;       // 33 <= k <= 63
+    prev = want_prev ? (s ? (uint32_t)(w0 >> (64 - s)) & 3 : (uint32_t)W[i - 1] & 3) : 0;
     int sh = 128 - 2 * k;  // 2..62
     Key2 r;
     r.hi = t0 >> sh;

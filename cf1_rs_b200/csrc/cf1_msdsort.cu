@@ -120,11 +120,17 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
   // used, and the keys stay in registers for the staging step
   constexpr bool HOLD = KOps<KeyT>::WORDS == 1;
   KeyT kk[HOLD ? MS_ITEMS : 1];
+  // the payload bytes are loaded with the keys, four to a register, so their
+  // latency is not paid again when the tile is staged
+  uint32_t pb[MS_ITEMS / 4];
+#pragma unroll
+  for (int q = 0; q < MS_ITEMS / 4; q++) pb[q] = 0;
   if constexpr (HOLD) {
 #pragma unroll
     for (int r = 0; r < MS_ITEMS; r++) {
       uint32_t li = warp * (MS_ITEMS * 32) + r * 32 + lane;
       kk[r] = li < n ? in[sp.start + li] : KeyT{};
+      if (pin && li < n) pb[r >> 2] |= (uint32_t)pin[sp.start + li] << (8 * (r & 3));
     }
   }
 #pragma unroll
@@ -170,7 +176,7 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
       uint32_t d = pk[r] & 0xFF, li = warp * (MS_ITEMS * 32) + r * 32 + lane;
       const uint32_t at = lstart[d] + wh[d] + (pk[r] >> 8);
       stage[at] = HOLD ? kk[HOLD ? r : 0] : in[sp.start + li];
-      if (pin) pstage[at] = pin[sp.start + li];
+      if (pin) pstage[at] = HOLD ? (uint8_t)(pb[r >> 2] >> (8 * (r & 3))) : pin[sp.start + li];
     }
   }
   __syncthreads();
@@ -245,12 +251,13 @@ CF1_D uint32_t cs_hash_dedup(uint64_t *T, uint64_t a, uint64_t n, uint64_t *S, u
     bool added = false;
     if (i < n) {
       const uint64_t key = T[a + i];
+      const uint32_t pay = TP ? TP[a + i] : 0u;  // loaded beside the key, not after the probe
       uint32_t h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - tbits));  // multiplicative hashing
       for (uint32_t probe = 0; probe < tsize; probe++) {
         unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long *>(S + h), EMPTY, key);
         if (old == EMPTY || old == key) {
           added = old == EMPTY;
-          if (TP) atomicOr(&SPw[h >> 2], (uint32_t)TP[a + i] << (8 * (h & 3)));
+          if (TP) atomicOr(&SPw[h >> 2], pay << (8 * (h & 3)));
           break;
         }
         h = (h + 1) & (tsize - 1);

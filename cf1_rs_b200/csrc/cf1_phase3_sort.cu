@@ -69,16 +69,21 @@ __global__ void __launch_bounds__(256) expand_kernel(const uint64_t *records, ui
         uint32_t t = j - oex;
         if (ooff + t < n_keys && opos + t + k <= L) {
           const uint64_t p = opos + t;
-          KeyT fw = KOps<KeyT>::extract(W, p, k);
-          KeyT rc = KOps<KeyT>::rc(fw, k);
-          keys[ooff + t] = kmin(fw, rc);
           if (sides) {
             // inside a super k-mer the windows before and after are valid, so
-            // only its first and last k-mers can lack a neighbour
+            // only its first and last k-mers can lack a neighbour; the
+            // neighbours come from the words the k-mer is read from
             const bool hp = t > 0 || (p > 0 && !is_n(NM, p - 1));
             const bool hn = t + 1 < onrec || (p + k < L && !is_n(NM, p + k));
-            const uint32_t pb = hp ? base_at(W, p - 1) : 0, nb = hn ? base_at(W, p + k) : 0;
-            sides[ooff + t] = (uint8_t)sideset_lookup(contribution(fw, rc, hp, pb, hn, nb, k));
+            uint32_t pb, nb;
+            KeyT fw = KOps<KeyT>::extract_nb(W, p, k, hp, pb, nb);
+            KeyT rc = KOps<KeyT>::rc(fw, k);
+            keys[ooff + t] = kmin(fw, rc);
+            sides[ooff + t] = (uint8_t)sideset_lookup(contribution(fw, rc, hp, pb, hn, hn ? nb : 0u, k));
+          } else {
+            KeyT fw = KOps<KeyT>::extract(W, p, k);
+            KeyT rc = KOps<KeyT>::rc(fw, k);
+            keys[ooff + t] = kmin(fw, rc);
           }
         } else {
           atomicOr(err, (uint32_t)DEV_OVERFLOW);

@@ -162,8 +162,11 @@ __global__ void __launch_bounds__(CL_BLOCK_DEFER) classify_defer_kernel(Classify
 
 // One warp per sub-bucket: each distinct key's side-set byte to its slot.
 // A learned bin's slot is the key's rank, which the dense layout already
-// gives; a BBHash bin walks the levels (one probe for most keys, in the bin's
-// block, which the neighbouring warps share).
+// gives; a BBHash bin probes level 0 first for PL_U keys per lane at once
+// (independent loads in flight: one probe after another would leave the
+// warp waiting on each), then walks the deeper levels for the ~12% level 0
+// did not place.
+constexpr int PL_U = 4;
 template <class KeyT>
 __global__ void __launch_bounds__(256) place_sides_kernel(MphfView<KeyT> m, const KeyT *kept, const KeyT *dense,
                                                           const uint8_t *kept_pay, const uint64_t *sb_off,
@@ -174,19 +177,54 @@ __global__ void __launch_bounds__(256) place_sides_kernel(MphfView<KeyT> m, cons
   const uint32_t c = cnt[j], bin = (uint32_t)(j >> P);
   const uint64_t a = sb_off[j], o = out_off[j], base = m.dist_off[bin], end = m.dist_off[bin + 1];
   const bool ranked = m.learned && m.li.roots[bin].use_learned;
+  const unsigned lane = lane_id();
   bool miss = false;
-  for (uint32_t i = lane_id(); i < c; i += 32) {
-    uint64_t slot;
-    if (ranked) {
-      slot = o + i;
-    } else {
-      const uint64_t local = bb_local_slot(m.bb, bin, dense ? dense[o + i] : kept[a + i]);
-      slot = local == SLOT_NONE ? SLOT_NONE : base + local;
+  if (ranked) {
+    for (uint32_t i = lane; i < c; i += 32) sides[o + i] = kept_pay[a + i];
+  } else {
+    const BBMeta m0 = m.bb.levels ? m.bb.meta[bin] : BBMeta{};  // level 0 of this bin
+    for (uint32_t i0 = 0; i0 < c; i0 += 32 * PL_U) {
+      uint64_t H[PL_U];
+      uint8_t pay[PL_U];
+      ulonglong2 e[PL_U];
+      uint32_t bit[PL_U];
+#pragma unroll
+      for (int u = 0; u < PL_U; u++) {
+        const uint32_t i = i0 + u * 32 + lane;
+        H[u] = 0;
+        pay[u] = 0;
+        if (i < c) {
+          H[u] = bb_key_hash(dense ? dense[o + i] : kept[a + i]);
+          pay[u] = kept_pay[a + i];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < PL_U; u++) {
+        const uint32_t i = i0 + u * 32 + lane;
+        e[u] = make_ulonglong2(0ull, 0ull);
+        bit[u] = 0;
+        if (i < c && m0.nwords) {
+          const uint64_t pos = bb_pos(H[u], 0, m0.nwords);
+          e[u] = m.bb.AR[m0.word_off + (pos >> 6)];
+          bit[u] = (uint32_t)(pos & 63);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < PL_U; u++) {
+        const uint32_t i = i0 + u * 32 + lane;
+        if (i >= c) continue;
+        uint64_t local;
+        if ((e[u].x >> bit[u]) & 1)
+          local = (uint32_t)(m0.rank_adj + (uint32_t)e[u].y + (uint32_t)popc64(e[u].x & ((1ull << bit[u]) - 1)));
+        else
+          local = m0.nwords ? bb_walk(m.bb, bin, H[u], 1, m.bb.levels) : SLOT_NONE;
+        const uint64_t slot = local == SLOT_NONE ? SLOT_NONE : base + local;
+        if (slot < end && slot >= base) sides[slot] = pay[u];
+        else miss = true;
+      }
     }
-    if (slot < end && slot >= base) sides[slot] = kept_pay[a + i];
-    else miss = true;
   }
-  if (__any_sync(FULL, miss) && lane_id() == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
+  if (__any_sync(FULL, miss) && lane == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
 }
 
 // Word w of the state vector from side-set bytes 12w .. 12w+11 (three u32).
