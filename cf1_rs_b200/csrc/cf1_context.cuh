@@ -76,6 +76,9 @@ struct cf1gpu_ctx {
       d_keys, d_dist, d_dist_off, d_states, d_scan, d_seen, d_qin, d_qout, d_queue;
   // state_update 0: one side-set byte per key beside the sort's two key buffers
   cf1::DevBuf d_pay, d_pay_alt;
+  // ... and, with BBHash level 0 built by the dedup, the bytes of the keys it
+  // leaves and the placed count of every slice
+  cf1::DevBuf d_l0survpay, d_l0placed;
   uint64_t rec_cap_hint = 0;  // phase-1 record list size of the last run
   // exchange-based sharding: the scanned slice's records wait in d_keys for
   // routing; d_xsend holds them grouped by owner shard, d_xcnt the counts

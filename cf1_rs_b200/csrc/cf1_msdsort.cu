@@ -435,9 +435,12 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
 // each; lb: lb_cap u16 of shared memory for the keys' bits in the slice (a
 // slice has at most L0_SW_MAX * 64 < 2^16 bits).  All threads call it.
 constexpr uint32_t L0_SW_MAX = 768;
+// With kpay (the keys' joined payload bytes) and o.with_pay, the payloads go
+// out as Level0Out describes; pw: L0_SW_MAX u32 of shared memory.
 CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const Level0Out &o,
                     unsigned long long *set, unsigned long long *col, uint16_t *lb, uint32_t lb_cap, uint32_t *sm,
-                    unsigned long long *s_base) {
+                    unsigned long long *s_base, const uint8_t *kpay, uint64_t a, uint32_t *pw) {
+  const bool pay = o.with_pay && kpay;
   const unsigned tid = threadIdx.x;
   const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
   const uint64_t W = o.woff[bin + 1] - o.woff[bin];
@@ -445,10 +448,14 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
   if (n == 0) {  // every slice writes all its entries (the array is not cleared first)
     for (uint32_t w = tid; w < sw; w += CS_BLOCK)
       o.AR[o.woff[bin] + (uint64_t)sub * sw + w] = make_ulonglong2(0ull, 0ull);
+    if (pay && tid == 0) o.placed[j] = 0;
     return;
   }
   if (sw > L0_SW_MAX || sw == 0 || n > lb_cap) {
-    if (tid == 0) atomicOr(o.err, 1u);
+    if (tid == 0) {
+      atomicOr(o.err, 1u);
+      if (pay) o.placed[j] = 0;
+    }
     return;
   }
   const uint64_t first = o.woff[bin] + (uint64_t)sub * sw;  // the slice's first entry
@@ -468,6 +475,26 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
   }
   __syncthreads();
   for (uint32_t w = tid; w < sw; w += CS_BLOCK) o.AR[first + w] = make_ulonglong2(set[w] & ~col[w], 0ull);
+  if (pay) {
+    // a placed key's rank in the slice: the placed bits before its bit
+    // (words 2t and 2t+1 per thread: sw <= L0_SW_MAX <= 2 CS_BLOCK)
+    const uint32_t w0 = 2 * tid, w1 = w0 + 1;
+    const uint32_t c0 = w0 < sw ? (uint32_t)popc64(set[w0] & ~col[w0]) : 0u;
+    const uint32_t c1 = w1 < sw ? (uint32_t)popc64(set[w1] & ~col[w1]) : 0u;
+    uint32_t placed_tot;
+    const uint32_t pre_w = block_exclusive_scan<CS_BLOCK>(c0 + c1, sm, placed_tot);
+    if (w0 < sw) pw[w0] = pre_w;
+    if (w1 < sw) pw[w1] = pre_w + c0;
+    if (tid == 0) o.placed[j] = placed_tot;
+    __syncthreads();
+    for (uint32_t i = tid; i < n; i += CS_BLOCK) {
+      const uint32_t b = lb[i];
+      if (b == 0xFFFF) continue;
+      const uint64_t fin = set[b >> 6] & ~col[b >> 6];
+      const uint64_t bit = 1ull << (b & 63);
+      if (fin & bit) o.l0pay[a + pw[b >> 6] + (uint32_t)popc64(fin & (bit - 1))] = kpay[i];
+    }
+  }
   // the keys whose bit collided go on to level 1
   uint32_t c = 0;
   for (uint32_t i = tid; i < n; i += CS_BLOCK) {
@@ -492,7 +519,10 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
     uint64_t out = o.surv_off[bin] + *s_base + pre;
     for (uint32_t i = tid; i < n; i += CS_BLOCK) {
       const uint32_t b = lb[i];
-      if (b != 0xFFFF && ((col[b >> 6] >> (b & 63)) & 1)) o.surv[out++] = keys[i];
+      if (b != 0xFFFF && ((col[b >> 6] >> (b & 63)) & 1)) {
+        if (pay) o.surv_pay[out] = kpay[i];
+        o.surv[out++] = keys[i];
+      }
     }
   }
   __syncthreads();
@@ -658,7 +688,8 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
       __syncthreads();
       unsigned long long *h64 = reinterpret_cast<unsigned long long *>(hist);
       l0_slice(reinterpret_cast<const uint64_t *>(T) + a, res, j, P, l0, h64, h64 + L0_SW_MAX,
-               reinterpret_cast<uint16_t *>(S), CAP * sizeof(KeyT) / 2, sm, &s_l0base);
+               reinterpret_cast<uint16_t *>(S), CAP * sizeof(KeyT) / 2, sm, &s_l0base, TP ? TP + a : nullptr, a,
+               SPw);
     }
   }
 }
@@ -794,7 +825,8 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted) {
 template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
                      KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted,
-                     const Level0Out *l0, KeyT **kept, uint8_t *pkeys, uint8_t *palt, uint8_t **kept_pay) {
+                     const Level0Out *l0, KeyT **kept, uint8_t *pkeys, uint8_t *palt, uint8_t **kept_pay,
+                     uint8_t **l0pay_buf) {
   uint8_t *PT = pkeys;  // payloads beside T (nullptr: keys carry none)
   // passes on the top P bits: P1 then P2 (P2 may be 0) -- of the key, or of
   // its hash when only distinct keys are wanted (64-bit keys)
@@ -849,9 +881,12 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
   CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   KeyT *U = T == keys ? alt : keys;
   uint8_t *PU = pkeys ? (PT == pkeys ? palt : pkeys) : nullptr;
+  if (l0pay_buf) *l0pay_buf = PU;
   if (nsub) {
     Level0Out lo;
     if (l0 && hashed) lo = *l0;
+    lo.with_pay = lo.with_pay && PT != nullptr;
+    lo.l0pay = PU;
     for (auto &e : sc.ev)
       if (!e) CF1_CUDA(cudaEventCreate(&e));
     // sorted form: consecutive small sub-buckets of a bin are packed into
@@ -901,7 +936,7 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
   template int msd_prefix_bits<KT>(uint64_t, bool);                                                                     \
   template bool msd_sort_unique<KT>(KT *, KT *, uint64_t, const uint64_t *, uint32_t, int, int, KT *, uint64_t *, \
                                     MsdScratch &, cudaStream_t, bool, const Level0Out *, KT **, uint8_t *,    \
-                                    uint8_t *, uint8_t **);                                                   \
+                                    uint8_t *, uint8_t **, uint8_t **);                                       \
   template void msd_compact<KT>(const KT *, uint64_t, KT *, MsdScratch &, cudaStream_t);
 CF1_INST(uint64_t)
 CF1_INST(Key2)

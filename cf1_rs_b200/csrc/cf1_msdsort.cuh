@@ -40,6 +40,14 @@ struct Level0Out {
   const uint64_t *surv_off = nullptr;      // [nbins + 1]; bin b's room is surv_off[b+1] - surv_off[b]
   unsigned long long *surv_cnt = nullptr;  // [nbins], zeroed
   uint32_t *err = nullptr;                 // set when a slice or a bin's room is too small
+  // Joined side sets (payload bytes beside the keys): a key level 0 places
+  // gets local rank r inside its slice (the set bits before its bit), and
+  // its byte goes to l0pay[sub-bucket start + r]; placed[j] = the slice's
+  // placed keys; a key level 0 leaves takes its byte along to surv_pay.
+  bool with_pay = false;
+  uint8_t *l0pay = nullptr;    // filled by msd_sort_unique: the payload buffer the kept bytes are not in
+  uint8_t *surv_pay = nullptr; // beside surv
+  uint32_t *placed = nullptr;  // [nsub]
 };
 
 // With dist = nullptr the distinct keys stay where the dedup left them, at
@@ -52,7 +60,7 @@ template <class KeyT>
 bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off, uint32_t nbins, int key_bits, int P,
                      KeyT *dist, uint64_t *dist_off, MsdScratch &sc, cudaStream_t s, bool sorted = true,
                      const Level0Out *l0 = nullptr, KeyT **kept = nullptr, uint8_t *pkeys = nullptr,
-                     uint8_t *palt = nullptr, uint8_t **kept_pay = nullptr);
+                     uint8_t *palt = nullptr, uint8_t **kept_pay = nullptr, uint8_t **l0pay_buf = nullptr);
 
 // The deferred copy: distinct keys of the last msd_sort_unique (nsub
 // sub-buckets, left in `kept`) to dist, bins in order.

@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) expand_kernel(const uint64_t *records, ui
             KeyT fw = KOps<KeyT>::extract_nb(W, p, k, hp, pb, nb);
             KeyT rc = KOps<KeyT>::rc(fw, k);
             keys[ooff + t] = kmin(fw, rc);
-            sides[ooff + t] = (uint8_t)sideset_lookup(contribution(fw, rc, hp, pb, hn, hn ? nb : 0u, k));
+            sides[ooff + t] = (uint8_t)contribution_sideset(fw, rc, hp, pb, hn, hn ? nb : 0u, k);
           } else {
             KeyT fw = KOps<KeyT>::extract(W, p, k);
             KeyT rc = KOps<KeyT>::rc(fw, k);

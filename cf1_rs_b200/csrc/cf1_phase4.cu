@@ -227,6 +227,45 @@ __global__ void __launch_bounds__(256) place_sides_kernel(MphfView<KeyT> m, cons
   if (__any_sync(FULL, miss) && lane == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
 }
 
+// One warp per sub-bucket: the level-0 keys' bytes, already in rank order,
+// to the slice's run of slots.
+__global__ void __launch_bounds__(256) place_l0_kernel(BBView bb, const uint64_t *dist_off, const uint64_t *sb_off,
+                                                       const uint32_t *placed, const uint8_t *l0pay, uint64_t j0,
+                                                       uint64_t j1, int P, uint8_t *sides, uint32_t *err) {
+  const uint64_t j = j0 + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (j >= j1) return;
+  const uint32_t np = placed[j];
+  if (!np) return;
+  const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
+  const BBMeta m0 = bb.meta[bin];
+  const uint64_t first = m0.word_off + (uint64_t)sub * (m0.nwords >> P);
+  const uint64_t base = dist_off[bin] + (uint32_t)(m0.rank_adj + (uint32_t)bb.AR[first].y);
+  if (base + np > dist_off[bin + 1]) {
+    if (lane_id() == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
+    return;
+  }
+  const uint8_t *src = l0pay + sb_off[j];
+  for (uint32_t r = lane_id(); r < np; r += 32) sides[base + r] = src[r];
+}
+
+// The keys level 0 left: SV_CTAS CTAs per bin, each key walks from level 1.
+constexpr uint32_t SV_CTAS = 32;
+__global__ void __launch_bounds__(256) place_surv_kernel(BBView bb, const uint64_t *dist_off, const uint64_t *surv,
+                                                         const uint8_t *surv_pay, const uint64_t *surv_off,
+                                                         const unsigned long long *surv_cnt, uint32_t b0,
+                                                         uint8_t *sides, uint32_t *err) {
+  const uint32_t bin = b0 + blockIdx.x / SV_CTAS, part = blockIdx.x % SV_CTAS;
+  const uint64_t n = surv_cnt[bin], s0 = surv_off[bin], base = dist_off[bin], end = dist_off[bin + 1];
+  bool miss = false;
+  for (uint64_t i = (uint64_t)part * blockDim.x + threadIdx.x; i < n; i += (uint64_t)SV_CTAS * blockDim.x) {
+    const uint64_t local = bb_walk(bb, bin, bb_key_hash(surv[s0 + i]), 1, bb.levels);
+    const uint64_t slot = local == SLOT_NONE ? SLOT_NONE : base + local;
+    if (slot >= base && slot < end) sides[slot] = surv_pay[s0 + i];
+    else miss = true;
+  }
+  if (__syncthreads_or(miss) && threadIdx.x == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
+}
+
 // Word w of the state vector from side-set bytes 12w .. 12w+11 (three u32).
 constexpr int PK_BLOCK = 256;
 __global__ void __launch_bounds__(PK_BLOCK) sideset_pack_kernel(const uint32_t *sides, uint64_t w0, uint64_t w1,
@@ -324,6 +363,24 @@ void launch_place_sides(const MphfView<KeyT> &m, const KeyT *kept, const KeyT *d
   if (j1 <= j0) return;
   place_sides_kernel<KeyT><<<(unsigned)ceil_div((j1 - j0) * 32, 256), 256, 0, s>>>(
       m, kept, dense, kept_pay, sb_off, cnt, out_off, j0, j1, P, sides, err);
+  CF1_LAUNCH_CHECK();
+}
+
+void launch_place_l0(const BBView &bb, const uint64_t *dist_off, const uint64_t *sb_off, const uint32_t *placed,
+                     const uint8_t *l0pay, uint64_t j0, uint64_t j1, int P, uint8_t *sides, uint32_t *err,
+                     cudaStream_t s) {
+  if (j1 <= j0) return;
+  place_l0_kernel<<<(unsigned)ceil_div((j1 - j0) * 32, 256), 256, 0, s>>>(bb, dist_off, sb_off, placed, l0pay, j0, j1,
+                                                                          P, sides, err);
+  CF1_LAUNCH_CHECK();
+}
+
+void launch_place_surv(const BBView &bb, const uint64_t *dist_off, const uint64_t *surv, const uint8_t *surv_pay,
+                       const uint64_t *surv_off, const unsigned long long *surv_cnt, uint32_t b0, uint32_t b1,
+                       uint8_t *sides, uint32_t *err, cudaStream_t s) {
+  if (b1 <= b0) return;
+  place_surv_kernel<<<(b1 - b0) * SV_CTAS, 256, 0, s>>>(bb, dist_off, surv, surv_pay, surv_off, surv_cnt, b0, sides,
+                                                        err);
   CF1_LAUNCH_CHECK();
 }
 

@@ -559,15 +559,20 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     l0.surv_off = room_off;
     l0.surv_cnt = scnt;
     l0.err = &sm->l0_err;
+    if (join3) {  // joined side sets: level 0 places its keys' bytes by rank (see Level0Out)
+      l0.with_pay = true;
+      l0.surv_pay = c->d_l0survpay.get<uint8_t>(l0_room + 1);
+      l0.placed = c->d_l0placed.get<uint32_t>(((uint64_t)B << P) + 1);
+    }
   }
   // The BBHash form leaves the distinct keys in their sub-buckets (kept):
   // nothing on the path reads them, so the dense copy waits until a
   // verification or dump asks for it.
   KeyT *kept = nullptr;
-  uint8_t *kept_pay = nullptr;
+  uint8_t *kept_pay = nullptr, *l0pay = nullptr;
   bool done = P >= 0 && msd_sort_unique<KeyT>(keys, alt, NO, seg, B, 2 * k, P, l0_fuse ? nullptr : dist_buf(), dist_off,
                                               be.msd, s, sorted, l0_fuse ? &l0 : nullptr, &kept, pay, pay_alt,
-                                              &kept_pay);
+                                              &kept_pay, &l0pay);
   c->msd_bits = done ? P : -1;
   if (tune_now) {
     tuned.sk_tile = c->tune.sk_tile;
@@ -627,10 +632,28 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   unsigned long long *states = c->d_states.get<unsigned long long>(nwords + 1);
   // joined: phase 3 left each distinct key's side-set byte beside it, and
   // the other payload buffer takes the bytes in slot order
+  // (with level 0 placed by rank, the other payload buffer holds the level-0
+  // bytes in rank order, so the free sort buffer takes the slots)
+  const bool joined_l0 = joined && l0_ready;
   uint32_t *sides = !sideset ? nullptr
-                    : joined ? reinterpret_cast<uint32_t *>(kept_pay == pay ? pay_alt : pay)
-                             : reinterpret_cast<uint32_t *>(c->dist_pending ? twin : keys);
-  const KeyT *dense = c->dist_pending ? nullptr : c->d_dist.as<const KeyT>();
+                    : (joined && !joined_l0) ? reinterpret_cast<uint32_t *>(kept_pay == pay ? pay_alt : pay)
+                                             : reinterpret_cast<uint32_t *>(c->dist_pending ? twin : keys);
+  // the phase-4 work of a stage of bins [b0, b1)
+  auto place = [&](uint32_t b0, uint32_t b1) {
+    uint8_t *sb = reinterpret_cast<uint8_t *>(sides);
+    const uint64_t *sbo = be.msd.sb_off.template as<const uint64_t>();
+    if (joined_l0) {
+      launch_place_l0(be.bb.view(), dist_off, sbo, l0.placed, l0pay, (uint64_t)b0 << P, (uint64_t)b1 << P, P, sb,
+                      &sm->err, s);
+      launch_place_surv(be.bb.view(), dist_off, reinterpret_cast<const uint64_t *>(l0.surv), l0.surv_pay, l0.surv_off,
+                        l0.surv_cnt, b0, b1, sb, &sm->err, s);
+    } else {
+      launch_place_sides<KeyT>(make_view<KeyT>(c), kept, c->dist_pending ? nullptr : c->d_dist.as<const KeyT>(),
+                               kept_pay, sbo, be.msd.cnt.template as<const uint32_t>(),
+                               be.msd.out_off.template as<const uint64_t>(), (uint64_t)b0 << P, (uint64_t)b1 << P, P, sb,
+                               &sm->err, s);
+    }
+  };
   if (sideset) {
     if (joined) {  // every slot gets its byte; only the last word's unused tail is cleared
       if (nwords * 12 > c->n_distinct)
@@ -674,9 +697,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
         while (b1 < B && hro[b1] < target) b1++;
       }
       if (joined) {
-        launch_place_sides<KeyT>(ca.mphf, kept, dense, kept_pay, be.msd.sb_off.template as<const uint64_t>(),
-                                 be.msd.cnt.template as<const uint32_t>(), be.msd.out_off.template as<const uint64_t>(),
-                                 (uint64_t)b0 << P, (uint64_t)b1 << P, P, reinterpret_cast<uint8_t *>(sides), &sm->err, s);
+        place(b0, b1);
       } else {
         ClassifyArgs<KeyT> cs = ca;
         cs.records = records + hro[b0];
@@ -700,9 +721,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     io->words_done = true;
   } else {
     if (joined)
-      launch_place_sides<KeyT>(ca.mphf, kept, dense, kept_pay, be.msd.sb_off.template as<const uint64_t>(),
-                               be.msd.cnt.template as<const uint32_t>(), be.msd.out_off.template as<const uint64_t>(), 0,
-                               nsub, P, reinterpret_cast<uint8_t *>(sides), &sm->err, s);
+      place(0, B);
     else
       launch_classify<KeyT>(ca, pctas, s);
     CF1_CUDA(cudaEventRecord(c->ev[6], s));
