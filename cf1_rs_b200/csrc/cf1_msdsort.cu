@@ -549,7 +549,8 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
                                                                   uint64_t nsub, int shift, int bits, uint32_t *cnt,
                                                                   uint32_t *oversize, int P, Level0Out l0,
                                                                   uint8_t *TP, uint8_t *UP, const uint2 *clist,
-                                                                  const uint64_t *coff, uint32_t nbins) {
+                                                                  const uint64_t *coff, uint32_t nbins,
+                                                                  const uint32_t *jlist) {
   constexpr uint32_t CAP = cs_cap<KeyT, SORTED>();
   constexpr bool L0 = !SORTED && KOps<KeyT>::WORDS == 1;
   __shared__ unsigned long long s_l0base;
@@ -564,7 +565,10 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
   __shared__ int s_big, s_nchunks, s_bad;
   __shared__ uint32_t s_cnt;
   uint64_t j = blockIdx.x, jend = j + 1;
-  if (clist) {
+  if (jlist) {  // the sub-buckets the warp dedup left
+    j = jlist[blockIdx.x];
+    jend = j + 1;
+  } else if (clist) {
     const uint32_t bin = upper_segment(coff, nbins, (uint64_t)blockIdx.x);
     const uint2 r = clist[((uint64_t)bin << P) + (blockIdx.x - coff[bin])];
     j = ((uint64_t)bin << P) + r.x;
@@ -694,6 +698,167 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
   }
 }
 
+// ---------------------------------------------------------------- warp dedup
+// The unsorted (BBHash) form's dedup, one warp per sub-bucket and no block
+// barriers: sub-buckets of a few hundred keys (the split of key *
+// KEY_SPREAD_MUL spreads them evenly), a private 512-slot open-addressing set
+// per warp in shared memory, and, with level 0 on, the sub-bucket's slice of
+// BBHash level 0 marked, written and ranked by the same warp.  A warp walks
+// the sub-buckets j = warp, warp + all warps, ...  A sub-bucket with more
+// than WD_MAXD distinct keys (or a slice above WD_SWMAX words) is left
+// untouched and listed in ov for the block kernel.
+constexpr int WD_WARPS = 8;                 // warps per CTA
+constexpr uint32_t WD_TW = 512;             // set slots per warp
+constexpr uint32_t WD_MAXD = WD_TW / 4 * 3; // distinct keys a warp's set takes
+constexpr uint32_t WD_SWMAX = 64;           // level-0 slice words a warp takes
+struct WdSmem {
+  unsigned long long tab[WD_TW];
+  uint8_t tpay[WD_TW];
+  uint16_t ins[WD_MAXD];                    // slots in insertion order
+  unsigned long long set[WD_SWMAX], col[WD_SWMAX];
+  uint32_t pw[WD_SWMAX];                    // placed bits before each word
+};
+
+__global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T, uint8_t *TP, const uint64_t *sb_off,
+                                                                   uint64_t nsub, int P, uint32_t *cnt, Level0Out l0,
+                                                                   uint32_t *ov, uint32_t *ov_cnt) {
+  extern __shared__ __align__(16) unsigned char wd_smem[];
+  WdSmem &m = reinterpret_cast<WdSmem *>(wd_smem)[threadIdx.x >> 5];
+  const unsigned lane = lane_id(), lt = lanemask_lt();
+  const unsigned long long EMPTY = ~0ull;  // above every key (keys use at most 62 bits)
+  const bool pay = TP != nullptr, lv0 = l0.AR != nullptr, lpay = lv0 && l0.with_pay && pay;
+  for (uint32_t i = lane; i < WD_TW; i += 32) {
+    m.tab[i] = EMPTY;
+    m.tpay[i] = 0;
+  }
+  __syncwarp();
+  const uint64_t nwarps = (uint64_t)gridDim.x * WD_WARPS;
+  for (uint64_t j = (uint64_t)blockIdx.x * WD_WARPS + (threadIdx.x >> 5); j < nsub; j += nwarps) {
+    const uint64_t a = sb_off[j], n = sb_off[j + 1] - a;
+    const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
+    uint64_t W = 0, first = 0;
+    uint32_t sw = 0;
+    if (lv0) {
+      W = l0.woff[bin + 1] - l0.woff[bin];
+      sw = (uint32_t)(W >> P);
+      first = l0.woff[bin] + (uint64_t)sub * sw;
+    }
+    bool over = lv0 && sw > WD_SWMAX;
+    // 1. one copy of each key, its copies' payloads ORed
+    uint32_t d = 0;
+    for (uint64_t base = 0; base < n && !over; base += 32) {
+      const uint64_t i = base + lane;
+      bool claimed = false;
+      uint32_t h = 0;
+      if (i < n) {
+        const unsigned long long key = T[a + i];
+        const uint32_t p = pay ? TP[a + i] : 0u;
+        h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 55);  // top 9 bits: WD_TW = 512
+        for (uint32_t probe = 0; probe < WD_TW; probe++) {
+          const unsigned long long old = atomicCAS(&m.tab[h], EMPTY, key);
+          if (old == EMPTY || old == key) {
+            claimed = old == EMPTY;
+            if (pay) atomicOr(reinterpret_cast<uint32_t *>(m.tpay) + (h >> 2), p << (8 * (h & 3)));
+            break;
+          }
+          h = (h + 1) & (WD_TW - 1);
+        }
+      }
+      const unsigned b = __ballot_sync(FULL, claimed);
+      const uint32_t r = d + __popc(b & lt);
+      if (claimed && r < WD_MAXD) m.ins[r] = (uint16_t)h;
+      d += __popc(b);
+      over = d > WD_MAXD;
+    }
+    __syncwarp();
+    if (over) {  // left to the block kernel: clear the whole set, list j
+      for (uint32_t i = lane; i < WD_TW; i += 32) {
+        m.tab[i] = EMPTY;
+        m.tpay[i] = 0;
+      }
+      if (lane == 0) ov[atomicAdd(ov_cnt, 1u)] = (uint32_t)j;
+      __syncwarp();
+      continue;
+    }
+    // 2. the distinct keys (and bytes) to T[a, a + d); the set is emptied
+    for (uint32_t r = lane; r < d; r += 32) {
+      const uint32_t h = m.ins[r];
+      T[a + r] = m.tab[h];
+      if (pay) TP[a + r] = m.tpay[h];
+      m.tab[h] = EMPTY;
+      m.tpay[h] = 0;
+    }
+    if (lane == 0) cnt[j] = d;
+    __syncwarp();
+    if (!lv0) continue;
+    // 3. level 0: mark the slice, clear collided bits, write it
+    const uint64_t lo_bit = (uint64_t)sub * sw * 64;
+    for (uint32_t w = lane; w < sw; w += 32) m.set[w] = m.col[w] = 0;
+    __syncwarp();
+    bool bad = false;
+    for (uint32_t r = lane; r < d; r += 32) {
+      const uint64_t b = bb_pos(T[a + r], 0, (uint32_t)W) - lo_bit;
+      if (b >= (uint64_t)sw * 64) {  // not this slice's key: cannot happen with the shared hash
+        bad = true;
+        continue;
+      }
+      const unsigned long long bit = 1ull << (b & 63);
+      if (atomicOr(&m.set[b >> 6], bit) & bit) atomicOr(&m.col[b >> 6], bit);
+    }
+    if (__any_sync(FULL, bad) && lane == 0) atomicOr(l0.err, 1u);
+    __syncwarp();
+    // placed bits per word, and their exclusive prefix (sw <= 64: two words a lane)
+    const unsigned long long f0 = lane < sw ? m.set[lane] & ~m.col[lane] : 0ull;
+    const unsigned long long f1 = lane + 32 < sw ? m.set[lane + 32] & ~m.col[lane + 32] : 0ull;
+    if (lane < sw) l0.AR[first + lane] = make_ulonglong2(f0, 0ull);
+    if (lane + 32 < sw) l0.AR[first + lane + 32] = make_ulonglong2(f1, 0ull);
+    const uint32_t c0 = (uint32_t)__popcll(f0), c1 = (uint32_t)__popcll(f1);
+    const uint32_t i0 = warp_inclusive_scan(c0), i1 = warp_inclusive_scan(c1);
+    const uint32_t t0 = __shfl_sync(FULL, i0, 31), placed = t0 + __shfl_sync(FULL, i1, 31);
+    if (lane < sw) m.pw[lane] = i0 - c0;
+    if (lane + 32 < sw) m.pw[lane + 32] = t0 + i1 - c1;
+    if (lpay && lane == 0) l0.placed[j] = placed;
+    // survivors: one reservation in the bin's list
+    unsigned long long sbase = 0;
+    if (lane == 0 && d > placed) {
+      sbase = atomicAdd(&l0.surv_cnt[bin], (unsigned long long)(d - placed));
+      if (sbase + (d - placed) > l0.surv_off[bin + 1] - l0.surv_off[bin]) {
+        atomicOr(l0.err, 1u);
+        sbase = ~0ull;
+      }
+    }
+    sbase = __shfl_sync(FULL, sbase, 0);
+    __syncwarp();
+    // 4. each key: its byte to its rank (placed) or the key to level 1
+    uint64_t so = l0.surv_off[bin] + sbase;
+    for (uint32_t r0 = 0; r0 < d; r0 += 32) {
+      const uint32_t r = r0 + lane;
+      bool surv = false;
+      uint64_t key = 0;
+      if (r < d) {
+        key = T[a + r];
+        const uint64_t b = bb_pos(key, 0, (uint32_t)W) - lo_bit;
+        if (b < (uint64_t)sw * 64) {
+          const unsigned long long fin = m.set[b >> 6] & ~m.col[b >> 6], bit = 1ull << (b & 63);
+          if (fin & bit) {
+            if (lpay) l0.l0pay[a + m.pw[b >> 6] + (uint32_t)__popcll(fin & (bit - 1))] = TP[a + r];
+          } else {
+            surv = true;
+          }
+        }
+      }
+      const unsigned sb = __ballot_sync(FULL, surv);
+      if (surv && sbase != ~0ull) {
+        const uint64_t at = so + __popc(sb & lt);
+        l0.surv[at] = key;
+        if (lpay) l0.surv_pay[at] = TP[a + r];
+      }
+      so += __popc(sb);
+    }
+    __syncwarp();
+  }
+}
+
 // Chunk plan of the sorted form: per bin (one thread), runs of consecutive
 // sub-buckets packed greedily up to cap keys and at most CS_BUCKETS
 // sub-buckets (the run's counting sort buckets a key by its sub-bucket's
@@ -815,8 +980,10 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted) {
   // size run several times over it (the first bases of canonical k-mers are
   // skewed ~5x), so 64-bit keys aim lower to stay within shared memory
   // (3.1 Gbp, k = 31: 14 bits instead of 12, phase 3 245 -> 230 ms).
-  const uint64_t target = sorted && KOps<KeyT>::WORDS == 1 ? cs_cap<KeyT, true>() / 8
-                                                            : cs_cap_for(KOps<KeyT>::WORDS == 2, sorted) / 2;
+  // The unsorted 64-bit form (a warp per sub-bucket, WD_MAXD distinct keys
+  // at most) aims at a third of a warp's set for the largest bin.
+  const uint64_t target = KOps<KeyT>::WORDS == 1 ? (sorted ? cs_cap<KeyT, true>() / 8 : WD_MAXD / 2)
+                                                 : cs_cap_for(true, sorted) / 2;
   int p = 0;
   while (p < 16 && (max_bin_keys >> p) > target) p++;
   return p;
@@ -911,9 +1078,32 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
       coff = co;
     }
     CF1_CUDA(cudaEventRecord(sc.ev[0], s));
-    kern<<<(unsigned)grid, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over, P, lo, PT,
-                                                PU, clist, coff, nbins);
-    CF1_LAUNCH_CHECK();
+    if (hashed) {
+      // the unsorted form: one warp per sub-bucket; the few it cannot hold
+      // (more than WD_MAXD distinct keys) go to the block kernel after it
+      uint32_t *ov = sc.ov.get<uint32_t>(nsub + 1);
+      uint32_t *ovc = sc.ovc.get<uint32_t>(1);
+      CF1_CUDA(cudaMemsetAsync(ovc, 0, sizeof(uint32_t), s));
+      const size_t wsm = WD_WARPS * sizeof(WdSmem);
+      CF1_CUDA(cudaFuncSetAttribute(wd_dedup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+      const unsigned wgrid = persistent_grid(wd_dedup_kernel, WD_WARPS * 32, wsm, -1, ceil_div(nsub, WD_WARPS));
+      wd_dedup_kernel<<<wgrid, WD_WARPS * 32, wsm, s>>>(reinterpret_cast<uint64_t *>(T), PT, sb_off, nsub, P, cnt, lo,
+                                                        ov, ovc);
+      CF1_LAUNCH_CHECK();
+      uint32_t h_ov = 0;
+      CF1_CUDA(cudaMemcpyAsync(&h_ov, ovc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+      CF1_CUDA(cudaStreamSynchronize(s));
+      sc.last_overflow = h_ov;
+      if (h_ov) {
+        kern<<<h_ov, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over, P, lo, PT, PU,
+                                          nullptr, nullptr, nbins, ov);
+        CF1_LAUNCH_CHECK();
+      }
+    } else {
+      kern<<<(unsigned)grid, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over, P, lo, PT,
+                                                  PU, clist, coff, nbins, nullptr);
+      CF1_LAUNCH_CHECK();
+    }
     CF1_CUDA(cudaEventRecord(sc.ev[1], s));
   }
   uint32_t h_over = 0;

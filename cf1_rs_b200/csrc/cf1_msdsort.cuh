@@ -6,7 +6,8 @@
 namespace cf1 {
 
 struct MsdScratch {
-  DevBuf tile_off, hist, hscan, scan_tmp, sb_off, sb_off1, cnt, out_off, flag, clist, ccount, coff;
+  DevBuf tile_off, hist, hscan, scan_tmp, sb_off, sb_off1, cnt, out_off, flag, clist, ccount, coff, ov, ovc;
+  uint32_t last_overflow = 0;  // sub-buckets the last unsorted run left to the block kernel
   cudaEvent_t ev[2] = {nullptr, nullptr};  // around the last dedup kernel launch
   float ms_dedup = 0;                      // its device time
   ~MsdScratch() {
