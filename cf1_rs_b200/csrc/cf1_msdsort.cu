@@ -703,159 +703,189 @@ __global__ void __launch_bounds__(CS_BLOCK, SORTED ? 2 : 4) cs_sort_unique_kerne
 // barriers: sub-buckets of a few hundred keys (the split of key *
 // KEY_SPREAD_MUL spreads them evenly), a private 512-slot open-addressing set
 // per warp in shared memory, and, with level 0 on, the sub-bucket's slice of
-// BBHash level 0 marked, written and ranked by the same warp.  A warp walks
-// the sub-buckets j = warp, warp + all warps, ...  A sub-bucket with more
-// than WD_MAXD distinct keys (or a slice above WD_SWMAX words) is left
-// untouched and listed in ov for the block kernel.
+// BBHash level 0 marked, written and ranked by the same warp.  A warp takes
+// runs of WD_RUN consecutive sub-buckets from a work counter (their offsets,
+// keys and bins are then read in order, and uneven bins still balance).  A
+// sub-bucket with more than WD_MAXD distinct keys (or a slice
+// above WD_SWMAX words) is left untouched and listed in ov for the block
+// kernel.
 constexpr int WD_WARPS = 8;                 // warps per CTA
 constexpr uint32_t WD_TW = 512;             // set slots per warp
 constexpr uint32_t WD_MAXD = WD_TW / 4 * 3; // distinct keys a warp's set takes
 constexpr uint32_t WD_SWMAX = 64;           // level-0 slice words a warp takes
+constexpr int WD_U = 4;                     // key loads in flight per lane
+constexpr uint32_t WD_RUN = 64;             // sub-buckets a warp takes at a time
 struct WdSmem {
   unsigned long long tab[WD_TW];
   uint8_t tpay[WD_TW];
-  uint16_t ins[WD_MAXD];                    // slots in insertion order
+  uint16_t ins[WD_MAXD];                    // slots in insertion order, then the keys' level-0 bits
+  uint8_t dp[WD_MAXD];                      // the distinct keys' joined payloads
   unsigned long long set[WD_SWMAX], col[WD_SWMAX];
   uint32_t pw[WD_SWMAX];                    // placed bits before each word
 };
 
 __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T, uint8_t *TP, const uint64_t *sb_off,
                                                                    uint64_t nsub, int P, uint32_t *cnt, Level0Out l0,
-                                                                   uint32_t *ov, uint32_t *ov_cnt) {
+                                                                   uint32_t *ov, uint32_t *ov_cnt, uint32_t *queue) {
   extern __shared__ __align__(16) unsigned char wd_smem[];
   WdSmem &m = reinterpret_cast<WdSmem *>(wd_smem)[threadIdx.x >> 5];
   const unsigned lane = lane_id(), lt = lanemask_lt();
   const unsigned long long EMPTY = ~0ull;  // above every key (keys use at most 62 bits)
   const bool pay = TP != nullptr, lv0 = l0.AR != nullptr, lpay = lv0 && l0.with_pay && pay;
+  constexpr uint16_t NO_BIT = 0xFFFF;      // a key outside its slice (cannot happen with the shared hash)
   for (uint32_t i = lane; i < WD_TW; i += 32) {
     m.tab[i] = EMPTY;
     m.tpay[i] = 0;
   }
   __syncwarp();
-  const uint64_t nwarps = (uint64_t)gridDim.x * WD_WARPS;
-  for (uint64_t j = (uint64_t)blockIdx.x * WD_WARPS + (threadIdx.x >> 5); j < nsub; j += nwarps) {
-    const uint64_t a = sb_off[j], n = sb_off[j + 1] - a;
-    const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
-    uint64_t W = 0, first = 0;
-    uint32_t sw = 0;
-    if (lv0) {
-      W = l0.woff[bin + 1] - l0.woff[bin];
-      sw = (uint32_t)(W >> P);
-      first = l0.woff[bin] + (uint64_t)sub * sw;
-    }
-    bool over = lv0 && sw > WD_SWMAX;
-    // 1. one copy of each key, its copies' payloads ORed
-    uint32_t d = 0;
-    for (uint64_t base = 0; base < n && !over; base += 32) {
-      const uint64_t i = base + lane;
-      bool claimed = false;
-      uint32_t h = 0;
-      if (i < n) {
-        const unsigned long long key = T[a + i];
-        const uint32_t p = pay ? TP[a + i] : 0u;
-        h = (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 55);  // top 9 bits: WD_TW = 512
-        for (uint32_t probe = 0; probe < WD_TW; probe++) {
-          const unsigned long long old = atomicCAS(&m.tab[h], EMPTY, key);
-          if (old == EMPTY || old == key) {
-            claimed = old == EMPTY;
-            if (pay) atomicOr(reinterpret_cast<uint32_t *>(m.tpay) + (h >> 2), p << (8 * (h & 3)));
-            break;
+  const uint64_t nruns = (nsub + WD_RUN - 1) / WD_RUN;
+  for (;;) {
+    uint32_t run = 0;
+    if (lane == 0) run = atomicAdd(queue, 1u);
+    run = __shfl_sync(FULL, run, 0);
+    if (run >= nruns) break;
+    const uint64_t j0 = (uint64_t)run * WD_RUN, j1 = j0 + WD_RUN < nsub ? j0 + WD_RUN : nsub;
+    for (uint64_t j = j0; j < j1; j++) {
+      const uint64_t a = sb_off[j], n = sb_off[j + 1] - a;
+      const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
+      uint64_t W = 0, first = 0;
+      uint32_t sw = 0;
+      if (lv0) {
+        W = l0.woff[bin + 1] - l0.woff[bin];
+        sw = (uint32_t)(W >> P);
+        first = l0.woff[bin] + (uint64_t)sub * sw;
+      }
+      bool over = lv0 && sw > WD_SWMAX;
+      // 1. one copy of each key, its copies' payloads ORed (WD_U keys per lane
+      //    loaded before the first is inserted)
+      uint32_t d = 0;
+      for (uint64_t base = 0; base < n && !over; base += 32 * WD_U) {
+        unsigned long long key[WD_U];
+        uint32_t p[WD_U];
+  #pragma unroll
+        for (int u = 0; u < WD_U; u++) {
+          const uint64_t i = base + u * 32 + lane;
+          key[u] = i < n ? T[a + i] : EMPTY;
+          p[u] = (pay && i < n) ? TP[a + i] : 0u;
+        }
+  #pragma unroll
+        for (int u = 0; u < WD_U; u++) {
+          if (over) break;  // the set stays below full: at most WD_MAXD + 32 keys in it
+          bool claimed = false;
+          uint32_t h = 0;
+          if (key[u] != EMPTY) {
+            h = (uint32_t)((key[u] * 0x9E3779B97F4A7C15ull) >> 55);  // top 9 bits: WD_TW = 512
+            for (uint32_t probe = 0; probe < WD_TW; probe++) {
+              const unsigned long long old = atomicCAS(&m.tab[h], EMPTY, key[u]);
+              if (old == EMPTY || old == key[u]) {
+                claimed = old == EMPTY;
+                if (pay) atomicOr(reinterpret_cast<uint32_t *>(m.tpay) + (h >> 2), p[u] << (8 * (h & 3)));
+                break;
+              }
+              h = (h + 1) & (WD_TW - 1);
+            }
           }
-          h = (h + 1) & (WD_TW - 1);
+          const unsigned b = __ballot_sync(FULL, claimed);
+          const uint32_t r = d + __popc(b & lt);
+          if (claimed && r < WD_MAXD) m.ins[r] = (uint16_t)h;
+          d += __popc(b);
+          over = d > WD_MAXD;
         }
       }
-      const unsigned b = __ballot_sync(FULL, claimed);
-      const uint32_t r = d + __popc(b & lt);
-      if (claimed && r < WD_MAXD) m.ins[r] = (uint16_t)h;
-      d += __popc(b);
-      over = d > WD_MAXD;
-    }
-    __syncwarp();
-    if (over) {  // left to the block kernel: clear the whole set, list j
-      for (uint32_t i = lane; i < WD_TW; i += 32) {
-        m.tab[i] = EMPTY;
-        m.tpay[i] = 0;
-      }
-      if (lane == 0) ov[atomicAdd(ov_cnt, 1u)] = (uint32_t)j;
       __syncwarp();
-      continue;
-    }
-    // 2. the distinct keys (and bytes) to T[a, a + d); the set is emptied
-    for (uint32_t r = lane; r < d; r += 32) {
-      const uint32_t h = m.ins[r];
-      T[a + r] = m.tab[h];
-      if (pay) TP[a + r] = m.tpay[h];
-      m.tab[h] = EMPTY;
-      m.tpay[h] = 0;
-    }
-    if (lane == 0) cnt[j] = d;
-    __syncwarp();
-    if (!lv0) continue;
-    // 3. level 0: mark the slice, clear collided bits, write it
-    const uint64_t lo_bit = (uint64_t)sub * sw * 64;
-    for (uint32_t w = lane; w < sw; w += 32) m.set[w] = m.col[w] = 0;
-    __syncwarp();
-    bool bad = false;
-    for (uint32_t r = lane; r < d; r += 32) {
-      const uint64_t b = bb_pos(T[a + r], 0, (uint32_t)W) - lo_bit;
-      if (b >= (uint64_t)sw * 64) {  // not this slice's key: cannot happen with the shared hash
-        bad = true;
+      if (over) {  // left to the block kernel: clear the whole set, list j
+        for (uint32_t i = lane; i < WD_TW; i += 32) {
+          m.tab[i] = EMPTY;
+          m.tpay[i] = 0;
+        }
+        if (lane == 0) ov[atomicAdd(ov_cnt, 1u)] = (uint32_t)j;
+        __syncwarp();
         continue;
       }
-      const unsigned long long bit = 1ull << (b & 63);
-      if (atomicOr(&m.set[b >> 6], bit) & bit) atomicOr(&m.col[b >> 6], bit);
-    }
-    if (__any_sync(FULL, bad) && lane == 0) atomicOr(l0.err, 1u);
-    __syncwarp();
-    // placed bits per word, and their exclusive prefix (sw <= 64: two words a lane)
-    const unsigned long long f0 = lane < sw ? m.set[lane] & ~m.col[lane] : 0ull;
-    const unsigned long long f1 = lane + 32 < sw ? m.set[lane + 32] & ~m.col[lane + 32] : 0ull;
-    if (lane < sw) l0.AR[first + lane] = make_ulonglong2(f0, 0ull);
-    if (lane + 32 < sw) l0.AR[first + lane + 32] = make_ulonglong2(f1, 0ull);
-    const uint32_t c0 = (uint32_t)__popcll(f0), c1 = (uint32_t)__popcll(f1);
-    const uint32_t i0 = warp_inclusive_scan(c0), i1 = warp_inclusive_scan(c1);
-    const uint32_t t0 = __shfl_sync(FULL, i0, 31), placed = t0 + __shfl_sync(FULL, i1, 31);
-    if (lane < sw) m.pw[lane] = i0 - c0;
-    if (lane + 32 < sw) m.pw[lane + 32] = t0 + i1 - c1;
-    if (lpay && lane == 0) l0.placed[j] = placed;
-    // survivors: one reservation in the bin's list
-    unsigned long long sbase = 0;
-    if (lane == 0 && d > placed) {
-      sbase = atomicAdd(&l0.surv_cnt[bin], (unsigned long long)(d - placed));
-      if (sbase + (d - placed) > l0.surv_off[bin + 1] - l0.surv_off[bin]) {
-        atomicOr(l0.err, 1u);
-        sbase = ~0ull;
+      const uint64_t lo_bit = (uint64_t)sub * sw * 64;
+      if (lv0) {
+        for (uint32_t w = lane; w < sw; w += 32) m.set[w] = m.col[w] = 0;
+        __syncwarp();
       }
-    }
-    sbase = __shfl_sync(FULL, sbase, 0);
-    __syncwarp();
-    // 4. each key: its byte to its rank (placed) or the key to level 1
-    uint64_t so = l0.surv_off[bin] + sbase;
-    for (uint32_t r0 = 0; r0 < d; r0 += 32) {
-      const uint32_t r = r0 + lane;
-      bool surv = false;
-      uint64_t key = 0;
-      if (r < d) {
-        key = T[a + r];
-        const uint64_t b = bb_pos(key, 0, (uint32_t)W) - lo_bit;
-        if (b < (uint64_t)sw * 64) {
-          const unsigned long long fin = m.set[b >> 6] & ~m.col[b >> 6], bit = 1ull << (b & 63);
+      // 2. the distinct keys (and bytes) to T[a, a + d), the set emptied; with
+      //    level 0, each key's bit marked and kept in ins, its byte in dp
+      bool bad = false;
+      for (uint32_t r = lane; r < d; r += 32) {
+        const uint32_t h = m.ins[r];
+        const unsigned long long key = m.tab[h];
+        const uint8_t pr = m.tpay[h];
+        T[a + r] = key;
+        if (pay) TP[a + r] = pr;
+        m.tab[h] = EMPTY;
+        m.tpay[h] = 0;
+        if (lv0) {
+          const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
+          uint16_t bb = NO_BIT;
+          if (bpos < (uint64_t)sw * 64) {
+            bb = (uint16_t)bpos;
+            const unsigned long long bit = 1ull << (bpos & 63);
+            if (atomicOr(&m.set[bpos >> 6], bit) & bit) atomicOr(&m.col[bpos >> 6], bit);
+          } else {
+            bad = true;
+          }
+          m.ins[r] = bb;
+          m.dp[r] = pr;
+        }
+      }
+      if (lane == 0) cnt[j] = d;
+      if (!lv0) {
+        __syncwarp();
+        continue;
+      }
+      if (__any_sync(FULL, bad) && lane == 0) atomicOr(l0.err, 1u);
+      __syncwarp();
+      // 3. the slice written; placed bits per word and their exclusive prefix
+      //    (sw <= 64: two words a lane)
+      const unsigned long long f0 = lane < sw ? m.set[lane] & ~m.col[lane] : 0ull;
+      const unsigned long long f1 = lane + 32 < sw ? m.set[lane + 32] & ~m.col[lane + 32] : 0ull;
+      if (lane < sw) l0.AR[first + lane] = make_ulonglong2(f0, 0ull);
+      if (lane + 32 < sw) l0.AR[first + lane + 32] = make_ulonglong2(f1, 0ull);
+      const uint32_t c0 = (uint32_t)__popcll(f0), c1 = (uint32_t)__popcll(f1);
+      const uint32_t i0 = warp_inclusive_scan(c0), i1 = warp_inclusive_scan(c1);
+      const uint32_t t0 = __shfl_sync(FULL, i0, 31), placed = t0 + __shfl_sync(FULL, i1, 31);
+      if (lane < sw) m.pw[lane] = i0 - c0;
+      if (lane + 32 < sw) m.pw[lane + 32] = t0 + i1 - c1;
+      if (lpay && lane == 0) l0.placed[j] = placed;
+      // survivors: one reservation in the bin's list
+      unsigned long long sbase = 0;
+      if (lane == 0 && d > placed) {
+        sbase = atomicAdd(&l0.surv_cnt[bin], (unsigned long long)(d - placed));
+        if (sbase + (d - placed) > l0.surv_off[bin + 1] - l0.surv_off[bin]) {
+          atomicOr(l0.err, 1u);
+          sbase = ~0ull;
+        }
+      }
+      sbase = __shfl_sync(FULL, sbase, 0);
+      __syncwarp();
+      // 4. each key: its byte to its rank (placed) or the key to level 1
+      uint64_t so = l0.surv_off[bin] + sbase;
+      for (uint32_t r0 = 0; r0 < d; r0 += 32) {
+        const uint32_t r = r0 + lane;
+        bool surv = false;
+        if (r < d && m.ins[r] != NO_BIT) {
+          const uint32_t bb = m.ins[r];
+          const unsigned long long fin = m.set[bb >> 6] & ~m.col[bb >> 6], bit = 1ull << (bb & 63);
           if (fin & bit) {
-            if (lpay) l0.l0pay[a + m.pw[b >> 6] + (uint32_t)__popcll(fin & (bit - 1))] = TP[a + r];
+            if (lpay) l0.l0pay[a + m.pw[bb >> 6] + (uint32_t)__popcll(fin & (bit - 1))] = m.dp[r];
           } else {
             surv = true;
           }
         }
+        const unsigned sb = __ballot_sync(FULL, surv);
+        if (surv && sbase != ~0ull) {
+          const uint64_t at = so + __popc(sb & lt);
+          l0.surv[at] = T[a + r];
+          if (lpay) l0.surv_pay[at] = m.dp[r];
+        }
+        so += __popc(sb);
       }
-      const unsigned sb = __ballot_sync(FULL, surv);
-      if (surv && sbase != ~0ull) {
-        const uint64_t at = so + __popc(sb & lt);
-        l0.surv[at] = key;
-        if (lpay) l0.surv_pay[at] = TP[a + r];
-      }
-      so += __popc(sb);
+      __syncwarp();
     }
-    __syncwarp();
   }
 }
 
@@ -1082,13 +1112,13 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
       // the unsorted form: one warp per sub-bucket; the few it cannot hold
       // (more than WD_MAXD distinct keys) go to the block kernel after it
       uint32_t *ov = sc.ov.get<uint32_t>(nsub + 1);
-      uint32_t *ovc = sc.ovc.get<uint32_t>(1);
-      CF1_CUDA(cudaMemsetAsync(ovc, 0, sizeof(uint32_t), s));
+      uint32_t *ovc = sc.ovc.get<uint32_t>(2);  // overflow count, work counter
+      CF1_CUDA(cudaMemsetAsync(ovc, 0, 2 * sizeof(uint32_t), s));
       const size_t wsm = WD_WARPS * sizeof(WdSmem);
       CF1_CUDA(cudaFuncSetAttribute(wd_dedup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
       const unsigned wgrid = persistent_grid(wd_dedup_kernel, WD_WARPS * 32, wsm, -1, ceil_div(nsub, WD_WARPS));
       wd_dedup_kernel<<<wgrid, WD_WARPS * 32, wsm, s>>>(reinterpret_cast<uint64_t *>(T), PT, sb_off, nsub, P, cnt, lo,
-                                                        ov, ovc);
+                                                        ov, ovc, ovc + 1);
       CF1_LAUNCH_CHECK();
       uint32_t h_ov = 0;
       CF1_CUDA(cudaMemcpyAsync(&h_ov, ovc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
