@@ -50,6 +50,15 @@ __global__ void __launch_bounds__(256) expand_kernel(const uint64_t *records, ui
     uint32_t n = valid ? rec_n(rec) : 0;
     uint64_t pos = rec_pos(rec);
     uint64_t off = valid ? kpre[r] : 0;
+    // whether the record's first k-mer has a base before it and its last one
+    // a base after it (inside a super k-mer the windows before and after are
+    // valid, so only these two can lack a neighbour): read once per record,
+    // not in the k-mer loop
+    uint32_t ends = 0;
+    if (sides && valid) {
+      const uint64_t q = pos + n - 1;  // the last k-mer
+      ends = (uint32_t)(pos > 0 && !is_n(NM, pos - 1)) | ((uint32_t)(q + k < L && !is_n(NM, q + k)) << 1);
+    }
     uint32_t incl = warp_inclusive_scan(n);
     uint32_t total = __shfl_sync(FULL, incl, 31);
     uint32_t excl = incl - n;
@@ -64,17 +73,15 @@ __global__ void __launch_bounds__(256) expand_kernel(const uint64_t *records, ui
       uint64_t opos = __shfl_sync(FULL, pos, lo);
       uint32_t oex = __shfl_sync(FULL, excl, lo);
       uint64_t ooff = __shfl_sync(FULL, off, lo);
-      const uint32_t onrec = __shfl_sync(FULL, n, lo);
+      const uint32_t onrec = __shfl_sync(FULL, n, lo), oends = __shfl_sync(FULL, ends, lo);
       if (j < total) {
         uint32_t t = j - oex;
         if (ooff + t < n_keys && opos + t + k <= L) {
           const uint64_t p = opos + t;
           if (sides) {
-            // inside a super k-mer the windows before and after are valid, so
-            // only its first and last k-mers can lack a neighbour; the
-            // neighbours come from the words the k-mer is read from
-            const bool hp = t > 0 || (p > 0 && !is_n(NM, p - 1));
-            const bool hn = t + 1 < onrec || (p + k < L && !is_n(NM, p + k));
+            // the neighbours come from the words the k-mer is read from
+            const bool hp = t > 0 || (oends & 1u);
+            const bool hn = t + 1 < onrec || (oends & 2u);
             uint32_t pb, nb;
             KeyT fw = KOps<KeyT>::extract_nb(W, p, k, hp, pb, nb);
             KeyT rc = KOps<KeyT>::rc(fw, k);
