@@ -517,6 +517,7 @@ def gpu_arm(args):
                       "ms_classify_kernel": v["ms_classify_kernel"], "phases_ms": v["phases_ms"],
                       "bbhash_levels": int(v["stats"]["bbhash_levels"]), "mphf_bytes": int(v["stats"]["mphf_bytes"]),
                       "mphf_image_bytes": int(v["image_bytes"]), "state_path": int(v["stats"]["state_path"]),
+                      "dedup_overflow": int(v["stats"]["dedup_overflow"]),
                       "ms_dedup_kernel": v["ms_dedup_kernel"],
                       "sort": ("lsd" if v["stats"]["sort_msd_bits"] == 2**64 - 1
                                else f"msd{v['stats']['sort_msd_bits']}"),

@@ -48,13 +48,13 @@ class Opts(C.Structure):
 
 _STAT_U = ["n_bases", "n_records", "n_short", "n_superkmers", "n_kmer_occurrences", "n_distinct", "n_bins",
            "n_state_words", "mphf_bytes", "bbhash_levels", "learned_bins", "fallback_bins", "learned_max_err",
-           "classify_cas_retries", "n_kernel_launches", "sort_msd_bits", "tuner_state", "sk_tile", "state_path"]
+           "classify_cas_retries", "n_kernel_launches", "sort_msd_bits", "tuner_state", "sk_tile", "state_path", "dedup_overflow"]
 _STAT_D = ["ms_h2d", "ms_phase1", "ms_phase2", "ms_phase3_sort", "ms_phase3_mphf", "ms_phase4", "ms_total",
            "ms_classify_kernel", "ms_dedup_kernel"]
 
 
 class Stats(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in _STAT_U] + [("reserved_u", C.c_uint64 * 1)] + \
+    _fields_ = [(n, C.c_uint64) for n in _STAT_U] + \
                [(n, C.c_double) for n in _STAT_D] + [("reserved_d", C.c_double * 3)]
 
 

@@ -764,6 +764,7 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
   st.ms_phase4 = elapsed(c->ev[4], c->ev[7]);
   st.ms_classify_kernel = elapsed(c->ev[5], c->ev[6]);
   st.ms_dedup_kernel = done ? be.msd.ms_dedup : 0.0;
+  st.dedup_overflow = done && !sorted ? be.msd.last_overflow : 0;
   st.state_path = joined ? 0 : (c->opts.state_update == 1 ? 1 : 2);
   st.ms_total = elapsed(c->ev[0], c->ev[7]) + p1_before;
 }

@@ -116,7 +116,7 @@ typedef struct cf1gpu_stats {
   uint64_t sk_tile;            /* phase-1 tile this run used */
   uint64_t state_path;         /* how the last run formed the states: 0 joined in phase 3, 1 CAS classification,
                                   2 side-set classification (state_update, or 2 when the LSD sort ran) */
-  uint64_t reserved_u[1];
+  uint64_t dedup_overflow;     /* sub-buckets the warp dedup left to the block kernel (BBHash form) */
   double ms_h2d;               /* host->device copy of the input */
   double ms_phase1;            /* pack + minimizer histogram + partition */
   double ms_phase2;            /* super k-mer routing */
