@@ -757,7 +757,10 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
       }
       bool over = lv0 && sw > WD_SWMAX;
       // 1. one copy of each key, its copies' payloads ORed (WD_U keys per lane
-      //    loaded before the first is inserted)
+      //    loaded before the first is inserted).  Double hashing: the probe
+      //    step is odd (so a probe sequence visits every slot) and comes from
+      //    other bits of the same product, which keeps the runs a warp waits
+      //    for (the longest of its 32 lanes) short at the set's load.
       uint32_t d = 0;
       for (uint64_t base = 0; base < n && !over; base += 32 * WD_U) {
         unsigned long long key[WD_U];
@@ -774,7 +777,9 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
           bool claimed = false;
           uint32_t h = 0;
           if (key[u] != EMPTY) {
-            h = (uint32_t)((key[u] * 0x9E3779B97F4A7C15ull) >> 55);  // top 9 bits: WD_TW = 512
+            const unsigned long long hk = key[u] * 0x9E3779B97F4A7C15ull;
+            h = (uint32_t)(hk >> 55);                               // top 9 bits: WD_TW = 512
+            const uint32_t step = ((uint32_t)(hk >> 40) | 1u) & (WD_TW - 1);
             for (uint32_t probe = 0; probe < WD_TW; probe++) {
               const unsigned long long old = atomicCAS(&m.tab[h], EMPTY, key[u]);
               if (old == EMPTY || old == key[u]) {
@@ -782,7 +787,7 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
                 if (pay) atomicOr(reinterpret_cast<uint32_t *>(m.tpay) + (h >> 2), p[u] << (8 * (h & 3)));
                 break;
               }
-              h = (h + 1) & (WD_TW - 1);
+              h = (h + step) & (WD_TW - 1);
             }
           }
           const unsigned b = __ballot_sync(FULL, claimed);

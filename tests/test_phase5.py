@@ -91,19 +91,27 @@ def test_phase5_output_is_free_of_slot_numbering():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("queries", ["host_image", "device_batches"])
 @pytest.mark.parametrize("mode", ["bbhash", "learned"])
 @pytest.mark.parametrize("k", [31, 63])
-def test_phase5_on_gpu_structures_matches_oracle(k, mode):
+def test_phase5_on_gpu_structures_matches_oracle(k, mode, queries):
+    """Phase 5's MPHF queries answered either by the exported host image
+    (cf1gpu_mphf_host_query) or by cf1gpu_query on the device, one call per
+    batch of a record's k-mers, the MPHF never leaving the GPU."""
     recs = random_records(9000 + k, k, n_records=40, max_len=3000)
     seq, off = o.concat_records(recs)
     ref = o.run(k, seq, off, nthreads=8)
     g = gpu_run(seq, off, k, mode=mode, num_bins=16)
     try:
-        image = g.export_mphf()
         words = g.states()
+        if queries == "host_image":
+            image = g.export_mphf()
+            gpu = p5.extract_and_output(named(recs), k, lambda q: cg.host_query(image, q), words,
+                                        poly_n_stretch=True)
+        else:
+            gpu = p5.extract_and_output(named(recs), k, g.query, words, poly_n_stretch=True)
     finally:
         g.close()
-    gpu = p5.extract_and_output(named(recs), k, lambda q: cg.host_query(image, q), words, poly_n_stretch=True)
     cpu = p5.extract_and_output(named(recs), k, oracle_slot_of(ref), ref.state_words, poly_n_stretch=True)
     assert len(gpu.segs) == len(cpu.segs)
     assert p5.canonical(gpu) == p5.canonical(cpu)
