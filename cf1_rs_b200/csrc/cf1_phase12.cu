@@ -87,7 +87,7 @@ constexpr uint32_t SK_INVALID = 0xFFFFFFFFu;
 template <int BLOCK, int ITEMS, int KC>
 __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
   constexpr uint32_t T = BLOCK * ITEMS;
-  extern __shared__ uint32_t dyn32[];
+  extern __shared__ __align__(16) uint32_t dyn32[];
   uint32_t *bufA = dyn32;
   uint32_t *bufB = dyn32 + T + 64;
   __shared__ uint32_t s_tile;
@@ -108,39 +108,116 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
     const uint64_t P0 = tile * T;
     const uint32_t nk = (uint32_t)min((uint64_t)T, NK - P0);
     const uint32_t nm = nk + w - 1;
-    for (uint32_t q = tid; q < nm; q += BLOCK) {
-      uint32_t fw = (uint32_t)KOps<uint64_t>::extract(a.W, P0 + q, m);
-      uint32_t r = mmer_rc(fw, m);
-      bufA[q] = mix_order(fw < r ? fw : r);
-    }
-    __syncthreads();
-    uint32_t *src = bufA, *dst = bufB;
-    uint32_t len = nm, span = 1;
-    while (span * 2 <= (uint32_t)w) {
-      for (uint32_t q = tid; q + span < len; q += BLOCK) dst[q] = min(src[q], src[q + span]);
-      __syncthreads();
-      uint32_t *t2 = src;
-      src = dst;
-      dst = t2;
-      len -= span;
-      span *= 2;
-    }
-    for (uint32_t p = tid; p < nk; p += BLOCK) {
-      uint32_t v = min(src[p], src[p + w - span]);
-      dst[p] = window_clean(a.NM, P0 + p, k) ? v : SK_INVALID;
-    }
-    __syncthreads();
-    const uint32_t *z = dst;
-    uint32_t *starts = src;  // free now: segment starts
     // thread tid owns k-mers [p0, p0 + ITEMS)
     const uint32_t p0 = tid * ITEMS;
     uint32_t zv[ITEMS];
+    uint32_t prev = SK_INVALID;
+    uint32_t *starts;  // segment starts, once the windows are taken
+    if constexpr (KC != 0) {
+      // k, m, w fixed: each thread rolls the m-mers of its ITEMS positions
+      // (one extraction, then one base each) and takes its windows' minima
+      // in registers; no doubling passes.
+      static_assert(ITEMS % 4 == 0 && ITEMS <= W_FIXED, "window split needs ITEMS <= w");
+      constexpr uint32_t MM = (1u << (2 * M_FIXED)) - 1;
+      auto order_run = [&](uint32_t q0) {  // order values of m-mers q0 .. q0 + ITEMS - 1
+        uint32_t fw = (uint32_t)KOps<uint64_t>::extract(a.W, P0 + q0, M_FIXED), r = mmer_rc(fw, M_FIXED);
+        uint64_t nxt = KOps<uint64_t>::extract(a.W, P0 + q0 + M_FIXED, 32);  // the bases after, left-aligned
+        uint32_t v[ITEMS];
+        v[0] = mix_order(fw < r ? fw : r);
+#pragma unroll
+        for (int i = 1; i < ITEMS; i++) {
+          const uint32_t b = (uint32_t)(nxt >> 62);
+          nxt <<= 2;
+          fw = ((fw << 2) | b) & MM;
+          r = (r >> 2) | ((3u - b) << (2 * M_FIXED - 2));
+          v[i] = mix_order(fw < r ? fw : r);
+        }
+#pragma unroll
+        for (int i = 0; i < ITEMS; i += 4)
+          *reinterpret_cast<uint4 *>(bufA + q0 + i) = make_uint4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+      };
+      if (p0 < nm) order_run(p0);
+      constexpr uint32_t TAIL = (W_FIXED - 1 + ITEMS - 1) / ITEMS;  // threads for the w - 1 m-mers past T
+      if (tid < TAIL && T + tid * ITEMS < nm) order_run(T + tid * ITEMS);
+      __syncthreads();
+      // window i = A[i .. i + w - 1] (A = bufA + p0): the part left of the
+      // shared middle A[ITEMS - 1 .. w - 1] by suffix minima, the part right
+      // of it by prefix minima; window -1 (k-mer p0 - 1) for the segment test
+      constexpr int NA = ITEMS + W_FIXED - 1, NV = (NA + 3) / 4;
+      uint32_t A[NV * 4];
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        const uint4 x = *reinterpret_cast<const uint4 *>(bufA + p0 + 4 * v);
+        A[4 * v] = x.x;
+        A[4 * v + 1] = x.y;
+        A[4 * v + 2] = x.z;
+        A[4 * v + 3] = x.w;
+      }
+      uint32_t mid0 = A[ITEMS - 1];
+#pragma unroll
+      for (int j = ITEMS; j <= W_FIXED - 2; j++) mid0 = min(mid0, A[j]);
+      const uint32_t mid = min(mid0, A[W_FIXED - 1]);
+      uint32_t S = SK_INVALID, win[ITEMS];
+#pragma unroll
+      for (int i = ITEMS - 1; i >= 0; i--) {
+        if (i < ITEMS - 1) S = min(S, A[i]);
+        win[i] = min(S, mid);
+      }
+      uint32_t Pf = SK_INVALID;
+#pragma unroll
+      for (int i = 1; i < ITEMS; i++) {
+        Pf = min(Pf, A[W_FIXED + i - 1]);
+        win[i] = min(win[i], Pf);
+      }
+      // placeholders: the k bases of window i are bits i .. i + k - 1 of nmb
+      uint64_t nmb = ~0ull;
+      if (p0 <= nk) {
+        const uint64_t bs = P0 + p0, wi = bs >> 6;
+        const int sh = (int)(bs & 63);
+        nmb = a.NM[wi] >> sh;
+        if (sh) nmb |= a.NM[wi + 1] << (64 - sh);
+      }
+      constexpr uint64_t KMASK = (1ull << KC) - 1;
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) zv[i] = (p0 + i < nk && ((nmb >> i) & KMASK) == 0) ? win[i] : SK_INVALID;
+      if (p0 > 0 && p0 <= nk && !is_n(a.NM, P0 + p0 - 1) && (nmb & (KMASK >> 1)) == 0) {
+        const uint32_t am1 = bufA[p0 - 1];
+        prev = min(am1, min(S, mid0));
+      }
+      starts = bufB;
+    } else {
+      for (uint32_t q = tid; q < nm; q += BLOCK) {
+        uint32_t fw = (uint32_t)KOps<uint64_t>::extract(a.W, P0 + q, m);
+        uint32_t r = mmer_rc(fw, m);
+        bufA[q] = mix_order(fw < r ? fw : r);
+      }
+      __syncthreads();
+      uint32_t *src = bufA, *dst = bufB;
+      uint32_t len = nm, span = 1;
+      while (span * 2 <= (uint32_t)w) {
+        for (uint32_t q = tid; q + span < len; q += BLOCK) dst[q] = min(src[q], src[q + span]);
+        __syncthreads();
+        uint32_t *t2 = src;
+        src = dst;
+        dst = t2;
+        len -= span;
+        span *= 2;
+      }
+      for (uint32_t p = tid; p < nk; p += BLOCK) {
+        uint32_t v = min(src[p], src[p + w - span]);
+        dst[p] = window_clean(a.NM, P0 + p, k) ? v : SK_INVALID;
+      }
+      __syncthreads();
+      const uint32_t *z = dst;
+      starts = src;  // free now: segment starts
+      prev = p0 > 0 && p0 <= nk ? z[p0 - 1] : SK_INVALID;
+#pragma unroll
+      for (int i = 0; i < ITEMS; i++) zv[i] = p0 + i < nk ? z[p0 + i] : SK_INVALID;
+    }
     uint32_t bflags = 0, nb = 0, nv = 0;
-    uint32_t prev = p0 > 0 && p0 <= nk ? z[p0 - 1] : SK_INVALID;
 #pragma unroll
     for (int i = 0; i < ITEMS; i++) {
       const uint32_t p = p0 + i;
-      zv[i] = p < nk ? z[p] : SK_INVALID;
       const bool b = p < nk && (p == 0 || zv[i] != prev);
       bflags |= (uint32_t)b << i;
       nb += b;
@@ -188,44 +265,67 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
 constexpr int SK_BLOCK = 256;
 
 // Phase 2: every record of the unordered list goes to its bin's range
-// (records of a bin end up in no particular order).  A CTA takes BS_TILE
-// records, counts them per bin in shared memory, reserves each bin's slots
-// with one atomic add, and writes.
+// (records of a bin end up in no particular order).  A CTA takes a tile of
+// 4096 records: each record is ranked inside its bin by a shared-memory
+// counter, each bin of the tile reserves its run of slots with one global
+// atomic, the tile is staged in shared memory in bin order, and the runs are
+// written out by consecutive threads on consecutive addresses (a tile gives
+// each of 256 bins a run of ~16 records, which a direct store from the
+// ranking thread would scatter over 32 sectors per warp store).
 constexpr int BS_BLOCK = 256;
 constexpr int BS_ITEMS = 16;
-__global__ void __launch_bounds__(BS_BLOCK) bin_scatter_kernel(const uint64_t *rec_tmp, const uint16_t *rec_bucket,
+constexpr uint32_t BS_TILE = BS_BLOCK * BS_ITEMS;
+__global__ void __launch_bounds__(BS_BLOCK, 3) bin_scatter_kernel(const uint64_t *rec_tmp, const uint16_t *rec_bucket,
                                                                uint64_t n, const uint16_t *lut, uint32_t num_bins,
                                                                const uint64_t *rec_off, uint32_t *cursor,
                                                                uint64_t *records, uint32_t *err) {
-  extern __shared__ uint32_t bs_smem[];
-  uint32_t *s_cnt = bs_smem;             // [num_bins]
-  uint32_t *s_base = bs_smem + num_bins;  // [num_bins]
+  extern __shared__ __align__(16) uint64_t bs_smem[];
+  uint64_t *stage = bs_smem;                                           // [BS_TILE]
+  uint32_t *s_cnt = reinterpret_cast<uint32_t *>(bs_smem + BS_TILE);  // [num_bins]
+  uint32_t *s_start = s_cnt + num_bins;                                // [num_bins] tile-local
+  uint32_t *s_base = s_start + num_bins;                               // [num_bins] in the bin's range
+  __shared__ uint32_t sm[BS_BLOCK / 32];
   const unsigned tid = threadIdx.x;
   for (uint32_t b = tid; b < num_bins; b += BS_BLOCK) s_cnt[b] = 0;
   __syncthreads();
-  const uint64_t r0 = (uint64_t)blockIdx.x * BS_BLOCK * BS_ITEMS;
-  uint32_t bin[BS_ITEMS], li[BS_ITEMS];
+  const uint64_t r0 = (uint64_t)blockIdx.x * BS_TILE;
+  const uint32_t nt = (uint32_t)(n - r0 < BS_TILE ? n - r0 : BS_TILE);
+  uint32_t li[BS_ITEMS];  // rank inside the bin, ~0u past the tile's end
+  uint64_t rec[BS_ITEMS];  // the routed record (its bin in the low bits)
 #pragma unroll
   for (int i = 0; i < BS_ITEMS; i++) {
-    uint64_t r = r0 + (uint64_t)i * BS_BLOCK + tid;
-    bin[i] = 0xFFFFFFFFu;
-    if (r < n) {
-      bin[i] = rec_bucket ? lut[rec_bucket[r]] : rec_bin(rec_tmp[r]);  // no buckets: the records carry their bin
-      li[i] = atomicAdd(&s_cnt[bin[i]], 1u);
+    const uint32_t j = (uint32_t)i * BS_BLOCK + tid;
+    li[i] = 0xFFFFFFFFu;
+    if (j < nt) {
+      const uint64_t t = rec_tmp[r0 + j];
+      const uint32_t b = rec_bucket ? lut[rec_bucket[r0 + j]] : rec_bin(t);  // no buckets: the records carry their bin
+      rec[i] = rec_pack(rec_pos(t), rec_n(t), b);
+      li[i] = atomicAdd(&s_cnt[b], 1u);
     }
+  }
+  __syncthreads();
+  // tile-local starts: each thread scans a run of consecutive bins
+  const uint32_t per = (num_bins + BS_BLOCK - 1) / BS_BLOCK, b0 = tid * per;
+  uint32_t own = 0;
+  for (uint32_t b = b0; b < b0 + per && b < num_bins; b++) own += s_cnt[b];
+  uint32_t tot;
+  uint32_t run = block_exclusive_scan<BS_BLOCK>(own, sm, tot);
+  for (uint32_t b = b0; b < b0 + per && b < num_bins; b++) {
+    const uint32_t c = s_cnt[b];
+    s_start[b] = run;
+    if (c) s_base[b] = atomicAdd(&cursor[b], c);
+    run += c;
   }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < BS_ITEMS; i++)
-    if (bin[i] != 0xFFFFFFFFu && li[i] == 0) s_base[bin[i]] = atomicAdd(&cursor[bin[i]], s_cnt[bin[i]]);
+    if (li[i] != 0xFFFFFFFFu) stage[s_start[rec_bin(rec[i])] + li[i]] = rec[i];
   __syncthreads();
-#pragma unroll
-  for (int i = 0; i < BS_ITEMS; i++) {
-    if (bin[i] == 0xFFFFFFFFu) continue;
-    uint64_t r = r0 + (uint64_t)i * BS_BLOCK + tid;
-    uint64_t idx = rec_off[bin[i]] + s_base[bin[i]] + li[i];
-    uint64_t t = rec_tmp[r];
-    if (idx < rec_off[bin[i] + 1]) records[idx] = rec_pack(rec_pos(t), rec_n(t), bin[i]);
+  for (uint32_t i = tid; i < nt; i += BS_BLOCK) {
+    const uint64_t r = stage[i];
+    const uint32_t b = rec_bin(r);
+    const uint64_t idx = rec_off[b] + s_base[b] + (i - s_start[b]);
+    if (idx < rec_off[b + 1]) records[idx] = r;
     else atomicOr(err, (uint32_t)DEV_OVERFLOW);
   }
 }
@@ -343,9 +443,9 @@ void launch_bin_scatter(const uint64_t *rec_tmp, const uint16_t *rec_bucket, uin
                         uint32_t num_bins, const uint64_t *rec_off, uint32_t *cursor, uint64_t *records, uint32_t *err,
                         cudaStream_t s) {
   if (n == 0) return;
-  size_t smem = 2 * num_bins * sizeof(uint32_t);
+  size_t smem = BS_TILE * sizeof(uint64_t) + 3 * num_bins * sizeof(uint32_t);
   CF1_CUDA(cudaFuncSetAttribute(bin_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  bin_scatter_kernel<<<(unsigned)ceil_div(n, (uint64_t)BS_BLOCK * BS_ITEMS), BS_BLOCK, smem, s>>>(
+  bin_scatter_kernel<<<(unsigned)ceil_div(n, (uint64_t)BS_TILE), BS_BLOCK, smem, s>>>(
       rec_tmp, rec_bucket, n, lut, num_bins, rec_off, cursor, records, err);
   CF1_LAUNCH_CHECK();
 }
