@@ -107,6 +107,8 @@ def measured_peaks():
 def traffic_md(form: str, kernel: str) -> str:
     if kernel == "classify":
         return os.path.join(ROOT, "profiles", "classify_traffic_workload5_full.md")
+    if form == "bbhash":
+        return os.path.join(ROOT, "profiles", "wd_dedup_kernel_workload5_scale0.05.md")
     return os.path.join(ROOT, "profiles", f"cs_sort_unique_{form}_traffic_workload5.md")
 
 
@@ -468,7 +470,11 @@ def gpu_arm(args):
         # entries per 64 bits, i.e. 2 B per occurrence)
         b_dd = (w + 1.0) * n_occ + (w + 1.0) * n_dist + (2.0 * n_occ if head_name == "bbhash" else 0.0)
         ach = b_dd / (head["ms_dedup_kernel"] / 1e3) / 1e9
-        roofline = {"kernel": "cs_sort_unique_kernel", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
+        # BBHash form: the warp dedup, with the block kernel for the few
+        # sub-buckets it leaves (timed together); learned form: the sorted
+        # chunk dedup
+        kname = "wd_dedup_kernel" if head_name == "bbhash" else "cs_sort_unique_kernel"
+        roofline = {"kernel": kname, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
                     "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "peak_kind": peak_kind,
                     "traffic": committed_traffic(args.workload, args.scale, head_name, "dedup"),
                     "algorithmic_bytes": b_dd}
