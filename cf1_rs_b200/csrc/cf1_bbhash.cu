@@ -205,6 +205,7 @@ void BBHashBuild<KeyT>::clear() {
   total_words = 0;
   levels = 0;
   bytes = 0;
+  l1_slice_bits = -1;
 }
 
 template <class KeyT>
@@ -327,24 +328,33 @@ void BBHashBuild<KeyT>::build(const KeyT *keys, const uint64_t *seg_off, uint32_
 }
 
 template <class KeyT>
-ulonglong2 *BBHashBuild<KeyT>::prepare_level0(uint64_t words, cudaStream_t s) {
-  reserve_entries(words + words / 2 + 64 * 1024, 0, s);
+ulonglong2 *BBHashBuild<KeyT>::prepare_levels01(uint64_t words0, uint64_t words1, cudaStream_t s) {
+  const uint64_t words = words0 + words1;
+  reserve_entries(words + words / 4 + 64 * 1024, 0, s);
   return ar_.as<ulonglong2>();
 }
 
 template <class KeyT>
-void BBHashBuild<KeyT>::build_from_level0(uint32_t nb, const uint64_t *woff0, uint64_t words0, const KeyT *surv,
-                                          const uint64_t *surv_off, const uint64_t *surv_cnt, uint64_t surv_total,
-                                          cudaStream_t s, KeyT *ws0, KeyT *ws1, uint64_t ws_cap) {
+void BBHashBuild<KeyT>::build_from_levels01(uint32_t nb, int P, const uint64_t *woff0, uint64_t words0,
+                                            const uint64_t *woff1, uint64_t words1, const KeyT *surv,
+                                            const uint64_t *surv_off, const uint64_t *surv_cnt, uint64_t surv_total,
+                                            cudaStream_t s, KeyT *ws0, KeyT *ws1, uint64_t ws_cap) {
   begin(nb, s);
   nwords.push_back(words0);
   level_off.push_back(0);
   finish_level(0, woff0, words0, s);
   total_words = words0;
-  CF1_CUDA(cudaMemcpyAsync(cnt_[1].as<uint64_t>(), surv_cnt, nbins * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+  nwords.push_back(words1);
+  level_off.push_back(words0);
+  finish_level(1, woff1, words1, s);
+  total_words += words1;
+  l1_slice_bits = P;
+  CF1_CUDA(cudaMemcpyAsync(cnt_[0].as<uint64_t>(), surv_cnt, nbins * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
   KeyT *r0 = (ws0 && ws_cap >= surv_total + 1) ? ws0 : rem_[0].get<KeyT>(surv_total + 1);
   KeyT *r1 = (ws1 && ws_cap >= surv_total + 1) ? ws1 : rem_[1].get<KeyT>(surv_total + 1);
-  run_levels(1, surv, surv_off, r1, r0, s);  // level 1 writes r[1 & 1] = r0
+  run_levels(2, surv, surv_off, r0, r1, s);  // level l reads cnt_[l & 1] and writes r[l & 1]
+  levels = std::max<uint32_t>(levels, 2);
+  bytes = total_words * sizeof(ulonglong2) + (size_t)levels * nbins * sizeof(BBMeta);
 }
 
 template <class KeyT>
@@ -354,6 +364,8 @@ BBView BBHashBuild<KeyT>::view() const {
   v.meta = meta_.as<const BBMeta>();
   v.levels = levels;
   v.nbins = nbins;
+  v.l1_slice_bits = l1_slice_bits;
+  v.pad = 0;
   return v;
 }
 

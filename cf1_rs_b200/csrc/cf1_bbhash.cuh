@@ -11,6 +11,7 @@ struct BBHashBuild {
   uint64_t total_words = 0;        // entries of all levels
   uint32_t levels = 0, nbins = 0;
   uint64_t bytes = 0;
+  int l1_slice_bits = -1;          // see BBView
 
   BBHashBuild() = default;
   BBHashBuild(const BBHashBuild &) = delete;
@@ -22,16 +23,19 @@ struct BBHashBuild {
   // still unplaced between levels; without them the builder allocates.
   void build(const KeyT *keys, const uint64_t *seg_off, uint32_t nbins, const uint32_t *sel, cudaStream_t s,
              KeyT *ws0 = nullptr, KeyT *ws1 = nullptr, uint64_t ws_cap = 0);
-  // Level 0 built elsewhere (the unsorted phase-3 dedup, one exclusive slice
-  // per sub-bucket): prepare_level0 gives the entry array to fill with level
-  // 0's cleaned bit words ({bits, 0}); build_from_level0 ranks it and builds
-  // the later levels over the keys level 0 left (bin b's at
-  // surv[surv_off[b] + [0, surv_cnt[b])]).  woff0: the bins' block offsets
-  // [nbins + 1] of level 0 (words0 words in all).
-  ulonglong2 *prepare_level0(uint64_t words, cudaStream_t s);
-  void build_from_level0(uint32_t nbins, const uint64_t *woff0, uint64_t words0, const KeyT *surv,
-                         const uint64_t *surv_off, const uint64_t *surv_cnt, uint64_t surv_total, cudaStream_t s,
-                         KeyT *ws0 = nullptr, KeyT *ws1 = nullptr, uint64_t ws_cap = 0);
+  // Levels 0 and 1 built elsewhere (the unsorted phase-3 dedup, one
+  // exclusive slice of each per sub-bucket; level 1 sliced, see BBView):
+  // prepare_levels01 gives the entry array to fill with level 0's cleaned
+  // bit words ({bits, 0}) at [0, words0) and level 1's at [words0, words0 +
+  // words1); build_from_levels01 ranks both and builds the later levels over
+  // the keys level 1 left (bin b's at surv[surv_off[b] + [0, surv_cnt[b])]).
+  // woff0 / woff1: the bins' block offsets [nbins + 1] of levels 0 and 1;
+  // P: the slice bits.
+  ulonglong2 *prepare_levels01(uint64_t words0, uint64_t words1, cudaStream_t s);
+  void build_from_levels01(uint32_t nbins, int P, const uint64_t *woff0, uint64_t words0, const uint64_t *woff1,
+                           uint64_t words1, const KeyT *surv, const uint64_t *surv_off, const uint64_t *surv_cnt,
+                           uint64_t surv_total, cudaStream_t s, KeyT *ws0 = nullptr, KeyT *ws1 = nullptr,
+                           uint64_t ws_cap = 0);
   BBView view() const;
   void clear();
   uint64_t level_words(uint32_t l) const;

@@ -5,10 +5,11 @@
 // The image holds everything a query needs: the bucket -> bin table, the
 // per-bin slot offsets, the BBHash levels and, in learned mode, the roots,
 // leaves and the sorted distinct keys.  The query code is the device code
-// (cf1_mphf.cuh), compiled for the host.  Image layout version 3: the BBHash
+// (cf1_mphf.cuh), compiled for the host.  Image layout version 4: the BBHash
 // levels are one array of 16-byte {bit word, level rank} entries addressed
 // through the 16-byte per-(level, bin) metadata, so the image and every
-// section in it start on a 16-byte boundary.
+// section in it start on a 16-byte boundary; the header says whether level 1
+// is sliced (and on how many bits).
 #include <cstring>
 #include <vector>
 
@@ -24,12 +25,13 @@ constexpr uint64_t IMAGE_MAGIC = 0x3146485048504D43ull;  // "CMPHPHF1"
 
 struct ImageHeader {
   uint64_t magic;
-  uint32_t version, k, m, nbins, levels, learned, key_words, pad;
+  uint32_t version, k, m, nbins, levels, learned, key_words;
+  int32_t l1_slice_bits;  // BBView::l1_slice_bits
   uint64_t n_distinct, n_leaves;
   uint64_t lut_off, dist_off_off, meta_off, ar_off, ar_words, roots_off, leaves_off, keys_off, total;
 };
 
-constexpr uint32_t IMAGE_VERSION = 3;
+constexpr uint32_t IMAGE_VERSION = 4;
 inline uint64_t align16(uint64_t x) { return (x + 15) & ~15ull; }  // sections are 16-byte aligned
 
 template <class KeyT>
@@ -48,6 +50,7 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   h.levels = NL;
   h.learned = learned;
   h.key_words = KOps<KeyT>::WORDS;
+  h.l1_slice_bits = be.bb.l1_slice_bits;
   h.n_distinct = c->n_distinct;
   h.n_leaves = nleaves;
   uint64_t off = align16(sizeof(ImageHeader));
@@ -99,6 +102,8 @@ void host_query_impl(const ImageHeader &h, const char *img, const uint64_t *keys
   v.bb.meta = reinterpret_cast<const BBMeta *>(img + h.meta_off);
   v.bb.levels = h.levels;
   v.bb.nbins = h.nbins;
+  v.bb.l1_slice_bits = h.l1_slice_bits;
+  v.bb.pad = 0;
   v.li.roots = reinterpret_cast<const LIRoot *>(img + h.roots_off);
   v.li.leaves = reinterpret_cast<const LILeaf *>(img + h.leaves_off);
   v.li.k = (int)h.k;

@@ -199,6 +199,12 @@ struct BBView {
   const ulonglong2 *AR;  // {cleaned bit word, level rank}, levels back to back
   const BBMeta *meta;    // [levels * nbins]
   uint32_t levels, nbins;
+  // >= 0: level 1 is sliced like level 0 (built by the phase-3 dedup): a
+  // bin's level-1 block is 2^l1_slice_bits slices of equal size, and a key's
+  // bit lies in the slice its level-0 hash's top l1_slice_bits bits name;
+  // -1: level 1 hashes over its bin's whole block like the later levels
+  int32_t l1_slice_bits;
+  uint32_t pad;
 };
 
 constexpr int LI_HIDDEN = 16;

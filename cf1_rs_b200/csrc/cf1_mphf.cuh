@@ -61,13 +61,34 @@ CF1_HD uint64_t bb_pos(uint64_t H, uint32_t l, uint32_t nwords) {
   return ((uint64_t)t * nwords) >> 26;
 }
 
+// Bit of a key (hash H) inside a slice of sw words at level l.
+CF1_HD uint32_t bb_slice_pos(uint64_t H, uint32_t l, uint32_t sw) {
+#ifdef __CUDA_ARCH__
+  const uint64_t mul = c_bb_mul[l];
+#else
+  const uint64_t mul = h_bb_mul[l];
+#endif
+  const uint32_t t = (uint32_t)((H * mul) >> 32);
+  return (uint32_t)(((uint64_t)t * sw) >> 26);
+}
+
+// Bit of a key at a sliced level l of nwords words in 2^P slices: the slice
+// is the top P bits of the level-0 hash (the key's phase-3 sub-bucket), the
+// bit inside it level l's own hash.
+CF1_HD uint64_t bb_pos_sliced(uint64_t H, uint32_t l, uint32_t nwords, int P) {
+  const uint32_t sw = nwords >> P;
+  const uint64_t sub = P ? (uint64_t)((uint32_t)((H * KEY_SPREAD_MUL) >> 32) >> (32 - P)) : 0;
+  return sub * 64 * sw + bb_slice_pos(H, l, sw);
+}
+
 // Levels [l0, l1) of a key's walk (hash H): the first level whose bit is set
 // gives the local slot.
 CF1_HD uint64_t bb_walk(const BBView &v, uint32_t bin, uint64_t H, uint32_t l0, uint32_t l1) {
   for (uint32_t l = l0; l < l1; l++) {
     const BBMeta mt = v.meta[(uint64_t)l * v.nbins + bin];
     if (mt.nwords == 0) return SLOT_NONE;
-    const uint64_t pos = bb_pos(H, l, mt.nwords);
+    const uint64_t pos = (l == 1 && v.l1_slice_bits >= 0) ? bb_pos_sliced(H, 1, mt.nwords, v.l1_slice_bits)
+                                                         : bb_pos(H, l, mt.nwords);
     const ulonglong2 e = v.AR[mt.word_off + (pos >> 6)];
     const uint32_t bit = (uint32_t)(pos & 63);
     if ((e.x >> bit) & 1) return (uint32_t)(mt.rank_adj + (uint32_t)e.y + (uint32_t)popc64(e.x & ((1ull << bit) - 1)));

@@ -430,28 +430,34 @@ CF1_D uint32_t cs_sort_unique_range(const KeyT *src, uint32_t m, const CsDigit &
       sh.sm);
 }
 
-// Level-0 slice of sub-bucket j (bin j >> P, slice j mod 2^P) over its n
-// distinct keys (see Level0Out); set/col: L0_SW_MAX words of shared memory
-// each; lb: lb_cap u16 of shared memory for the keys' bits in the slice (a
-// slice has at most L0_SW_MAX * 64 < 2^16 bits).  All threads call it.
+// Level-0 and level-1 slices of sub-bucket j (bin j >> P, slice j mod 2^P)
+// over its n distinct keys (see Level0Out); set/col: L0_SW_MAX words of
+// shared memory each (level 0's sw words, then level 1's sw1); lb: lb_cap
+// u16 of shared memory for the keys' bits in the slices (a slice has at most
+// L0_SW_MAX * 64 < 2^16 - 2 bits).  All threads call it.
 constexpr uint32_t L0_SW_MAX = 768;
 // With kpay (the keys' joined payload bytes) and o.with_pay, the payloads go
 // out as Level0Out describes; pw: L0_SW_MAX u32 of shared memory.
 CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const Level0Out &o,
                     unsigned long long *set, unsigned long long *col, uint16_t *lb, uint32_t lb_cap, uint32_t *sm,
                     unsigned long long *s_base, const uint8_t *kpay, uint64_t a, uint32_t *pw) {
+  constexpr uint16_t BAD = 0xFFFF, AT0 = 0xFFFE;  // lb[i]: no bit / placed at level 0 / else its level-1 bit
   const bool pay = o.with_pay && kpay;
   const unsigned tid = threadIdx.x;
   const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
   const uint64_t W = o.woff[bin + 1] - o.woff[bin];
   const uint32_t sw = (uint32_t)(W >> P);
+  const uint32_t sw1 = (uint32_t)((o.woff1[bin + 1] - o.woff1[bin]) >> P);
+  const uint64_t first1 = o.woff1[bin] + (uint64_t)sub * sw1;
   if (n == 0) {  // every slice writes all its entries (the array is not cleared first)
     for (uint32_t w = tid; w < sw; w += CS_BLOCK)
       o.AR[o.woff[bin] + (uint64_t)sub * sw + w] = make_ulonglong2(0ull, 0ull);
+    for (uint32_t w = tid; w < sw1; w += CS_BLOCK) o.AR1[first1 + w] = make_ulonglong2(0ull, 0ull);
     if (pay && tid == 0) o.placed[j] = 0;
     return;
   }
-  if (sw > L0_SW_MAX || sw == 0 || n > lb_cap) {
+  // level 1 uses the words of set, col and pw after level 0's
+  if (sw > L0_SW_MAX || sw + sw1 > L0_SW_MAX || sw1 > CS_BLOCK || sw == 0 || n > lb_cap) {
     if (tid == 0) {
       atomicOr(o.err, 1u);
       if (pay) o.placed[j] = 0;
@@ -466,7 +472,7 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
     const uint64_t b = bb_pos(keys[i], 0, (uint32_t)W) - lo_bit;
     if (b >= (uint64_t)sw * 64) {  // not this slice's key: cannot happen with the shared hash
       atomicOr(o.err, 1u);
-      lb[i] = 0xFFFF;
+      lb[i] = BAD;
       continue;
     }
     lb[i] = (uint16_t)b;
@@ -475,31 +481,58 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
   }
   __syncthreads();
   for (uint32_t w = tid; w < sw; w += CS_BLOCK) o.AR[first + w] = make_ulonglong2(set[w] & ~col[w], 0ull);
+  uint32_t placed0 = 0;
   if (pay) {
     // a placed key's rank in the slice: the placed bits before its bit
     // (words 2t and 2t+1 per thread: sw <= L0_SW_MAX <= 2 CS_BLOCK)
     const uint32_t w0 = 2 * tid, w1 = w0 + 1;
     const uint32_t c0 = w0 < sw ? (uint32_t)popc64(set[w0] & ~col[w0]) : 0u;
     const uint32_t c1 = w1 < sw ? (uint32_t)popc64(set[w1] & ~col[w1]) : 0u;
-    uint32_t placed_tot;
-    const uint32_t pre_w = block_exclusive_scan<CS_BLOCK>(c0 + c1, sm, placed_tot);
+    const uint32_t pre_w = block_exclusive_scan<CS_BLOCK>(c0 + c1, sm, placed0);
     if (w0 < sw) pw[w0] = pre_w;
     if (w1 < sw) pw[w1] = pre_w + c0;
-    if (tid == 0) o.placed[j] = placed_tot;
     __syncthreads();
     for (uint32_t i = tid; i < n; i += CS_BLOCK) {
       const uint32_t b = lb[i];
-      if (b == 0xFFFF) continue;
+      if (b == BAD) continue;
       const uint64_t fin = set[b >> 6] & ~col[b >> 6];
       const uint64_t bit = 1ull << (b & 63);
       if (fin & bit) o.l0pay[a + pw[b >> 6] + (uint32_t)popc64(fin & (bit - 1))] = kpay[i];
     }
   }
-  // the keys whose bit collided go on to level 1
-  uint32_t c = 0;
+  // level 1 (sliced, sw1 words): the keys whose level-0 bit collided
+  unsigned long long *set1 = set + sw, *col1 = col + sw;
+  uint32_t *pw1 = pw + sw;
+  for (uint32_t w = tid; w < sw1; w += CS_BLOCK) set1[w] = col1[w] = 0;
+  __syncthreads();
   for (uint32_t i = tid; i < n; i += CS_BLOCK) {
     const uint32_t b = lb[i];
-    c += b != 0xFFFF && ((col[b >> 6] >> (b & 63)) & 1);
+    if (b == BAD) continue;
+    if (!((col[b >> 6] >> (b & 63)) & 1)) {
+      lb[i] = AT0;
+      continue;
+    }
+    const uint32_t p1 = bb_slice_pos(keys[i], 1, sw1);
+    const unsigned long long bit = 1ull << (p1 & 63);
+    if (atomicOr(&set1[p1 >> 6], bit) & bit) atomicOr(&col1[p1 >> 6], bit);
+    lb[i] = (uint16_t)p1;
+  }
+  __syncthreads();
+  const unsigned long long g1 = tid < sw1 ? set1[tid] & ~col1[tid] : 0ull;  // sw1 <= CS_BLOCK
+  if (tid < sw1) o.AR1[first1 + tid] = make_ulonglong2(g1, 0ull);
+  uint32_t placed1;
+  const uint32_t pre1 = block_exclusive_scan<CS_BLOCK>((uint32_t)popc64(g1), sm, placed1);
+  if (tid < sw1) pw1[tid] = pre1;
+  if (pay && tid == 0) o.placed[j] = placed0 | (placed1 << 16);
+  __syncthreads();
+  // level-1 ranks, and the keys level 1 leaves go on to level 2
+  uint32_t c = 0;
+  for (uint32_t i = tid; i < n; i += CS_BLOCK) {
+    const uint32_t p1 = lb[i];
+    if (p1 == BAD || p1 == AT0) continue;
+    const uint64_t fin = set1[p1 >> 6] & ~col1[p1 >> 6], bit = 1ull << (p1 & 63);
+    if (!(fin & bit)) c++;
+    else if (pay) o.l0pay[a + placed0 + pw1[p1 >> 6] + (uint32_t)popc64(fin & (bit - 1))] = kpay[i];
   }
   uint32_t tot;
   uint32_t pre = block_exclusive_scan<CS_BLOCK>(c, sm, tot);
@@ -518,8 +551,9 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
   if (*s_base != ~0ull) {
     uint64_t out = o.surv_off[bin] + *s_base + pre;
     for (uint32_t i = tid; i < n; i += CS_BLOCK) {
-      const uint32_t b = lb[i];
-      if (b != 0xFFFF && ((col[b >> 6] >> (b & 63)) & 1)) {
+      const uint32_t p1 = lb[i];
+      if (p1 == BAD || p1 == AT0) continue;
+      if (!(((set1[p1 >> 6] & ~col1[p1 >> 6]) >> (p1 & 63)) & 1)) {
         if (pay) o.surv_pay[out] = kpay[i];
         o.surv[out++] = keys[i];
       }
@@ -713,16 +747,19 @@ constexpr int WD_WARPS = 8;                 // warps per CTA
 constexpr uint32_t WD_TW = 512;             // set slots per warp
 constexpr uint32_t WD_MAXD = WD_TW / 4 * 3; // distinct keys a warp's set takes
 constexpr uint32_t WD_SWMAX = 64;           // level-0 slice words a warp takes
+constexpr uint32_t WD_SW1MAX = (WD_SWMAX + 7) / 8;  // level-1 slice words (an eighth of level 0's)
 constexpr int WD_U = 4;                     // key loads in flight per lane
 constexpr uint32_t WD_RUN = 64;             // sub-buckets a warp takes at a time
 struct WdSmem {
   unsigned long long tab[WD_TW];
+  unsigned long long set[WD_SWMAX], col[WD_SWMAX];     // level-0 slice: bits set, bits set twice
+  unsigned long long set1[WD_SW1MAX], col1[WD_SW1MAX]; // level-1 slice
   uint8_t tpay[WD_TW];
-  uint16_t ins[WD_MAXD];                    // slots in insertion order, then the keys' level-0 bits
+  uint16_t ins[WD_MAXD];                    // the distinct keys' slots in insertion order
   uint8_t dp[WD_MAXD];                      // the distinct keys' joined payloads
-  unsigned long long set[WD_SWMAX], col[WD_SWMAX];
-  uint32_t pw[WD_SWMAX];                    // placed bits before each word
+  uint16_t pw[WD_SWMAX], pw1[WD_SW1MAX];    // placed bits before each word of the slices
 };
+static_assert(sizeof(WdSmem) % 8 == 0, "per-warp areas stay 8-byte aligned");
 
 __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T, uint8_t *TP, const uint64_t *sb_off,
                                                                    uint64_t nsub, int P, uint32_t *cnt, Level0Out l0,
@@ -732,7 +769,6 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
   const unsigned lane = lane_id(), lt = lanemask_lt();
   const unsigned long long EMPTY = ~0ull;  // above every key (keys use at most 62 bits)
   const bool pay = TP != nullptr, lv0 = l0.AR != nullptr, lpay = lv0 && l0.with_pay && pay;
-  constexpr uint16_t NO_BIT = 0xFFFF;      // a key outside its slice (cannot happen with the shared hash)
   for (uint32_t i = lane; i < WD_TW; i += 32) {
     m.tab[i] = EMPTY;
     m.tpay[i] = 0;
@@ -812,8 +848,10 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
         for (uint32_t w = lane; w < sw; w += 32) m.set[w] = m.col[w] = 0;
         __syncwarp();
       }
-      // 2. the distinct keys (and bytes) to T[a, a + d), the set emptied; with
-      //    level 0, each key's bit marked and kept in ins, its byte in dp
+      // 2. the distinct keys (and bytes) to T[a, a + d); with level 0, each
+      //    key's bit marked and its byte kept in dp, the key itself left in
+      //    the set (ins[r] stays its slot) until step 5 empties it; a key's
+      //    level-0 and level-1 bits are recomputed from it where needed
       bool bad = false;
       for (uint32_t r = lane; r < d; r += 32) {
         const uint32_t h = m.ins[r];
@@ -821,20 +859,18 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
         const uint8_t pr = m.tpay[h];
         T[a + r] = key;
         if (pay) TP[a + r] = pr;
-        m.tab[h] = EMPTY;
         m.tpay[h] = 0;
         if (lv0) {
           const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
-          uint16_t bb = NO_BIT;
           if (bpos < (uint64_t)sw * 64) {
-            bb = (uint16_t)bpos;
             const unsigned long long bit = 1ull << (bpos & 63);
             if (atomicOr(&m.set[bpos >> 6], bit) & bit) atomicOr(&m.col[bpos >> 6], bit);
           } else {
-            bad = true;
+            bad = true;  // not this slice's key: cannot happen with the shared hash
           }
-          m.ins[r] = bb;
           m.dp[r] = pr;
+        } else {
+          m.tab[h] = EMPTY;
         }
       }
       if (lane == 0) cnt[j] = d;
@@ -853,38 +889,73 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
       const uint32_t c0 = (uint32_t)__popcll(f0), c1 = (uint32_t)__popcll(f1);
       const uint32_t i0 = warp_inclusive_scan(c0), i1 = warp_inclusive_scan(c1);
       const uint32_t t0 = __shfl_sync(FULL, i0, 31), placed = t0 + __shfl_sync(FULL, i1, 31);
-      if (lane < sw) m.pw[lane] = i0 - c0;
-      if (lane + 32 < sw) m.pw[lane + 32] = t0 + i1 - c1;
-      if (lpay && lane == 0) l0.placed[j] = placed;
-      // survivors: one reservation in the bin's list
+      if (lane < sw) m.pw[lane] = (uint16_t)(i0 - c0);
+      if (lane + 32 < sw) m.pw[lane + 32] = (uint16_t)(t0 + i1 - c1);
+      // 4. level 1: each key level 0 leaves marks its bit in the sub-bucket's
+      //    level-1 slice (sw1 words, its bit from level 1's hash)
+      const uint32_t sw1 = (uint32_t)((l0.woff1[bin + 1] - l0.woff1[bin]) >> P);
+      const uint64_t first1 = l0.woff1[bin] + (uint64_t)sub * sw1;
+      const bool l1ok = sw1 <= WD_SW1MAX;  // always: level 1 is sized from level 0
+      if (lane < sw1 && l1ok) m.set1[lane] = m.col1[lane] = 0;
+      __syncwarp();
+      for (uint32_t r = lane; r < d && l1ok; r += 32) {
+        const unsigned long long key = m.tab[m.ins[r]];
+        const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
+        if (bpos >= (uint64_t)sw * 64 || !((m.col[bpos >> 6] >> (bpos & 63)) & 1)) continue;  // placed at level 0
+        const uint32_t p1 = bb_slice_pos(key, 1, sw1);
+        const unsigned long long bit = 1ull << (p1 & 63);
+        if (atomicOr(&m.set1[p1 >> 6], bit) & bit) atomicOr(&m.col1[p1 >> 6], bit);
+      }
+      __syncwarp();
+      const unsigned long long g1 = (lane < sw1 && l1ok) ? m.set1[lane] & ~m.col1[lane] : 0ull;
+      if (lane < sw1 && l1ok) l0.AR1[first1 + lane] = make_ulonglong2(g1, 0ull);
+      const uint32_t e1 = (uint32_t)__popcll(g1), k1 = warp_inclusive_scan(e1);
+      const uint32_t placed1 = __shfl_sync(FULL, k1, 31);
+      if (lane < sw1 && l1ok) m.pw1[lane] = (uint16_t)(k1 - e1);
+      if (lpay && lane == 0) l0.placed[j] = placed | (placed1 << 16);
+      // survivors of level 1: one reservation in the bin's list
       unsigned long long sbase = 0;
-      if (lane == 0 && d > placed) {
-        sbase = atomicAdd(&l0.surv_cnt[bin], (unsigned long long)(d - placed));
-        if (sbase + (d - placed) > l0.surv_off[bin + 1] - l0.surv_off[bin]) {
+      const uint32_t nsurv = d - placed - placed1;
+      if (lane == 0 && (nsurv || !l1ok)) {
+        if (l1ok) sbase = atomicAdd(&l0.surv_cnt[bin], (unsigned long long)nsurv);
+        if (!l1ok || sbase + nsurv > l0.surv_off[bin + 1] - l0.surv_off[bin]) {
           atomicOr(l0.err, 1u);
           sbase = ~0ull;
         }
       }
       sbase = __shfl_sync(FULL, sbase, 0);
       __syncwarp();
-      // 4. each key: its byte to its rank (placed) or the key to level 1
+      // 5. each key: its byte to its rank (level 0, then level 1) or the key
+      //    to level 2; the set emptied
       uint64_t so = l0.surv_off[bin] + sbase;
       for (uint32_t r0 = 0; r0 < d; r0 += 32) {
         const uint32_t r = r0 + lane;
         bool surv = false;
-        if (r < d && m.ins[r] != NO_BIT) {
-          const uint32_t bb = m.ins[r];
-          const unsigned long long fin = m.set[bb >> 6] & ~m.col[bb >> 6], bit = 1ull << (bb & 63);
-          if (fin & bit) {
-            if (lpay) l0.l0pay[a + m.pw[bb >> 6] + (uint32_t)__popcll(fin & (bit - 1))] = m.dp[r];
-          } else {
-            surv = true;
+        unsigned long long key = 0;
+        if (r < d) {
+          const uint32_t h = m.ins[r];
+          key = m.tab[h];
+          m.tab[h] = EMPTY;
+          const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
+          if (bpos < (uint64_t)sw * 64 && l1ok) {
+            const unsigned long long fin = m.set[bpos >> 6] & ~m.col[bpos >> 6], bit = 1ull << (bpos & 63);
+            if (fin & bit) {
+              if (lpay) l0.l0pay[a + m.pw[bpos >> 6] + (uint32_t)__popcll(fin & (bit - 1))] = m.dp[r];
+            } else {
+              const uint32_t p1 = bb_slice_pos(key, 1, sw1);
+              const unsigned long long fin1 = m.set1[p1 >> 6] & ~m.col1[p1 >> 6], bit1 = 1ull << (p1 & 63);
+              if (fin1 & bit1) {
+                if (lpay) l0.l0pay[a + placed + m.pw1[p1 >> 6] + (uint32_t)__popcll(fin1 & (bit1 - 1))] = m.dp[r];
+              } else {
+                surv = true;
+              }
+            }
           }
         }
         const unsigned sb = __ballot_sync(FULL, surv);
         if (surv && sbase != ~0ull) {
           const uint64_t at = so + __popc(sb & lt);
-          l0.surv[at] = T[a + r];
+          l0.surv[at] = key;
           if (lpay) l0.surv_pay[at] = m.dp[r];
         }
         so += __popc(sb);

@@ -34,17 +34,25 @@ int msd_prefix_bits(uint64_t max_bin_keys, bool sorted);
 // j of bin b owns words [j, j + 1) * (block / 2^P) of it alone, so its CTA
 // marks, clears and writes them with no atomics in global memory and lists
 // the keys it does not place.
+// BBHash levels 0 and 1 built by the unsorted dedup: each sub-bucket j (bin
+// b, slice sub) marks its keys in its slice of level 0 (sw0 words), and the
+// keys level 0 leaves in its slice of level 1 (sw1 words; level 1 is sliced,
+// see BBView); the keys level 1 leaves are listed for level 2.
 struct Level0Out {
   ulonglong2 *AR = nullptr;                // level-0 entries (each slice writes all of its); nullptr: off
-  const uint64_t *woff = nullptr;          // [nbins + 1] block offsets
-  uint64_t *surv = nullptr;                // keys level 0 leaves: bin b's from surv_off[b]
+  const uint64_t *woff = nullptr;          // [nbins + 1] level-0 block offsets (sw0 << P words per bin)
+  ulonglong2 *AR1 = nullptr;               // level-1 entries (each slice writes all of its)
+  const uint64_t *woff1 = nullptr;         // [nbins + 1] level-1 block offsets (sw1 << P words per bin)
+  uint64_t *surv = nullptr;                // keys level 1 leaves: bin b's from surv_off[b]
   const uint64_t *surv_off = nullptr;      // [nbins + 1]; bin b's room is surv_off[b+1] - surv_off[b]
   unsigned long long *surv_cnt = nullptr;  // [nbins], zeroed
   uint32_t *err = nullptr;                 // set when a slice or a bin's room is too small
   // Joined side sets (payload bytes beside the keys): a key level 0 places
   // gets local rank r inside its slice (the set bits before its bit), and
-  // its byte goes to l0pay[sub-bucket start + r]; placed[j] = the slice's
-  // placed keys; a key level 0 leaves takes its byte along to surv_pay.
+  // its byte goes to l0pay[sub-bucket start + r]; a key level 1 places, rank
+  // r1 in its level-1 slice, to l0pay[sub-bucket start + placed0 + r1];
+  // placed[j] = placed0 | placed1 << 16; a key level 1 leaves takes its byte
+  // along to surv_pay.
   bool with_pay = false;
   uint8_t *l0pay = nullptr;    // filled by msd_sort_unique: the payload buffer the kept bytes are not in
   uint8_t *surv_pay = nullptr; // beside surv

@@ -227,28 +227,41 @@ __global__ void __launch_bounds__(256) place_sides_kernel(MphfView<KeyT> m, cons
   if (__any_sync(FULL, miss) && lane == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
 }
 
-// One warp per sub-bucket: the level-0 keys' bytes, already in rank order,
-// to the slice's run of slots.
+// One warp per sub-bucket: the bytes of the keys levels 0 and 1 placed,
+// already in rank order, to the two slices' runs of slots (placed[j] =
+// placed0 | placed1 << 16; level 1's bytes follow level 0's in l0pay).
 __global__ void __launch_bounds__(256) place_l0_kernel(BBView bb, const uint64_t *dist_off, const uint64_t *sb_off,
                                                        const uint32_t *placed, const uint8_t *l0pay, uint64_t j0,
                                                        uint64_t j1, int P, uint8_t *sides, uint32_t *err) {
   const uint64_t j = j0 + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (j >= j1) return;
-  const uint32_t np = placed[j];
-  if (!np) return;
+  const uint32_t pl = placed[j];
+  if (!pl) return;
+  const uint32_t np0 = pl & 0xFFFFu, np1 = pl >> 16;
   const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
-  const BBMeta m0 = bb.meta[bin];
-  const uint64_t first = m0.word_off + (uint64_t)sub * (m0.nwords >> P);
-  const uint64_t base = dist_off[bin] + (uint32_t)(m0.rank_adj + (uint32_t)bb.AR[first].y);
-  if (base + np > dist_off[bin + 1]) {
-    if (lane_id() == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
-    return;
-  }
   const uint8_t *src = l0pay + sb_off[j];
-  for (uint32_t r = lane_id(); r < np; r += 32) sides[base + r] = src[r];
+  bool bad = false;
+  if (np0) {
+    const BBMeta m0 = bb.meta[bin];
+    const uint64_t first = m0.word_off + (uint64_t)sub * (m0.nwords >> P);
+    const uint64_t base = dist_off[bin] + (uint32_t)(m0.rank_adj + (uint32_t)bb.AR[first].y);
+    if (base + np0 > dist_off[bin + 1]) bad = true;
+    else
+      for (uint32_t r = lane_id(); r < np0; r += 32) sides[base + r] = src[r];
+  }
+  if (np1) {
+    const BBMeta m1 = bb.meta[bb.nbins + bin];
+    const uint64_t first = m1.word_off + (uint64_t)sub * (m1.nwords >> P);
+    const uint64_t base = dist_off[bin] + (uint32_t)(m1.rank_adj + (uint32_t)bb.AR[first].y);
+    if (base + np1 > dist_off[bin + 1] || bb.levels < 2) bad = true;
+    else
+      for (uint32_t r = lane_id(); r < np1; r += 32) sides[base + r] = src[np0 + r];
+  }
+  if (bad && lane_id() == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
 }
 
-// The keys level 0 left: SV_CTAS CTAs per bin, each key walks from level 1.
+// The keys levels 0 and 1 left: SV_CTAS CTAs per bin, each key walks from
+// level 2.
 constexpr uint32_t SV_CTAS = 32;
 __global__ void __launch_bounds__(256) place_surv_kernel(BBView bb, const uint64_t *dist_off, const uint64_t *surv,
                                                          const uint8_t *surv_pay, const uint64_t *surv_off,
@@ -258,7 +271,7 @@ __global__ void __launch_bounds__(256) place_surv_kernel(BBView bb, const uint64
   const uint64_t n = surv_cnt[bin], s0 = surv_off[bin], base = dist_off[bin], end = dist_off[bin + 1];
   bool miss = false;
   for (uint64_t i = (uint64_t)part * blockDim.x + threadIdx.x; i < n; i += (uint64_t)SV_CTAS * blockDim.x) {
-    const uint64_t local = bb_walk(bb, bin, bb_key_hash(surv[s0 + i]), 1, bb.levels);
+    const uint64_t local = bb_walk(bb, bin, bb_key_hash(surv[s0 + i]), 2, bb.levels);
     const uint64_t slot = local == SLOT_NONE ? SLOT_NONE : base + local;
     if (slot >= base && slot < end) sides[slot] = surv_pay[s0 + i];
     else miss = true;

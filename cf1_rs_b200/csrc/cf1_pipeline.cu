@@ -529,32 +529,40 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     if (batched) CF1_CUDA(cudaMemsetAsync(&sm->queues[4], 0, sizeof(uint32_t), s));
   }
   int P = msd_width(c->tune.msd_delta);
-  // BBHash form, 64-bit keys: the dedup builds BBHash level 0 on the way
-  // (Level0Out), 8 bits per k-mer occurrence of the bin rounded up to a
-  // multiple of the bin's 2^P slices; the keys it leaves go to a list with
-  // room for a quarter of the bin's occurrences.
+  // BBHash form, 64-bit keys: the dedup builds BBHash levels 0 and 1 on the
+  // way (Level0Out): level 0 with 8 bits per k-mer occurrence of the bin
+  // rounded up to a multiple of the bin's 2^P slices, level 1 with an eighth
+  // of level 0's words per slice (the keys level 0 leaves are ~10% of its
+  // distinct keys, so ~10 bits each); the keys level 1 leaves go to a list
+  // with room for a quarter of the bin's occurrences.
   const bool l0_fuse = !sorted && !c->wide && c->opts.mphf_mode == CF1GPU_MPHF_BBHASH && P >= 0;
   Level0Out l0;
-  uint64_t l0_words = 0, l0_room = 0;
+  uint64_t l0_words = 0, l1_words = 0, l0_room = 0;
   if (l0_fuse) {
-    std::vector<uint64_t> hw(B + 1, 0), hr(B + 1, 0);
+    std::vector<uint64_t> hw(B + 1, 0), hw1(B + 1, 0), hr(B + 1, 0);
     const uint64_t slices = 1ull << P;
     for (uint32_t b = 0; b < B; b++) {
       const uint64_t occ = hseg[b + 1] - hseg[b];
-      const uint64_t wb = occ ? ceil_div(ceil_div(8 * occ, 64), slices) * slices : 0;
-      hw[b + 1] = hw[b] + wb;
+      const uint64_t sw0 = occ ? ceil_div(ceil_div(8 * occ, 64), slices) : 0;
+      hw[b + 1] = hw[b] + sw0 * slices;
+      hw1[b + 1] = hw1[b] + ceil_div(sw0, 8) * slices;
       hr[b + 1] = hr[b] + (occ ? occ / 4 + 64 : 0);
     }
     l0_words = hw[B];
+    l1_words = hw1[B];
     l0_room = hr[B];
-    uint64_t *woff0 = c->d_l0.get<uint64_t>(3 * (size_t)(B + 1));
+    uint64_t *woff0 = c->d_l0.get<uint64_t>(4 * (size_t)(B + 1));
     uint64_t *room_off = woff0 + (B + 1);
     unsigned long long *scnt = reinterpret_cast<unsigned long long *>(room_off + (B + 1));
+    uint64_t *woff1 = room_off + 2 * (size_t)(B + 1);
     CF1_CUDA(cudaMemcpyAsync(woff0, hw.data(), (B + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    CF1_CUDA(cudaMemcpyAsync(woff1, hw1.data(), (B + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
     CF1_CUDA(cudaMemcpyAsync(room_off, hr.data(), (B + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
     CF1_CUDA(cudaMemsetAsync(scnt, 0, B * sizeof(uint64_t), s));
-    l0.AR = be.bb.prepare_level0(l0_words, s);  // every slice writes all of its entries
+    l0.AR = be.bb.prepare_levels01(l0_words, l1_words, s);  // every slice writes all of its entries
     l0.woff = woff0;
+    l0.AR1 = l0.AR + l0_words;
+    l0.woff1 = woff1;
     l0.surv = c->d_l0surv.get<uint64_t>(l0_room + 1);
     l0.surv_off = room_off;
     l0.surv_cnt = scnt;
@@ -616,8 +624,9 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     be.li.build(dist, dist_off, B, k, c->learned, s);
     be.bb.build(dist, dist_off, B, be.li.fallback_sel(), s, keys, ws1, NO + 1);
   } else if (l0_ready) {
-    be.bb.build_from_level0(B, l0.woff, l0_words, reinterpret_cast<const KeyT *>(l0.surv), l0.surv_off,
-                            reinterpret_cast<const uint64_t *>(l0.surv_cnt), l0_room, s, twin, twin + half, half);
+    be.bb.build_from_levels01(B, P, l0.woff, l0_words, l0.woff1, l1_words, reinterpret_cast<const KeyT *>(l0.surv),
+                              l0.surv_off, reinterpret_cast<const uint64_t *>(l0.surv_cnt), l0_room, s, twin,
+                              twin + half, half);
   } else {
     be.bb.build(dist, dist_off, B, nullptr, s, keys, ws1, NO + 1);
   }
