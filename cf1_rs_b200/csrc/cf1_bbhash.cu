@@ -157,6 +157,36 @@ __global__ void bb_meta_kernel(const uint64_t *woff, const uint64_t *R, uint64_t
   base[b] += R[w1] - R[w0];
 }
 
+// A sliced level (levels 0 and 1 of the phase-3 dedup): each entry holds
+// {placed bits, placed bits of its slice before it}; R = the exclusive scan
+// of the slices' placed counts over the whole level (slices of bin b are
+// [b << P, (b + 1) << P)).  One warp per slice adds the slice's level-wide
+// start to its entries' ranks.
+__global__ void bb_slice_rank_kernel(ulonglong2 *AR, const uint64_t *woff, const uint64_t *R, int P, uint64_t nsub) {
+  const uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (j >= nsub) return;
+  const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
+  const uint32_t sw = (uint32_t)((woff[bin + 1] - woff[bin]) >> P);
+  const uint64_t first = woff[bin] + (uint64_t)sub * sw, r0 = R[j];
+  for (uint32_t w = lane_id(); w < sw; w += 32) AR[first + w].y += r0;
+}
+
+// Metadata of a sliced level from the slices' scanned counts (as
+// bb_meta_kernel, with the level's rank at the bin's first and last word
+// read at the bin's first slice and one past its last).
+__global__ void bb_meta_sliced_kernel(const uint64_t *woff, const uint64_t *R, int P, uint64_t level_base,
+                                      uint64_t *base, BBMeta *meta, uint32_t nbins) {
+  uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbins) return;
+  const uint64_t r0 = R[(uint64_t)b << P], r1 = R[(uint64_t)(b + 1) << P];
+  BBMeta m;
+  m.word_off = level_base + woff[b];
+  m.nwords = (uint32_t)(woff[b + 1] - woff[b]);
+  m.rank_adj = (uint32_t)(base[b] - r0);
+  meta[b] = m;
+  base[b] += r1 - r0;
+}
+
 // Keys whose bit did not survive go to the next level: each tile appends its
 // survivors to out[start[b] + ...] behind one atomic on the bin's next count
 // (the order of the keys inside a bin does not matter to BBHash).
@@ -335,18 +365,33 @@ ulonglong2 *BBHashBuild<KeyT>::prepare_levels01(uint64_t words0, uint64_t words1
 }
 
 template <class KeyT>
+void BBHashBuild<KeyT>::finish_sliced(uint32_t l, const uint64_t *woff, const uint32_t *placed, int P,
+                                      cudaStream_t s) {
+  const uint64_t nsub = (uint64_t)nbins << P;
+  ulonglong2 *Al = ar_.as<ulonglong2>() + total_words;
+  uint64_t *R = rtmp_.get<uint64_t>(nsub + 1);
+  exclusive_scan_u32(placed, R, nsub, scan_tmp_, s);
+  bb_slice_rank_kernel<<<(unsigned)ceil_div(nsub * 32, 256), 256, 0, s>>>(Al, woff, R, P, nsub);
+  CF1_LAUNCH_CHECK();
+  bb_meta_sliced_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(
+      woff, R, P, total_words, base_.as<uint64_t>(), meta_.as<BBMeta>() + (size_t)l * nbins, nbins);
+  CF1_LAUNCH_CHECK();
+}
+
+template <class KeyT>
 void BBHashBuild<KeyT>::build_from_levels01(uint32_t nb, int P, const uint64_t *woff0, uint64_t words0,
-                                            const uint64_t *woff1, uint64_t words1, const KeyT *surv,
-                                            const uint64_t *surv_off, const uint64_t *surv_cnt, uint64_t surv_total,
-                                            cudaStream_t s, KeyT *ws0, KeyT *ws1, uint64_t ws_cap) {
+                                            const uint32_t *placed0, const uint64_t *woff1, uint64_t words1,
+                                            const uint32_t *placed1, const KeyT *surv, const uint64_t *surv_off,
+                                            const uint64_t *surv_cnt, uint64_t surv_total, cudaStream_t s, KeyT *ws0,
+                                            KeyT *ws1, uint64_t ws_cap) {
   begin(nb, s);
   nwords.push_back(words0);
   level_off.push_back(0);
-  finish_level(0, woff0, words0, s);
+  finish_sliced(0, woff0, placed0, P, s);
   total_words = words0;
   nwords.push_back(words1);
   level_off.push_back(words0);
-  finish_level(1, woff1, words1, s);
+  finish_sliced(1, woff1, placed1, P, s);
   total_words += words1;
   l1_slice_bits = P;
   CF1_CUDA(cudaMemcpyAsync(cnt_[0].as<uint64_t>(), surv_cnt, nbins * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));

@@ -26,16 +26,17 @@ struct BBHashBuild {
   // Levels 0 and 1 built elsewhere (the unsorted phase-3 dedup, one
   // exclusive slice of each per sub-bucket; level 1 sliced, see BBView):
   // prepare_levels01 gives the entry array to fill with level 0's cleaned
-  // bit words ({bits, 0}) at [0, words0) and level 1's at [words0, words0 +
-  // words1); build_from_levels01 ranks both and builds the later levels over
-  // the keys level 1 left (bin b's at surv[surv_off[b] + [0, surv_cnt[b])]).
-  // woff0 / woff1: the bins' block offsets [nbins + 1] of levels 0 and 1;
-  // P: the slice bits.
+  // bit words at [0, words0) and level 1's at [words0, words0 + words1), as
+  // {bits, placed bits of the slice before the word}; build_from_levels01
+  // ranks both from the slices' placed counts (placed0 / placed1, one per
+  // sub-bucket) and builds the later levels over the keys level 1 left (bin
+  // b's at surv[surv_off[b] + [0, surv_cnt[b])]).  woff0 / woff1: the bins'
+  // block offsets [nbins + 1] of levels 0 and 1; P: the slice bits.
   ulonglong2 *prepare_levels01(uint64_t words0, uint64_t words1, cudaStream_t s);
-  void build_from_levels01(uint32_t nbins, int P, const uint64_t *woff0, uint64_t words0, const uint64_t *woff1,
-                           uint64_t words1, const KeyT *surv, const uint64_t *surv_off, const uint64_t *surv_cnt,
-                           uint64_t surv_total, cudaStream_t s, KeyT *ws0 = nullptr, KeyT *ws1 = nullptr,
-                           uint64_t ws_cap = 0);
+  void build_from_levels01(uint32_t nbins, int P, const uint64_t *woff0, uint64_t words0, const uint32_t *placed0,
+                           const uint64_t *woff1, uint64_t words1, const uint32_t *placed1, const KeyT *surv,
+                           const uint64_t *surv_off, const uint64_t *surv_cnt, uint64_t surv_total, cudaStream_t s,
+                           KeyT *ws0 = nullptr, KeyT *ws1 = nullptr, uint64_t ws_cap = 0);
   BBView view() const;
   void clear();
   uint64_t level_words(uint32_t l) const;
@@ -48,6 +49,7 @@ struct BBHashBuild {
   void reserve_entries(uint64_t words, uint64_t keep, cudaStream_t s);
   void begin(uint32_t nbins, cudaStream_t s);
   void finish_level(uint32_t l, const uint64_t *woff, uint64_t nw, cudaStream_t s);
+  void finish_sliced(uint32_t l, const uint64_t *woff, const uint32_t *placed, int P, cudaStream_t s);
   void run_levels(uint32_t l, const KeyT *rem, const uint64_t *start, KeyT *r0, KeyT *r1, cudaStream_t s);
 
   // The entry array and the level buffers are kept across builds and grown on

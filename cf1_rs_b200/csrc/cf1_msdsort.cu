@@ -453,14 +453,14 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
     for (uint32_t w = tid; w < sw; w += CS_BLOCK)
       o.AR[o.woff[bin] + (uint64_t)sub * sw + w] = make_ulonglong2(0ull, 0ull);
     for (uint32_t w = tid; w < sw1; w += CS_BLOCK) o.AR1[first1 + w] = make_ulonglong2(0ull, 0ull);
-    if (pay && tid == 0) o.placed[j] = 0;
+    if (tid == 0) o.placed[j] = o.placed1[j] = 0;
     return;
   }
   // level 1 uses the words of set, col and pw after level 0's
   if (sw > L0_SW_MAX || sw + sw1 > L0_SW_MAX || sw1 > CS_BLOCK || sw == 0 || n > lb_cap) {
     if (tid == 0) {
       atomicOr(o.err, 1u);
-      if (pay) o.placed[j] = 0;
+      o.placed[j] = o.placed1[j] = 0;
     }
     return;
   }
@@ -480,17 +480,25 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
     if (atomicOr(&set[b >> 6], bit) & bit) atomicOr(&col[b >> 6], bit);
   }
   __syncthreads();
-  for (uint32_t w = tid; w < sw; w += CS_BLOCK) o.AR[first + w] = make_ulonglong2(set[w] & ~col[w], 0ull);
+  // the placed bits of the slice before each word (words 2t and 2t+1 per
+  // thread: sw <= L0_SW_MAX <= 2 CS_BLOCK), written beside the word
   uint32_t placed0 = 0;
-  if (pay) {
-    // a placed key's rank in the slice: the placed bits before its bit
-    // (words 2t and 2t+1 per thread: sw <= L0_SW_MAX <= 2 CS_BLOCK)
+  {
     const uint32_t w0 = 2 * tid, w1 = w0 + 1;
     const uint32_t c0 = w0 < sw ? (uint32_t)popc64(set[w0] & ~col[w0]) : 0u;
     const uint32_t c1 = w1 < sw ? (uint32_t)popc64(set[w1] & ~col[w1]) : 0u;
     const uint32_t pre_w = block_exclusive_scan<CS_BLOCK>(c0 + c1, sm, placed0);
-    if (w0 < sw) pw[w0] = pre_w;
-    if (w1 < sw) pw[w1] = pre_w + c0;
+    if (w0 < sw) {
+      pw[w0] = pre_w;
+      o.AR[first + w0] = make_ulonglong2(set[w0] & ~col[w0], (unsigned long long)pre_w);
+    }
+    if (w1 < sw) {
+      pw[w1] = pre_w + c0;
+      o.AR[first + w1] = make_ulonglong2(set[w1] & ~col[w1], (unsigned long long)(pre_w + c0));
+    }
+  }
+  if (pay) {
+    // a placed key's rank in the slice: the placed bits before its bit
     __syncthreads();
     for (uint32_t i = tid; i < n; i += CS_BLOCK) {
       const uint32_t b = lb[i];
@@ -519,11 +527,16 @@ CF1_D void l0_slice(const uint64_t *keys, uint32_t n, uint64_t j, int P, const L
   }
   __syncthreads();
   const unsigned long long g1 = tid < sw1 ? set1[tid] & ~col1[tid] : 0ull;  // sw1 <= CS_BLOCK
-  if (tid < sw1) o.AR1[first1 + tid] = make_ulonglong2(g1, 0ull);
   uint32_t placed1;
   const uint32_t pre1 = block_exclusive_scan<CS_BLOCK>((uint32_t)popc64(g1), sm, placed1);
-  if (tid < sw1) pw1[tid] = pre1;
-  if (pay && tid == 0) o.placed[j] = placed0 | (placed1 << 16);
+  if (tid < sw1) {
+    pw1[tid] = pre1;
+    o.AR1[first1 + tid] = make_ulonglong2(g1, (unsigned long long)pre1);
+  }
+  if (tid == 0) {
+    o.placed[j] = placed0;
+    o.placed1[j] = placed1;
+  }
   __syncthreads();
   // level-1 ranks, and the keys level 1 leaves go on to level 2
   uint32_t c = 0;
@@ -884,13 +897,17 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
       //    (sw <= 64: two words a lane)
       const unsigned long long f0 = lane < sw ? m.set[lane] & ~m.col[lane] : 0ull;
       const unsigned long long f1 = lane + 32 < sw ? m.set[lane + 32] & ~m.col[lane + 32] : 0ull;
-      if (lane < sw) l0.AR[first + lane] = make_ulonglong2(f0, 0ull);
-      if (lane + 32 < sw) l0.AR[first + lane + 32] = make_ulonglong2(f1, 0ull);
       const uint32_t c0 = (uint32_t)__popcll(f0), c1 = (uint32_t)__popcll(f1);
       const uint32_t i0 = warp_inclusive_scan(c0), i1 = warp_inclusive_scan(c1);
       const uint32_t t0 = __shfl_sync(FULL, i0, 31), placed = t0 + __shfl_sync(FULL, i1, 31);
-      if (lane < sw) m.pw[lane] = (uint16_t)(i0 - c0);
-      if (lane + 32 < sw) m.pw[lane + 32] = (uint16_t)(t0 + i1 - c1);
+      if (lane < sw) {
+        m.pw[lane] = (uint16_t)(i0 - c0);
+        l0.AR[first + lane] = make_ulonglong2(f0, (unsigned long long)(i0 - c0));
+      }
+      if (lane + 32 < sw) {
+        m.pw[lane + 32] = (uint16_t)(t0 + i1 - c1);
+        l0.AR[first + lane + 32] = make_ulonglong2(f1, (unsigned long long)(t0 + i1 - c1));
+      }
       // 4. level 1: each key level 0 leaves marks its bit in the sub-bucket's
       //    level-1 slice (sw1 words, its bit from level 1's hash)
       const uint32_t sw1 = (uint32_t)((l0.woff1[bin + 1] - l0.woff1[bin]) >> P);
@@ -908,11 +925,16 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
       }
       __syncwarp();
       const unsigned long long g1 = (lane < sw1 && l1ok) ? m.set1[lane] & ~m.col1[lane] : 0ull;
-      if (lane < sw1 && l1ok) l0.AR1[first1 + lane] = make_ulonglong2(g1, 0ull);
       const uint32_t e1 = (uint32_t)__popcll(g1), k1 = warp_inclusive_scan(e1);
       const uint32_t placed1 = __shfl_sync(FULL, k1, 31);
-      if (lane < sw1 && l1ok) m.pw1[lane] = (uint16_t)(k1 - e1);
-      if (lpay && lane == 0) l0.placed[j] = placed | (placed1 << 16);
+      if (lane < sw1 && l1ok) {
+        m.pw1[lane] = (uint16_t)(k1 - e1);
+        l0.AR1[first1 + lane] = make_ulonglong2(g1, (unsigned long long)(k1 - e1));
+      }
+      if (lane == 0) {
+        l0.placed[j] = placed;
+        l0.placed1[j] = placed1;
+      }
       // survivors of level 1: one reservation in the bin's list
       unsigned long long sbase = 0;
       const uint32_t nsurv = d - placed - placed1;

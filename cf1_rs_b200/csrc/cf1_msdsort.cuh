@@ -47,16 +47,20 @@ struct Level0Out {
   const uint64_t *surv_off = nullptr;      // [nbins + 1]; bin b's room is surv_off[b+1] - surv_off[b]
   unsigned long long *surv_cnt = nullptr;  // [nbins], zeroed
   uint32_t *err = nullptr;                 // set when a slice or a bin's room is too small
+  // Each slice's entries are written as {placed bits, placed bits of the
+  // slice before the word}; placed[j] / placed1[j] = the keys level 0 / 1
+  // places in sub-bucket j, from which the build turns the entries' ranks
+  // into level-wide ones.
+  uint32_t *placed = nullptr;   // [nsub]
+  uint32_t *placed1 = nullptr;  // [nsub]
   // Joined side sets (payload bytes beside the keys): a key level 0 places
   // gets local rank r inside its slice (the set bits before its bit), and
   // its byte goes to l0pay[sub-bucket start + r]; a key level 1 places, rank
-  // r1 in its level-1 slice, to l0pay[sub-bucket start + placed0 + r1];
-  // placed[j] = placed0 | placed1 << 16; a key level 1 leaves takes its byte
-  // along to surv_pay.
+  // r1 in its level-1 slice, to l0pay[sub-bucket start + placed[j] + r1]; a
+  // key level 1 leaves takes its byte along to surv_pay.
   bool with_pay = false;
   uint8_t *l0pay = nullptr;    // filled by msd_sort_unique: the payload buffer the kept bytes are not in
   uint8_t *surv_pay = nullptr; // beside surv
-  uint32_t *placed = nullptr;  // [nsub]
 };
 
 // With dist = nullptr the distinct keys stay where the dedup left them, at

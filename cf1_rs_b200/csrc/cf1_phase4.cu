@@ -227,17 +227,17 @@ __global__ void __launch_bounds__(256) place_sides_kernel(MphfView<KeyT> m, cons
   if (__any_sync(FULL, miss) && lane == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
 }
 
-// One warp per sub-bucket: the bytes of the keys levels 0 and 1 placed,
-// already in rank order, to the two slices' runs of slots (placed[j] =
-// placed0 | placed1 << 16; level 1's bytes follow level 0's in l0pay).
+// One warp per sub-bucket: the bytes of the keys levels 0 and 1 placed
+// (placed[j] and placed1[j] of them), already in rank order, to the two
+// slices' runs of slots (level 1's bytes follow level 0's in l0pay).
 __global__ void __launch_bounds__(256) place_l0_kernel(BBView bb, const uint64_t *dist_off, const uint64_t *sb_off,
-                                                       const uint32_t *placed, const uint8_t *l0pay, uint64_t j0,
-                                                       uint64_t j1, int P, uint8_t *sides, uint32_t *err) {
+                                                       const uint32_t *placed, const uint32_t *placed1,
+                                                       const uint8_t *l0pay, uint64_t j0, uint64_t j1, int P,
+                                                       uint8_t *sides, uint32_t *err) {
   const uint64_t j = j0 + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (j >= j1) return;
-  const uint32_t pl = placed[j];
-  if (!pl) return;
-  const uint32_t np0 = pl & 0xFFFFu, np1 = pl >> 16;
+  const uint32_t np0 = placed[j], np1 = placed1[j];
+  if (!(np0 | np1)) return;
   const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
   const uint8_t *src = l0pay + sb_off[j];
   bool bad = false;
@@ -380,11 +380,11 @@ void launch_place_sides(const MphfView<KeyT> &m, const KeyT *kept, const KeyT *d
 }
 
 void launch_place_l0(const BBView &bb, const uint64_t *dist_off, const uint64_t *sb_off, const uint32_t *placed,
-                     const uint8_t *l0pay, uint64_t j0, uint64_t j1, int P, uint8_t *sides, uint32_t *err,
-                     cudaStream_t s) {
+                     const uint32_t *placed1, const uint8_t *l0pay, uint64_t j0, uint64_t j1, int P, uint8_t *sides,
+                     uint32_t *err, cudaStream_t s) {
   if (j1 <= j0) return;
-  place_l0_kernel<<<(unsigned)ceil_div((j1 - j0) * 32, 256), 256, 0, s>>>(bb, dist_off, sb_off, placed, l0pay, j0, j1,
-                                                                          P, sides, err);
+  place_l0_kernel<<<(unsigned)ceil_div((j1 - j0) * 32, 256), 256, 0, s>>>(bb, dist_off, sb_off, placed, placed1, l0pay,
+                                                                          j0, j1, P, sides, err);
   CF1_LAUNCH_CHECK();
 }
 

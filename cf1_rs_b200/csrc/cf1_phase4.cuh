@@ -39,13 +39,13 @@ void launch_place_sides(const MphfView<KeyT> &m, const KeyT *kept, const KeyT *d
 // (Level0Out with payloads): the keys level 0 places in sub-bucket j have
 // the consecutive slots from its level-0 slice's first rank on, those level
 // 1 places the ones from its level-1 slice's first rank on, and their bytes
-// wait in rank order at l0pay[sb_off[j] ...] (level 0's placed[j] & 0xFFFF,
-// then level 1's placed[j] >> 16) -- two contiguous copies each; the keys
+// wait in rank order at l0pay[sb_off[j] ...] (level 0's placed[j], then
+// level 1's placed1[j]) -- two contiguous copies each; the keys
 // level 1 left (bin b's at surv[surv_off[b] ...], surv_cnt[b] of them, bytes
 // beside them) walk the levels from 2.  Sub-buckets [j0, j1), bins [b0, b1).
 void launch_place_l0(const BBView &bb, const uint64_t *dist_off, const uint64_t *sb_off, const uint32_t *placed,
-                     const uint8_t *l0pay, uint64_t j0, uint64_t j1, int P, uint8_t *sides, uint32_t *err,
-                     cudaStream_t s);
+                     const uint32_t *placed1, const uint8_t *l0pay, uint64_t j0, uint64_t j1, int P, uint8_t *sides,
+                     uint32_t *err, cudaStream_t s);
 void launch_place_surv(const BBView &bb, const uint64_t *dist_off, const uint64_t *surv, const uint8_t *surv_pay,
                        const uint64_t *surv_off, const unsigned long long *surv_cnt, uint32_t b0, uint32_t b1,
                        uint8_t *sides, uint32_t *err, cudaStream_t s);

@@ -567,10 +567,12 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     l0.surv_off = room_off;
     l0.surv_cnt = scnt;
     l0.err = &sm->l0_err;
-    if (join3) {  // joined side sets: level 0 places its keys' bytes by rank (see Level0Out)
+    uint32_t *placed = c->d_l0placed.get<uint32_t>(2 * (((uint64_t)B << P) + 1));
+    l0.placed = placed;
+    l0.placed1 = placed + ((uint64_t)B << P) + 1;
+    if (join3) {  // joined side sets: levels 0 and 1 place their keys' bytes by rank (see Level0Out)
       l0.with_pay = true;
       l0.surv_pay = c->d_l0survpay.get<uint8_t>(l0_room + 1);
-      l0.placed = c->d_l0placed.get<uint32_t>(((uint64_t)B << P) + 1);
     }
   }
   // The BBHash form leaves the distinct keys in their sub-buckets (kept):
@@ -624,9 +626,9 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     be.li.build(dist, dist_off, B, k, c->learned, s);
     be.bb.build(dist, dist_off, B, be.li.fallback_sel(), s, keys, ws1, NO + 1);
   } else if (l0_ready) {
-    be.bb.build_from_levels01(B, P, l0.woff, l0_words, l0.woff1, l1_words, reinterpret_cast<const KeyT *>(l0.surv),
-                              l0.surv_off, reinterpret_cast<const uint64_t *>(l0.surv_cnt), l0_room, s, twin,
-                              twin + half, half);
+    be.bb.build_from_levels01(B, P, l0.woff, l0_words, l0.placed, l0.woff1, l1_words, l0.placed1,
+                              reinterpret_cast<const KeyT *>(l0.surv), l0.surv_off,
+                              reinterpret_cast<const uint64_t *>(l0.surv_cnt), l0_room, s, twin, twin + half, half);
   } else {
     be.bb.build(dist, dist_off, B, nullptr, s, keys, ws1, NO + 1);
   }
@@ -652,8 +654,8 @@ void run_impl(cf1gpu_ctx *c, StreamIO *io = nullptr, Step step = Step::FULL, con
     uint8_t *sb = reinterpret_cast<uint8_t *>(sides);
     const uint64_t *sbo = be.msd.sb_off.template as<const uint64_t>();
     if (joined_l0) {
-      launch_place_l0(be.bb.view(), dist_off, sbo, l0.placed, l0pay, (uint64_t)b0 << P, (uint64_t)b1 << P, P, sb,
-                      &sm->err, s);
+      launch_place_l0(be.bb.view(), dist_off, sbo, l0.placed, l0.placed1, l0pay, (uint64_t)b0 << P,
+                      (uint64_t)b1 << P, P, sb, &sm->err, s);
       launch_place_surv(be.bb.view(), dist_off, reinterpret_cast<const uint64_t *>(l0.surv), l0.surv_pay, l0.surv_off,
                         l0.surv_cnt, b0, b1, sb, &sm->err, s);
     } else {
