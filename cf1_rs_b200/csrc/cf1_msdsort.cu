@@ -908,22 +908,54 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
         m.pw[lane + 32] = (uint16_t)(t0 + i1 - c1);
         l0.AR[first + lane + 32] = make_ulonglong2(f1, (unsigned long long)(t0 + i1 - c1));
       }
-      // 4. level 1: each key level 0 leaves marks its bit in the sub-bucket's
-      //    level-1 slice (sw1 words, its bit from level 1's hash)
+      // 4. each key level 0 places: its byte to its rank, its slot emptied;
+      //    each key it leaves marks its bit in the sub-bucket's level-1 slice
+      //    (sw1 words, its bit from level 1's hash) and is moved to the front
+      //    of ins / dp (nsv of them; a key's new index is never above its old
+      //    one, and the warp reads a group before it writes it)
       const uint32_t sw1 = (uint32_t)((l0.woff1[bin + 1] - l0.woff1[bin]) >> P);
       const uint64_t first1 = l0.woff1[bin] + (uint64_t)sub * sw1;
       const bool l1ok = sw1 <= WD_SW1MAX;  // always: level 1 is sized from level 0
       if (lane < sw1 && l1ok) m.set1[lane] = m.col1[lane] = 0;
       __syncwarp();
-      for (uint32_t r = lane; r < d && l1ok; r += 32) {
-        const unsigned long long key = m.tab[m.ins[r]];
-        const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
-        if (bpos >= (uint64_t)sw * 64 || !((m.col[bpos >> 6] >> (bpos & 63)) & 1)) continue;  // placed at level 0
-        const uint32_t p1 = bb_slice_pos(key, 1, sw1);
-        const unsigned long long bit = 1ull << (p1 & 63);
-        if (atomicOr(&m.set1[p1 >> 6], bit) & bit) atomicOr(&m.col1[p1 >> 6], bit);
+      uint32_t nsv = 0;
+      for (uint32_t r0 = 0; r0 < d; r0 += 32) {
+        const uint32_t r = r0 + lane;
+        bool lv = false;  // left by level 0
+        uint32_t h = 0;
+        uint8_t pr = 0;
+        if (r < d) {
+          h = m.ins[r];
+          pr = m.dp[r];
+          const unsigned long long key = m.tab[h];
+          const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
+          if (bpos < (uint64_t)sw * 64) {
+            const unsigned long long fin = m.set[bpos >> 6] & ~m.col[bpos >> 6], bit = 1ull << (bpos & 63);
+            if (fin & bit) {
+              if (lpay) l0.l0pay[a + m.pw[bpos >> 6] + (uint32_t)__popcll(fin & (bit - 1))] = pr;
+              m.tab[h] = EMPTY;
+            } else if (l1ok) {
+              lv = true;
+              const uint32_t p1 = bb_slice_pos(key, 1, sw1);
+              const unsigned long long bit1 = 1ull << (p1 & 63);
+              if (atomicOr(&m.set1[p1 >> 6], bit1) & bit1) atomicOr(&m.col1[p1 >> 6], bit1);
+            } else {
+              m.tab[h] = EMPTY;
+            }
+          } else {
+            m.tab[h] = EMPTY;
+          }
+        }
+        const unsigned lb = __ballot_sync(FULL, lv);
+        __syncwarp();  // every lane's reads of this group before any lane's writes
+        if (lv) {
+          const uint32_t k = nsv + __popc(lb & lt);
+          m.ins[k] = (uint16_t)h;
+          m.dp[k] = pr;
+        }
+        nsv += __popc(lb);
+        __syncwarp();
       }
-      __syncwarp();
       const unsigned long long g1 = (lane < sw1 && l1ok) ? m.set1[lane] & ~m.col1[lane] : 0ull;
       const uint32_t e1 = (uint32_t)__popcll(g1), k1 = warp_inclusive_scan(e1);
       const uint32_t placed1 = __shfl_sync(FULL, k1, 31);
@@ -937,7 +969,7 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
       }
       // survivors of level 1: one reservation in the bin's list
       unsigned long long sbase = 0;
-      const uint32_t nsurv = d - placed - placed1;
+      const uint32_t nsurv = nsv - placed1;
       if (lane == 0 && (nsurv || !l1ok)) {
         if (l1ok) sbase = atomicAdd(&l0.surv_cnt[bin], (unsigned long long)nsurv);
         if (!l1ok || sbase + nsurv > l0.surv_off[bin + 1] - l0.surv_off[bin]) {
@@ -947,38 +979,30 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
       }
       sbase = __shfl_sync(FULL, sbase, 0);
       __syncwarp();
-      // 5. each key: its byte to its rank (level 0, then level 1) or the key
-      //    to level 2; the set emptied
+      // 5. each key level 0 left: its byte to its level-1 rank or the key to
+      //    level 2; the rest of the set emptied
       uint64_t so = l0.surv_off[bin] + sbase;
-      for (uint32_t r0 = 0; r0 < d; r0 += 32) {
-        const uint32_t r = r0 + lane;
+      for (uint32_t k0 = 0; k0 < nsv; k0 += 32) {
+        const uint32_t k = k0 + lane;
         bool surv = false;
         unsigned long long key = 0;
-        if (r < d) {
-          const uint32_t h = m.ins[r];
+        if (k < nsv) {
+          const uint32_t h = m.ins[k];
           key = m.tab[h];
           m.tab[h] = EMPTY;
-          const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
-          if (bpos < (uint64_t)sw * 64 && l1ok) {
-            const unsigned long long fin = m.set[bpos >> 6] & ~m.col[bpos >> 6], bit = 1ull << (bpos & 63);
-            if (fin & bit) {
-              if (lpay) l0.l0pay[a + m.pw[bpos >> 6] + (uint32_t)__popcll(fin & (bit - 1))] = m.dp[r];
-            } else {
-              const uint32_t p1 = bb_slice_pos(key, 1, sw1);
-              const unsigned long long fin1 = m.set1[p1 >> 6] & ~m.col1[p1 >> 6], bit1 = 1ull << (p1 & 63);
-              if (fin1 & bit1) {
-                if (lpay) l0.l0pay[a + placed + m.pw1[p1 >> 6] + (uint32_t)__popcll(fin1 & (bit1 - 1))] = m.dp[r];
-              } else {
-                surv = true;
-              }
-            }
+          const uint32_t p1 = bb_slice_pos(key, 1, sw1);
+          const unsigned long long fin1 = m.set1[p1 >> 6] & ~m.col1[p1 >> 6], bit1 = 1ull << (p1 & 63);
+          if (fin1 & bit1) {
+            if (lpay) l0.l0pay[a + placed + m.pw1[p1 >> 6] + (uint32_t)__popcll(fin1 & (bit1 - 1))] = m.dp[k];
+          } else {
+            surv = true;
           }
         }
         const unsigned sb = __ballot_sync(FULL, surv);
         if (surv && sbase != ~0ull) {
           const uint64_t at = so + __popc(sb & lt);
           l0.surv[at] = key;
-          if (lpay) l0.surv_pay[at] = m.dp[r];
+          if (lpay) l0.surv_pay[at] = m.dp[k];
         }
         so += __popc(sb);
       }
