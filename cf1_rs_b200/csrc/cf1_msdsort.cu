@@ -152,15 +152,16 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
       whist[w * DIG + d] = run;
       run += v;
     }
-    if (DIG == MS_BLOCK) tot_d = run;
+    if (DIG <= MS_BLOCK) tot_d = run;
     else lstart[d] = run;
   }
   __syncthreads();
-  // tile-local start of each digit: exclusive scan over digits
-  if (DIG == MS_BLOCK) {
+  // tile-local start of each digit: exclusive scan over digits (one digit a
+  // thread; the threads past the digits add nothing)
+  if (DIG <= MS_BLOCK) {
     uint32_t tot;
     uint32_t pre = block_exclusive_scan<MS_BLOCK>(tot_d, sm, tot);
-    lstart[tid] = pre;
+    if (tid < DIG) lstart[tid] = pre;
   } else if (tid == 0) {
     uint32_t run = 0;
     for (uint32_t d = 0; d < DIG; d++) {
