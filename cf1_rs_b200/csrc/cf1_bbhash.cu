@@ -160,20 +160,14 @@ __global__ void bb_meta_kernel(const uint64_t *woff, const uint64_t *R, uint64_t
 // A sliced level (levels 0 and 1 of the phase-3 dedup): each entry holds
 // {placed bits, placed bits of its slice before it}; R = the exclusive scan
 // of the slices' placed counts over the whole level (slices of bin b are
-// [b << P, (b + 1) << P)).  One warp per slice adds the slice's level-wide
-// start to its entries' ranks.
-__global__ void bb_slice_rank_kernel(ulonglong2 *AR, const uint64_t *woff, const uint64_t *R, int P, uint64_t nsub) {
-  const uint64_t j = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (j >= nsub) return;
-  const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
-  const uint32_t sw = (uint32_t)((woff[bin + 1] - woff[bin]) >> P);
-  const uint64_t first = woff[bin] + (uint64_t)sub * sw, r0 = R[j];
-  for (uint32_t w = lane_id(); w < sw; w += 32) AR[first + w].y += r0;
+// [b << P, (b + 1) << P)).  srank[j] = the placed keys of slice j's bin
+// before slice j; the bin's metadata takes the keys earlier levels placed as
+// its rank adjustment.
+__global__ void bb_srank_kernel(const uint64_t *R, int P, uint64_t nsub, uint32_t *srank) {
+  const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < nsub) srank[j] = (uint32_t)(R[j] - R[(j >> P) << P]);
 }
 
-// Metadata of a sliced level from the slices' scanned counts (as
-// bb_meta_kernel, with the level's rank at the bin's first and last word
-// read at the bin's first slice and one past its last).
 __global__ void bb_meta_sliced_kernel(const uint64_t *woff, const uint64_t *R, int P, uint64_t level_base,
                                       uint64_t *base, BBMeta *meta, uint32_t nbins) {
   uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -182,7 +176,7 @@ __global__ void bb_meta_sliced_kernel(const uint64_t *woff, const uint64_t *R, i
   BBMeta m;
   m.word_off = level_base + woff[b];
   m.nwords = (uint32_t)(woff[b + 1] - woff[b]);
-  m.rank_adj = (uint32_t)(base[b] - r0);
+  m.rank_adj = (uint32_t)base[b];
   meta[b] = m;
   base[b] += r1 - r0;
 }
@@ -236,6 +230,7 @@ void BBHashBuild<KeyT>::clear() {
   levels = 0;
   bytes = 0;
   l1_slice_bits = -1;
+  srank_words = 0;
 }
 
 template <class KeyT>
@@ -368,10 +363,9 @@ template <class KeyT>
 void BBHashBuild<KeyT>::finish_sliced(uint32_t l, const uint64_t *woff, const uint32_t *placed, int P,
                                       cudaStream_t s) {
   const uint64_t nsub = (uint64_t)nbins << P;
-  ulonglong2 *Al = ar_.as<ulonglong2>() + total_words;
   uint64_t *R = rtmp_.get<uint64_t>(nsub + 1);
   exclusive_scan_u32(placed, R, nsub, scan_tmp_, s);
-  bb_slice_rank_kernel<<<(unsigned)ceil_div(nsub * 32, 256), 256, 0, s>>>(Al, woff, R, P, nsub);
+  bb_srank_kernel<<<(unsigned)ceil_div(nsub, 256), 256, 0, s>>>(R, P, nsub, srank_[l].get<uint32_t>(nsub + 1));
   CF1_LAUNCH_CHECK();
   bb_meta_sliced_kernel<<<(unsigned)ceil_div(nbins, 256), 256, 0, s>>>(
       woff, R, P, total_words, base_.as<uint64_t>(), meta_.as<BBMeta>() + (size_t)l * nbins, nbins);
@@ -394,12 +388,13 @@ void BBHashBuild<KeyT>::build_from_levels01(uint32_t nb, int P, const uint64_t *
   finish_sliced(1, woff1, placed1, P, s);
   total_words += words1;
   l1_slice_bits = P;
+  srank_words = (uint64_t)nbins << P;
   CF1_CUDA(cudaMemcpyAsync(cnt_[0].as<uint64_t>(), surv_cnt, nbins * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
   KeyT *r0 = (ws0 && ws_cap >= surv_total + 1) ? ws0 : rem_[0].get<KeyT>(surv_total + 1);
   KeyT *r1 = (ws1 && ws_cap >= surv_total + 1) ? ws1 : rem_[1].get<KeyT>(surv_total + 1);
   run_levels(2, surv, surv_off, r0, r1, s);  // level l reads cnt_[l & 1] and writes r[l & 1]
   levels = std::max<uint32_t>(levels, 2);
-  bytes = total_words * sizeof(ulonglong2) + (size_t)levels * nbins * sizeof(BBMeta);
+  bytes = total_words * sizeof(ulonglong2) + (size_t)levels * nbins * sizeof(BBMeta) + 2 * srank_words * sizeof(uint32_t);
 }
 
 template <class KeyT>
@@ -411,6 +406,8 @@ BBView BBHashBuild<KeyT>::view() const {
   v.nbins = nbins;
   v.l1_slice_bits = l1_slice_bits;
   v.pad = 0;
+  v.srank[0] = l1_slice_bits >= 0 ? srank_[0].as<const uint32_t>() : nullptr;
+  v.srank[1] = l1_slice_bits >= 0 ? srank_[1].as<const uint32_t>() : nullptr;
   return v;
 }
 

@@ -12,6 +12,7 @@ struct BBHashBuild {
   uint32_t levels = 0, nbins = 0;
   uint64_t bytes = 0;
   int l1_slice_bits = -1;          // see BBView
+  uint64_t srank_words = 0;        // entries of each sliced level's srank table
 
   BBHashBuild() = default;
   BBHashBuild(const BBHashBuild &) = delete;
@@ -43,6 +44,8 @@ struct BBHashBuild {
   const BBMeta *meta_device() const { return meta_.as<const BBMeta>(); }
   // {bit word, level rank} entries of all levels (total_words of them)
   const ulonglong2 *entries_device() const { return ar_.as<const ulonglong2>(); }
+  // per-slice start ranks of sliced level l (srank_words of them)
+  const uint32_t *srank_device(int l) const { return srank_[l].as<const uint32_t>(); }
 
  private:
   // Grows the entry array to hold `words` entries, keeping the first `keep`.
@@ -54,7 +57,7 @@ struct BBHashBuild {
 
   // The entry array and the level buffers are kept across builds and grown on
   // demand, so a rebuild allocates nothing once sizes settle.
-  DevBuf ar_, meta_, base_, rem_[2], cnt_[2], tot_, tile_off_, wcnt_, woff_, pc_, rtmp_, scan_tmp_;
+  DevBuf ar_, meta_, base_, rem_[2], cnt_[2], tot_, tile_off_, wcnt_, woff_, pc_, rtmp_, scan_tmp_, srank_[2];
 };
 
 }  // namespace cf1

@@ -5,11 +5,12 @@
 // The image holds everything a query needs: the bucket -> bin table, the
 // per-bin slot offsets, the BBHash levels and, in learned mode, the roots,
 // leaves and the sorted distinct keys.  The query code is the device code
-// (cf1_mphf.cuh), compiled for the host.  Image layout version 4: the BBHash
+// (cf1_mphf.cuh), compiled for the host.  Image layout version 5: the BBHash
 // levels are one array of 16-byte {bit word, level rank} entries addressed
 // through the 16-byte per-(level, bin) metadata, so the image and every
-// section in it start on a 16-byte boundary; the header says whether level 1
-// is sliced (and on how many bits).
+// section in it start on a 16-byte boundary; the header says whether levels 0
+// and 1 are sliced (and on how many bits), whose per-slice start ranks follow
+// the entries.
 #include <cstring>
 #include <vector>
 
@@ -29,9 +30,10 @@ struct ImageHeader {
   int32_t l1_slice_bits;  // BBView::l1_slice_bits
   uint64_t n_distinct, n_leaves;
   uint64_t lut_off, dist_off_off, meta_off, ar_off, ar_words, roots_off, leaves_off, keys_off, total;
+  uint64_t srank_off, srank_words;  // sliced levels 0 and 1: their per-slice start ranks, one table each
 };
 
-constexpr uint32_t IMAGE_VERSION = 4;
+constexpr uint32_t IMAGE_VERSION = 5;
 inline uint64_t align16(uint64_t x) { return (x + 15) & ~15ull; }  // sections are 16-byte aligned
 
 template <class KeyT>
@@ -63,6 +65,9 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   h.ar_off = off;
   h.ar_words = be.bb.total_words;
   off = align16(off + h.ar_words * sizeof(ulonglong2));
+  h.srank_off = off;
+  h.srank_words = h.l1_slice_bits >= 0 ? be.bb.srank_words : 0;
+  off = align16(off + 2 * h.srank_words * sizeof(uint32_t));
   h.roots_off = off;
   off = align16(off + (learned ? B * sizeof(LIRoot) : 0));
   h.leaves_off = off;
@@ -84,6 +89,9 @@ size_t export_impl(cf1gpu_ctx *c, void *dst, size_t cap) {
   if (h.ar_words)
     CF1_CUDA(cudaMemcpyAsync(d + h.ar_off, be.bb.entries_device(), h.ar_words * sizeof(ulonglong2),
                              cudaMemcpyDeviceToHost, s));
+  for (int l = 0; l < 2 && h.srank_words; l++)
+    CF1_CUDA(cudaMemcpyAsync(d + h.srank_off + l * h.srank_words * sizeof(uint32_t), be.bb.srank_device(l),
+                             h.srank_words * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   if (learned) {
     CF1_CUDA(cudaMemcpyAsync(d + h.roots_off, be.li.roots_device(), B * sizeof(LIRoot), cudaMemcpyDeviceToHost, s));
     CF1_CUDA(cudaMemcpyAsync(d + h.leaves_off, be.li.leaves_device(), nleaves * sizeof(LILeaf), cudaMemcpyDeviceToHost, s));
@@ -104,6 +112,8 @@ void host_query_impl(const ImageHeader &h, const char *img, const uint64_t *keys
   v.bb.nbins = h.nbins;
   v.bb.l1_slice_bits = h.l1_slice_bits;
   v.bb.pad = 0;
+  v.bb.srank[0] = reinterpret_cast<const uint32_t *>(img + h.srank_off);
+  v.bb.srank[1] = v.bb.srank[0] + h.srank_words;
   v.li.roots = reinterpret_cast<const LIRoot *>(img + h.roots_off);
   v.li.leaves = reinterpret_cast<const LILeaf *>(img + h.leaves_off);
   v.li.k = (int)h.k;

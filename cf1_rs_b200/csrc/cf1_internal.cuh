@@ -199,12 +199,18 @@ struct BBView {
   const ulonglong2 *AR;  // {cleaned bit word, level rank}, levels back to back
   const BBMeta *meta;    // [levels * nbins]
   uint32_t levels, nbins;
-  // >= 0: level 1 is sliced like level 0 (built by the phase-3 dedup): a
-  // bin's level-1 block is 2^l1_slice_bits slices of equal size, and a key's
-  // bit lies in the slice its level-0 hash's top l1_slice_bits bits name;
-  // -1: level 1 hashes over its bin's whole block like the later levels
+  // >= 0: levels 0 and 1 were built by the phase-3 dedup, one slice per
+  // sub-bucket: a bin's block of either level is 2^l1_slice_bits slices of
+  // equal size, and a key's bit lies in the slice its level-0 hash's top
+  // l1_slice_bits bits name (level 0's bit is its hash scaled to the block,
+  // level 1's its own hash scaled to the slice).  Their entries' rank halves
+  // count the placed bits of the slice before the word, srank[l][slice] the
+  // placed bits of the bin's slices before it, and a bin's rank_adj is the
+  // keys its earlier levels placed.  -1: every level hashes over its bin's
+  // whole block and the entries hold level-wide ranks.
   int32_t l1_slice_bits;
   uint32_t pad;
+  const uint32_t *srank[2];  // [nbins << l1_slice_bits] each, when sliced
 };
 
 constexpr int LI_HIDDEN = 16;

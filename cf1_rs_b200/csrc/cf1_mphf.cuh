@@ -72,13 +72,17 @@ CF1_HD uint32_t bb_slice_pos(uint64_t H, uint32_t l, uint32_t sw) {
   return (uint32_t)(((uint64_t)t * sw) >> 26);
 }
 
-// Bit of a key at a sliced level l of nwords words in 2^P slices: the slice
-// is the top P bits of the level-0 hash (the key's phase-3 sub-bucket), the
-// bit inside it level l's own hash.
+// Slice of a key among 2^P: the top P bits of its level-0 hash (its phase-3
+// sub-bucket).
+CF1_HD uint64_t bb_slice(uint64_t H, int P) {
+  return P ? (uint64_t)((uint32_t)((H * KEY_SPREAD_MUL) >> 32) >> (32 - P)) : 0;
+}
+
+// Bit of a key at a sliced level l of nwords words in 2^P slices: its slice,
+// and the bit inside it from level l's own hash.
 CF1_HD uint64_t bb_pos_sliced(uint64_t H, uint32_t l, uint32_t nwords, int P) {
   const uint32_t sw = nwords >> P;
-  const uint64_t sub = P ? (uint64_t)((uint32_t)((H * KEY_SPREAD_MUL) >> 32) >> (32 - P)) : 0;
-  return sub * 64 * sw + bb_slice_pos(H, l, sw);
+  return bb_slice(H, P) * 64 * sw + bb_slice_pos(H, l, sw);
 }
 
 // Levels [l0, l1) of a key's walk (hash H): the first level whose bit is set
@@ -87,11 +91,16 @@ CF1_HD uint64_t bb_walk(const BBView &v, uint32_t bin, uint64_t H, uint32_t l0, 
   for (uint32_t l = l0; l < l1; l++) {
     const BBMeta mt = v.meta[(uint64_t)l * v.nbins + bin];
     if (mt.nwords == 0) return SLOT_NONE;
-    const uint64_t pos = (l == 1 && v.l1_slice_bits >= 0) ? bb_pos_sliced(H, 1, mt.nwords, v.l1_slice_bits)
-                                                         : bb_pos(H, l, mt.nwords);
+    const bool sliced = l < 2 && v.l1_slice_bits >= 0;
+    const uint64_t pos = (sliced && l == 1) ? bb_pos_sliced(H, 1, mt.nwords, v.l1_slice_bits) : bb_pos(H, l, mt.nwords);
     const ulonglong2 e = v.AR[mt.word_off + (pos >> 6)];
     const uint32_t bit = (uint32_t)(pos & 63);
-    if ((e.x >> bit) & 1) return (uint32_t)(mt.rank_adj + (uint32_t)e.y + (uint32_t)popc64(e.x & ((1ull << bit) - 1)));
+    if ((e.x >> bit) & 1) {
+      uint32_t r = mt.rank_adj + (uint32_t)e.y + (uint32_t)popc64(e.x & ((1ull << bit) - 1));
+      if (sliced)  // the placed keys of the bin's slices before this one
+        r += v.srank[l][((uint64_t)bin << v.l1_slice_bits) + bb_slice(H, v.l1_slice_bits)];
+      return r;
+    }
   }
   return SLOT_NONE;
 }

@@ -214,9 +214,12 @@ __global__ void __launch_bounds__(256) place_sides_kernel(MphfView<KeyT> m, cons
         const uint32_t i = i0 + u * 32 + lane;
         if (i >= c) continue;
         uint64_t local;
-        if ((e[u].x >> bit[u]) & 1)
+        if ((e[u].x >> bit[u]) & 1) {
           local = (uint32_t)(m0.rank_adj + (uint32_t)e[u].y + (uint32_t)popc64(e[u].x & ((1ull << bit[u]) - 1)));
-        else
+          if (m.bb.l1_slice_bits >= 0)  // sliced levels: the bin's slices before this one
+            local = (uint32_t)(local + m.bb.srank[0][((uint64_t)bin << m.bb.l1_slice_bits) +
+                                                     bb_slice(H[u], m.bb.l1_slice_bits)]);
+        } else
           local = m0.nwords ? bb_walk(m.bb, bin, H[u], 1, m.bb.levels) : SLOT_NONE;
         const uint64_t slot = local == SLOT_NONE ? SLOT_NONE : base + local;
         if (slot < end && slot >= base) sides[slot] = pay[u];
@@ -238,24 +241,26 @@ __global__ void __launch_bounds__(256) place_l0_kernel(BBView bb, const uint64_t
   if (j >= j1) return;
   const uint32_t np0 = placed[j], np1 = placed1[j];
   if (!(np0 | np1)) return;
-  const uint32_t bin = (uint32_t)(j >> P), sub = (uint32_t)(j & ((1ull << P) - 1));
+  const uint32_t bin = (uint32_t)(j >> P);
   const uint8_t *src = l0pay + sb_off[j];
   bool bad = false;
-  if (np0) {
-    const BBMeta m0 = bb.meta[bin];
-    const uint64_t first = m0.word_off + (uint64_t)sub * (m0.nwords >> P);
-    const uint64_t base = dist_off[bin] + (uint32_t)(m0.rank_adj + (uint32_t)bb.AR[first].y);
-    if (base + np0 > dist_off[bin + 1]) bad = true;
-    else
-      for (uint32_t r = lane_id(); r < np0; r += 32) sides[base + r] = src[r];
-  }
-  if (np1) {
-    const BBMeta m1 = bb.meta[bb.nbins + bin];
-    const uint64_t first = m1.word_off + (uint64_t)sub * (m1.nwords >> P);
-    const uint64_t base = dist_off[bin] + (uint32_t)(m1.rank_adj + (uint32_t)bb.AR[first].y);
-    if (base + np1 > dist_off[bin + 1] || bb.levels < 2) bad = true;
-    else
-      for (uint32_t r = lane_id(); r < np1; r += 32) sides[base + r] = src[np0 + r];
+  if (bb.l1_slice_bits != P || bb.levels < 2) {
+    bad = true;
+  } else {
+    // a slice's first slot: the bin's slots, the keys earlier levels placed,
+    // the placed keys of the bin's slices before it
+    if (np0) {
+      const uint64_t base = dist_off[bin] + (uint32_t)(bb.meta[bin].rank_adj + bb.srank[0][j]);
+      if (base + np0 > dist_off[bin + 1]) bad = true;
+      else
+        for (uint32_t r = lane_id(); r < np0; r += 32) sides[base + r] = src[r];
+    }
+    if (np1) {
+      const uint64_t base = dist_off[bin] + (uint32_t)(bb.meta[bb.nbins + bin].rank_adj + bb.srank[1][j]);
+      if (base + np1 > dist_off[bin + 1]) bad = true;
+      else
+        for (uint32_t r = lane_id(); r < np1; r += 32) sides[base + r] = src[np0 + r];
+    }
   }
   if (bad && lane_id() == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
 }
