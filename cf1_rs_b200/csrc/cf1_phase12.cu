@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
     const uint32_t p0 = tid * ITEMS;
     uint32_t zv[ITEMS];
     uint32_t prev = SK_INVALID;
-    uint32_t *starts;  // segment starts, once the windows are taken
+    uint32_t *starts;     // segment starts, once the windows are taken
+    const uint32_t *zrow;  // window minima by position (read at segment starts)
     if constexpr (KC != 0) {
       // k, m, w fixed: each thread rolls the m-mers of its ITEMS positions
       // (one extraction, then one base each) and takes its windows' minima
@@ -185,6 +186,7 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
         prev = min(am1, min(S, mid0));
       }
       starts = bufB;
+      zrow = bufA;  // written at the segment starts after the scan below
     } else {
       for (uint32_t q = tid; q < nm; q += BLOCK) {
         uint32_t fw = (uint32_t)KOps<uint64_t>::extract(a.W, P0 + q, m);
@@ -210,6 +212,7 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
       __syncthreads();
       const uint32_t *z = dst;
       starts = src;  // free now: segment starts
+      zrow = z;
       prev = p0 > 0 && p0 <= nk ? z[p0 - 1] : SK_INVALID;
 #pragma unroll
       for (int i = 0; i < ITEMS; i++) zv[i] = p0 + i < nk ? z[p0 + i] : SK_INVALID;
@@ -228,32 +231,37 @@ __global__ void __launch_bounds__(BLOCK) superkmer_kernel(SuperkmerArgs a) {
     uint32_t tot;
     const uint32_t pre = block_exclusive_scan<BLOCK>((nb << 16) | nv, sm, tot);
     const uint32_t nseg = tot >> 16, nrec = tot & 0xFFFFu;
-    uint32_t seg = pre >> 16;
+    // starts[s] = the segment's first position | its record number << 16
+    // (0xFFFF: its window holds a placeholder, no record); then one thread
+    // per segment writes the records, so the per-record work runs on full
+    // warps instead of on the ~1 lane in 9 whose item starts a segment
+    uint32_t seg = pre >> 16, vi = pre & 0xFFFFu;
 #pragma unroll
     for (int i = 0; i < ITEMS; i++)
-      if ((bflags >> i) & 1) starts[seg++] = p0 + i;
+      if ((bflags >> i) & 1) {
+        const bool valid = zv[i] != SK_INVALID;
+        starts[seg++] = (p0 + i) | ((valid ? vi : 0xFFFFu) << 16);
+        if constexpr (KC != 0)
+          if (valid) bufA[p0 + i] = zv[i];
+        vi += valid;
+      }
     if (tid == 0) {
       starts[nseg] = nk;
       s_base = nrec ? atomicAdd(a.rec_count, (unsigned long long)nrec) : 0;
     }
     __syncthreads();
-    uint64_t o = s_base + (pre & 0xFFFFu);
-    seg = pre >> 16;
-#pragma unroll
-    for (int i = 0; i < ITEMS; i++) {
-      if (!((bflags >> i) & 1)) continue;
-      const uint32_t e = starts[seg + 1];
-      seg++;
-      if (zv[i] == SK_INVALID) continue;
-      const uint32_t n = e - (p0 + i);
-      const uint32_t bk = mix_bucket(mix_order_inv(zv[i]));
+    for (uint32_t sg = tid; sg < nseg; sg += BLOCK) {
+      const uint32_t st = starts[sg], rn = st >> 16;
+      if (rn == 0xFFFFu) continue;
+      const uint32_t p = st & 0xFFFFu, n = (starts[sg + 1] & 0xFFFFu) - p;
+      const uint32_t bk = mix_bucket(mix_order_inv(zrow[p]));
       atomicAdd(&a.hist[bk], 1u);
       my_kmers += n;
+      const uint64_t o = s_base + rn;
       if (o < a.rec_cap) {
-        a.rec_tmp[o] = rec_pack(P0 + p0 + i, n, 0);
+        a.rec_tmp[o] = rec_pack(P0 + p, n, 0);
         a.rec_bucket[o] = (uint16_t)bk;
       }
-      o++;
     }
     __syncthreads();
     if (!a.tile_counter) break;
