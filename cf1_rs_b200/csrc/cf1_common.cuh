@@ -372,22 +372,31 @@ CF1_HD uint32_t contribution(KeyT fw, KeyT rcv, bool has_prev, uint32_t prev, bo
 }
 
 // sideset_lookup(contribution(...)) computed directly: the side-set byte of
-// one occurrence (front nibble low, back nibble high; M = 0xF).
+// one occurrence (front nibble low, back nibble high; M = 0xF).  This form
+// takes the next k-mer's forward and reverse-complement values (nf, nr: the
+// k-mer rolled by `next`), which a caller walking the sequence has already;
+// with !has_next they are not read.  contribution_sideset rolls them itself.
 template <class KeyT>
-CF1_HD uint32_t contribution_sideset(KeyT fw, KeyT rcv, bool has_prev, uint32_t prev, bool has_next, uint32_t next,
-                                     int k) {
+CF1_HD uint32_t contribution_sideset_rolled(KeyT fw, KeyT rcv, KeyT nf, KeyT nr, bool has_prev, uint32_t prev,
+                                            bool has_next, uint32_t next) {
   const KeyT can = kmin(fw, rcv);
   const bool fwd = fw == can;
   if (!has_prev && !has_next) return 0xFFu;
   const uint32_t cp = side_code(prev), cpc = side_code(3 - prev);
   const uint32_t right = fwd ? (cp | 0xF0u) : (0x0Fu | (cpc << 4));
   if (!has_next) return right;
-  KeyT nf = fw, nr = rcv;
-  KOps<KeyT>::roll(nf, nr, next, k);
   if (kmin(nf, nr) == can) return (!has_prev || nf == fw) ? 0xFFu : right;
   const uint32_t cn = side_code(next), cnc = side_code(3 - next);
   if (!has_prev) return fwd ? (0x0Fu | (cn << 4)) : (cnc | 0xF0u);
   return fwd ? (cp | (cn << 4)) : (cnc | (cpc << 4));
+}
+
+template <class KeyT>
+CF1_HD uint32_t contribution_sideset(KeyT fw, KeyT rcv, bool has_prev, uint32_t prev, bool has_next, uint32_t next,
+                                     int k) {
+  KeyT nf = fw, nr = rcv;
+  KOps<KeyT>::roll(nf, nr, next, k);
+  return contribution_sideset_rolled(fw, rcv, nf, nr, has_prev, prev, has_next, next);
 }
 
 // ------------------------------------------------------------- error flags ----

@@ -101,6 +101,163 @@ __global__ void __launch_bounds__(256) expand_kernel(const uint64_t *records, ui
   }
 }
 
+// Rolling expansion (64-bit keys, k <= 31, with side-set bytes).  A warp
+// takes 32 records, whose keys are consecutive in the output; each round,
+// every lane takes a run of `er` consecutive occurrences of the warp's
+// flattened index space (er <= XR_E, the same for all lanes, so the lanes
+// stay balanced whatever the record lengths).  A lane extracts its run's
+// first k-mer from the packed words once, then rolls forward and backward
+// forms one base at a time (src/kmer.rs:240-262) from a 32-base look-ahead
+// word; when its run crosses into the next record it takes that record's
+// first k-mer, look-ahead and preceding base, prepared once per record by
+// the record's own lane, through shuffles.  The rolled k-mer is also the
+// "next k-mer" the side-set byte needs for its self-loop test.  Keys and
+// bytes are staged per warp in shared memory and written out contiguously.
+constexpr int XR_E = 16;                       // most occurrences a lane takes per round
+constexpr int XR_WARPS = 8;
+constexpr uint32_t XR_SPAN = 32 * XR_E;        // occurrences a warp takes per round at most
+constexpr uint32_t XR_PAD = XR_SPAN + XR_SPAN / 16;
+constexpr uint32_t XR_BPAD = XR_SPAN + XR_SPAN / 4;
+// Staging slots of key i and byte i: a pad word per 16 keys and four pad
+// bytes per 16 bytes, so that the lanes' runs (stride er) fall on different
+// shared-memory banks.
+CF1_D uint32_t xr_slot(uint32_t i) { return i + (i >> 4); }
+CF1_D uint32_t xr_bslot(uint32_t i) { return i + ((i >> 4) << 2); }
+
+// The k-mer starting at base p (k <= 31), the 32 bases after it (p + k ...,
+// most significant first) and, with want_prev, the base before it.  Reads
+// words p/32 .. p/32 + 2, which the packed sequence's padding covers for any
+// p < L.
+CF1_D void xr_window(const uint64_t *W, uint64_t p, int k, bool want_prev, uint64_t &fw, uint64_t &ahead,
+                     uint32_t &prev) {
+  const uint64_t i = p >> 5;
+  const int s = (int)(p & 31) * 2;
+  const uint64_t w0 = W[i], w1 = W[i + 1], w2 = W[i + 2];
+  const uint64_t t0 = s ? ((w0 << s) | (w1 >> (64 - s))) : w0;  // bases p .. p + 31
+  const uint64_t t1 = s ? ((w1 << s) | (w2 >> (64 - s))) : w1;  // bases p + 32 .. p + 63
+  fw = t0 >> (64 - 2 * k);
+  ahead = (t0 << (2 * k)) | (t1 >> (64 - 2 * k));
+  prev = want_prev ? (s ? (uint32_t)(w0 >> (64 - s)) & 3 : (uint32_t)W[i - 1] & 3) : 0u;
+}
+
+__global__ void __launch_bounds__(XR_WARPS * 32) expand_roll_kernel(const uint64_t *records, uint64_t n_rec,
+                                                                    const uint64_t *kpre, const uint64_t *W, int k,
+                                                                    uint64_t *keys, uint64_t n_keys, uint64_t L,
+                                                                    uint32_t *queue, uint32_t *err,
+                                                                    const uint64_t *NM, uint8_t *sides) {
+  __shared__ uint64_t skey[XR_WARPS][XR_PAD];
+  __shared__ uint8_t sside[XR_WARPS][XR_BPAD];
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  uint64_t *sk = skey[warp];
+  uint8_t *ss = sside[warp];
+  const uint64_t n_chunks = ceil_div_dev(n_rec);
+  const uint64_t kmask = KOps<uint64_t>::mask(k);
+  const int top = 2 * k - 2;
+  uint64_t chunk = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (;;) {
+    if (queue) {
+      uint32_t c = 0;
+      if (lane == 0) c = atomicAdd(queue, 1u);
+      chunk = __shfl_sync(FULL, c, 0);
+    }
+    if (chunk >= n_chunks) break;
+    const uint64_t r = chunk * 32 + lane;
+    const bool valid = r < n_rec;
+    const uint64_t rec = valid ? records[r] : 0;
+    const uint32_t n = valid ? rec_n(rec) : 0;
+    const uint64_t pos = rec_pos(rec);
+    const uint64_t out0 = kpre[chunk * 32];  // the chunk's records are consecutive in the key array
+    // a record whose windows leave the input is flagged and its bases are
+    // never read (its keys' slots get zeros)
+    const bool inb = valid && pos + n - 1 + k <= L;
+    if (valid && !inb) atomicOr(err, (uint32_t)DEV_OVERFLOW);
+    uint32_t ends = 0, pb0 = 0;
+    uint64_t fw0 = 0, rc0 = 0, ah0 = 0;
+    if (inb) {
+      const uint64_t q = pos + n - 1;  // the last k-mer
+      ends = (uint32_t)(pos > 0 && !is_n(NM, pos - 1)) | ((uint32_t)(q + k < L && !is_n(NM, q + k)) << 1);
+      xr_window(W, pos, k, ends & 1u, fw0, ah0, pb0);
+      rc0 = KOps<uint64_t>::rc(fw0, k);
+    }
+    // n (13 bits), whether the record has a base before / after (2), the
+    // base before it (2), whether its bases may be read (1)
+    const uint32_t info0 = n | (ends << 16) | (pb0 << 18) | ((uint32_t)inb << 20);
+    const uint32_t incl = warp_inclusive_scan(n);
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    for (uint32_t base = 0; base < total;) {
+      const uint32_t rem = total - base;
+      const uint32_t er = rem >= XR_SPAN ? (uint32_t)XR_E : (rem + 31) / 32;
+      const uint32_t j0 = base + lane * er;
+      // the record holding j0: the number of records ending at or before it
+      int cur = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const uint32_t v = __shfl_sync(FULL, incl, cur + step - 1);
+        if (v <= j0) cur += step;
+      }
+      uint32_t info = __shfl_sync(FULL, info0, cur);
+      uint32_t rec_end = __shfl_sync(FULL, incl, cur);
+      const uint64_t cpos = __shfl_sync(FULL, pos, cur);
+      uint32_t t = j0 - (rec_end - (info & 0x1FFFu));
+      uint64_t fw = 0, rc = 0, ah = 0;
+      uint32_t prevb = 0;
+      if (j0 < total && (info >> 20 & 1u)) {
+        xr_window(W, cpos + t, k, t > 0 || (info >> 16 & 1u), fw, ah, prevb);
+        rc = KOps<uint64_t>::rc(fw, k);
+      }
+      for (uint32_t e = 0; e < er; e++) {
+        const uint32_t j = j0 + e;
+        // the next record's first k-mer, taken when the run crosses into it
+        const int nx = cur < 31 ? cur + 1 : 31;
+        const uint64_t fwN = __shfl_sync(FULL, fw0, nx), rcN = __shfl_sync(FULL, rc0, nx),
+                       ahN = __shfl_sync(FULL, ah0, nx);
+        const uint32_t infoN = __shfl_sync(FULL, info0, nx), endN = __shfl_sync(FULL, incl, nx);
+        if (j == rec_end && j < total) {
+          cur = nx;
+          fw = fwN;
+          rc = rcN;
+          ah = ahN;
+          info = infoN;
+          rec_end = endN;
+          t = 0;
+          prevb = (infoN >> 18) & 3u;
+        }
+        const bool hp = t > 0 || (info >> 16 & 1u);
+        const bool hn = t + 1 < (info & 0x1FFFu) || (info >> 17 & 1u);
+        const uint32_t nb = (uint32_t)(ah >> 62);
+        const uint64_t nf = ((fw << 2) | nb) & kmask;
+        const uint64_t nr = (rc >> 2) | ((uint64_t)(3 - nb) << top);
+        if (j < total) {
+          const uint32_t i = lane * er + e;
+          sk[xr_slot(i)] = kmin(fw, rc);
+          ss[xr_bslot(i)] = (uint8_t)contribution_sideset_rolled(fw, rc, nf, nr, hp, prevb, hn, nb);
+        }
+        prevb = (uint32_t)(fw >> top);  // this k-mer's first base precedes the next one
+        fw = nf;
+        rc = nr;
+        ah <<= 2;
+        t++;
+      }
+      __syncwarp();
+      const uint32_t span = 32 * er;
+      for (uint32_t i = lane; i < span; i += 32) {
+        const uint64_t o = out0 + base + i;
+        if (base + i < total) {
+          if (o < n_keys) {
+            keys[o] = sk[xr_slot(i)];
+            sides[o] = ss[xr_bslot(i)];
+          } else {
+            atomicOr(err, (uint32_t)DEV_OVERFLOW);
+          }
+        }
+      }
+      __syncwarp();
+      base += span;
+    }
+    if (!queue) break;
+  }
+}
+
 // Per tile digit counts, stored segment-major then digit-major so that one
 // exclusive scan over the array yields every (segment, digit, tile) output
 // position: previous segments' sizes + smaller digits of this segment +
@@ -251,6 +408,17 @@ void launch_expand(const uint64_t *records, uint64_t n_rec, const uint64_t *kpre
                    const uint64_t *NM, uint8_t *sides) {
   if (n_rec == 0) return;
   uint64_t warps = ceil_div(n_rec, 32);
+  if constexpr (KOps<KeyT>::WORDS == 1) {
+    if (sides && k <= 31) {
+      unsigned grid = persistent_ctas ? persistent_grid(expand_roll_kernel, XR_WARPS * 32, 0, persistent_ctas,
+                                                        ceil_div(warps, XR_WARPS))
+                                      : (unsigned)ceil_div(warps, XR_WARPS);
+      expand_roll_kernel<<<grid, XR_WARPS * 32, 0, s>>>(records, n_rec, kpre, W, k, keys, n_keys, L,
+                                                        persistent_ctas ? queue : nullptr, err, NM, sides);
+      CF1_LAUNCH_CHECK();
+      return;
+    }
+  }
   unsigned grid = persistent_ctas ? persistent_grid(expand_kernel<KeyT>, 256, 0, persistent_ctas, ceil_div(warps, 8))
                                   : (unsigned)ceil_div(warps, 8);
   expand_kernel<KeyT><<<grid, 256, 0, s>>>(records, n_rec, kpre, W, k, keys, n_keys, L,
