@@ -372,23 +372,33 @@ CF1_HD uint32_t contribution(KeyT fw, KeyT rcv, bool has_prev, uint32_t prev, bo
 }
 
 // sideset_lookup(contribution(...)) computed directly: the side-set byte of
-// one occurrence (front nibble low, back nibble high; M = 0xF).  This form
-// takes the next k-mer's forward and reverse-complement values (nf, nr: the
-// k-mer rolled by `next`), which a caller walking the sequence has already;
-// with !has_next they are not read.  contribution_sideset rolls them itself.
-template <class KeyT>
-CF1_HD uint32_t contribution_sideset_rolled(KeyT fw, KeyT rcv, KeyT nf, KeyT nr, bool has_prev, uint32_t prev,
-                                            bool has_next, uint32_t next) {
-  const KeyT can = kmin(fw, rcv);
-  const bool fwd = fw == can;
+// one occurrence (front nibble low, back nibble high; M = 0xF), from what it
+// depends on: whether the k-mer is read forward (fwd), whether it has a base
+// before / after it (and which), whether the next k-mer is the same vertex
+// (next_same) and, if so, the same oriented k-mer (next_same_fw).  prev is
+// not read without has_prev, nor next, next_same, next_same_fw without
+// has_next.
+CF1_HD uint32_t sideset_byte(bool fwd, bool has_prev, uint32_t prev, bool has_next, uint32_t next, bool next_same,
+                             bool next_same_fw) {
   if (!has_prev && !has_next) return 0xFFu;
   const uint32_t cp = side_code(prev), cpc = side_code(3 - prev);
   const uint32_t right = fwd ? (cp | 0xF0u) : (0x0Fu | (cpc << 4));
   if (!has_next) return right;
-  if (kmin(nf, nr) == can) return (!has_prev || nf == fw) ? 0xFFu : right;
+  if (next_same) return (!has_prev || next_same_fw) ? 0xFFu : right;
   const uint32_t cn = side_code(next), cnc = side_code(3 - next);
   if (!has_prev) return fwd ? (0x0Fu | (cn << 4)) : (cnc | 0xF0u);
   return fwd ? (cp | (cn << 4)) : (cnc | (cpc << 4));
+}
+
+// The same from the k-mer's forward and reverse-complement values and the
+// next k-mer's (nf, nr: the k-mer rolled by `next`), which a caller walking
+// the sequence has already; with !has_next nf and nr are not read.
+template <class KeyT>
+CF1_HD uint32_t contribution_sideset_rolled(KeyT fw, KeyT rcv, KeyT nf, KeyT nr, bool has_prev, uint32_t prev,
+                                            bool has_next, uint32_t next) {
+  const KeyT can = kmin(fw, rcv);
+  return sideset_byte(fw == can, has_prev, prev, has_next, next, has_next && kmin(nf, nr) == can,
+                      has_next && nf == fw);
 }
 
 template <class KeyT>

@@ -14,55 +14,55 @@ namespace cf1 {
 namespace {
 
 // ---------------------------------------------------------------- pack ----
-// One thread per 64 input bytes: two words of W and one word of NM.  A byte is
-// a base when (byte & 0xDF) is one of 'A' 'C' 'G' 'T' (upper- or lower-case,
-// src/dna.rs:64-92); bits 1-2 of the upper-case letter give A0 C1 G3 T2, and
-// one xor fixes G/T.
+// Four threads per word of NM (64 input bytes): each loads its 16 bytes with
+// one 16-byte load, so a warp reads 512 consecutive bytes; a pair of threads
+// makes one word of W and a quad one word of NM (by shuffles), and the words
+// are stored by the even / first lanes.  A byte is a base when (byte & 0xDF)
+// is one of 'A' 'C' 'G' 'T' (upper- or lower-case, src/dna.rs:64-92); bits
+// 1-2 of the upper-case letter give A0 C1 G3 T2, and one xor fixes G/T.
+// Bytes past L read as placeholders.
 __global__ void pack_kernel(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, uint64_t t0, uint64_t n_nm) {
-  uint64_t t = t0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n_nm) return;
-  uint64_t base = t * 64;
-  uint64_t bytes[8];
-  if (base + 64 <= L) {
-    const uint4 *src = reinterpret_cast<const uint4 *>(ascii + base);
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      uint4 v = src[i];
-      bytes[2 * i] = ((uint64_t)v.y << 32) | v.x;
-      bytes[2 * i + 1] = ((uint64_t)v.w << 32) | v.z;
-    }
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t t = t0 + (g >> 2);  // the NM word this thread's 16 bases belong to
+  const uint32_t q = (uint32_t)(g & 3);
+  const bool live = t < n_nm;
+  const uint64_t base = t * 64 + q * 16;
+  uint32_t v[4];
+  if (live && base + 16 <= L) {
+    const uint4 x = *reinterpret_cast<const uint4 *>(ascii + base);
+    v[0] = x.x;
+    v[1] = x.y;
+    v[2] = x.z;
+    v[3] = x.w;
   } else {
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      uint64_t x = 0;
-      for (int j = 0; j < 8; j++) {
-        uint64_t p = base + 8 * i + j;
-        uint64_t c = p < L ? ascii[p] : (uint64_t)'N';
-        x |= c << (8 * j);
+    for (int i = 0; i < 4; i++) {
+      uint32_t y = 0;
+      for (int j = 0; j < 4; j++) {
+        const uint64_t p = base + 4 * i + j;
+        y |= (uint32_t)(live && p < L ? ascii[p] : (uint8_t)'N') << (8 * j);
       }
-      bytes[i] = x;
+      v[i] = y;
     }
   }
-  uint64_t w0 = 0, w1 = 0, nm = 0;
+  uint32_t w = 0, nm = 0;  // base i of the 16 at bits 30-2i of w, its placeholder bit at bit i of nm
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      uint32_t c = (uint32_t)(bytes[i] >> (8 * j)) & 0xFF;
-      uint32_t u = c & 0xDF;
-      bool ok = (u == 'A') | (u == 'C') | (u == 'G') | (u == 'T');
-      uint32_t b = (u >> 1) & 3;
-      b ^= b >> 1;
-      b = ok ? b : 0;
-      int idx = 8 * i + j;
-      if (idx < 32) w0 |= (uint64_t)b << (62 - 2 * idx);
-      else w1 |= (uint64_t)b << (62 - 2 * (idx - 32));
-      nm |= (uint64_t)(!ok) << idx;
-    }
+  for (int i = 0; i < 16; i++) {
+    const uint32_t c = (v[i >> 2] >> (8 * (i & 3))) & 0xFF;
+    const uint32_t u = c & 0xDF;
+    const bool ok = (u == 'A') | (u == 'C') | (u == 'G') | (u == 'T');
+    uint32_t b = (u >> 1) & 3;
+    b ^= b >> 1;
+    w |= (ok ? b : 0u) << (30 - 2 * i);
+    nm |= (uint32_t)(!ok) << i;
   }
-  W[2 * t] = w0;
-  W[2 * t + 1] = w1;
-  NM[t] = nm;
+  const uint32_t w_next = __shfl_down_sync(FULL, w, 1);
+  const uint32_t pair = nm | (__shfl_down_sync(FULL, nm, 1) << 16);
+  const uint32_t pair_next = __shfl_down_sync(FULL, pair, 2);
+  if (live) {
+    if ((q & 1) == 0) W[2 * t + (q >> 1)] = ((uint64_t)w << 32) | w_next;
+    if (q == 0) NM[t] = pair | ((uint64_t)pair_next << 32);
+  }
 }
 
 // -------------------------------------------------------------- super k-mers ----
@@ -439,7 +439,7 @@ void launch_pack(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, cu
 void launch_pack_words(const uint8_t *ascii, uint64_t L, uint64_t *W, uint64_t *NM, uint64_t w0, uint64_t w1,
                        cudaStream_t s) {
   if (w1 <= w0) return;
-  pack_kernel<<<(unsigned)ceil_div(w1 - w0, 256), 256, 0, s>>>(ascii, L, W, NM, w0, w1);
+  pack_kernel<<<(unsigned)ceil_div((w1 - w0) * 4, 256), 256, 0, s>>>(ascii, L, W, NM, w0, w1);
   CF1_LAUNCH_CHECK();
 }
 

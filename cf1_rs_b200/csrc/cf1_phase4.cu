@@ -230,39 +230,52 @@ __global__ void __launch_bounds__(256) place_sides_kernel(MphfView<KeyT> m, cons
   if (__any_sync(FULL, miss) && lane == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
 }
 
-// One warp per sub-bucket: the bytes of the keys levels 0 and 1 placed
-// (placed[j] and placed1[j] of them), already in rank order, to the two
-// slices' runs of slots (level 1's bytes follow level 0's in l0pay).
+// One warp per PL_GROUP consecutive sub-buckets: the bytes of the keys
+// levels 0 and 1 placed (placed[j] and placed1[j] of them), already in rank
+// order, to the two slices' runs of slots (level 1's bytes follow level 0's
+// in l0pay).  The group's counts and slot bases are loaded by one lane each,
+// in parallel, then every sub-bucket's bytes are copied by the whole warp.
+constexpr uint32_t PL_GROUP = 8;
 __global__ void __launch_bounds__(256) place_l0_kernel(BBView bb, const uint64_t *dist_off, const uint64_t *sb_off,
                                                        const uint32_t *placed, const uint32_t *placed1,
                                                        const uint8_t *l0pay, uint64_t j0, uint64_t j1, int P,
                                                        uint8_t *sides, uint32_t *err) {
-  const uint64_t j = j0 + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (j >= j1) return;
-  const uint32_t np0 = placed[j], np1 = placed1[j];
-  if (!(np0 | np1)) return;
-  const uint32_t bin = (uint32_t)(j >> P);
-  const uint8_t *src = l0pay + sb_off[j];
+  const unsigned lane = lane_id();
+  const uint64_t g0 = j0 + (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * PL_GROUP;
+  if (g0 >= j1) return;  // the same for the whole warp
+  const uint64_t j = g0 + lane;
+  uint32_t np0 = 0, np1 = 0;
+  uint64_t src = 0, base0 = 0, base1 = 0;
   bool bad = false;
-  if (bb.l1_slice_bits != P || bb.levels < 2) {
-    bad = true;
-  } else {
-    // a slice's first slot: the bin's slots, the keys earlier levels placed,
-    // the placed keys of the bin's slices before it
-    if (np0) {
-      const uint64_t base = dist_off[bin] + (uint32_t)(bb.meta[bin].rank_adj + bb.srank[0][j]);
-      if (base + np0 > dist_off[bin + 1]) bad = true;
-      else
-        for (uint32_t r = lane_id(); r < np0; r += 32) sides[base + r] = src[r];
-    }
-    if (np1) {
-      const uint64_t base = dist_off[bin] + (uint32_t)(bb.meta[bb.nbins + bin].rank_adj + bb.srank[1][j]);
-      if (base + np1 > dist_off[bin + 1]) bad = true;
-      else
-        for (uint32_t r = lane_id(); r < np1; r += 32) sides[base + r] = src[np0 + r];
+  if (lane < PL_GROUP && j < j1) {
+    np0 = placed[j];
+    np1 = placed1[j];
+    if (np0 | np1) {
+      if (bb.l1_slice_bits != P || bb.levels < 2) {
+        bad = true;
+      } else {
+        // a slice's first slot: the bin's slots, the keys earlier levels
+        // placed, the placed keys of the bin's slices before it
+        const uint32_t bin = (uint32_t)(j >> P);
+        const uint64_t lo = dist_off[bin], hi = dist_off[bin + 1];
+        src = sb_off[j];
+        base0 = lo + (uint32_t)(bb.meta[bin].rank_adj + bb.srank[0][j]);
+        base1 = lo + (uint32_t)(bb.meta[bb.nbins + bin].rank_adj + bb.srank[1][j]);
+        bad = (np0 && base0 + np0 > hi) || (np1 && base1 + np1 > hi);
+      }
+      if (bad) np0 = np1 = 0;
     }
   }
-  if (bad && lane_id() == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
+  if (__any_sync(FULL, bad) && lane == 0) atomicOr(err, (uint32_t)DEV_MPHF_MISS);
+  for (uint32_t i = 0; i < PL_GROUP; i++) {
+    const uint32_t a0 = __shfl_sync(FULL, np0, i), a1 = __shfl_sync(FULL, np1, i);
+    if (!(a0 | a1)) continue;
+    const uint64_t s0 = __shfl_sync(FULL, src, i), b0 = __shfl_sync(FULL, base0, i),
+                   b1 = __shfl_sync(FULL, base1, i);
+    const uint8_t *sp = l0pay + s0;
+    for (uint32_t r = lane; r < a0; r += 32) sides[b0 + r] = sp[r];
+    for (uint32_t r = lane; r < a1; r += 32) sides[b1 + r] = sp[a0 + r];
+  }
 }
 
 // The keys levels 0 and 1 left: SV_CTAS CTAs per bin, each key walks from
@@ -388,8 +401,8 @@ void launch_place_l0(const BBView &bb, const uint64_t *dist_off, const uint64_t 
                      const uint32_t *placed1, const uint8_t *l0pay, uint64_t j0, uint64_t j1, int P, uint8_t *sides,
                      uint32_t *err, cudaStream_t s) {
   if (j1 <= j0) return;
-  place_l0_kernel<<<(unsigned)ceil_div((j1 - j0) * 32, 256), 256, 0, s>>>(bb, dist_off, sb_off, placed, placed1, l0pay,
-                                                                          j0, j1, P, sides, err);
+  place_l0_kernel<<<(unsigned)ceil_div(ceil_div(j1 - j0, (uint64_t)PL_GROUP) * 32, 256), 256, 0, s>>>(
+      bb, dist_off, sb_off, placed, placed1, l0pay, j0, j1, P, sides, err);
   CF1_LAUNCH_CHECK();
 }
 
