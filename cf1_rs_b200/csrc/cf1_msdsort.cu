@@ -810,11 +810,17 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
       //    loaded before the first is inserted).  Double hashing: the probe
       //    step is odd (so a probe sequence visits every slot) and comes from
       //    other bits of the same product, which keeps the runs a warp waits
-      //    for (the longest of its 32 lanes) short at the set's load.
+      //    for (the longest of its 32 lanes) short at the set's load.  The
+      //    first probes of a lane's WD_U keys are issued back to back; only
+      //    the keys whose first slot held another key then walk on, one key
+      //    index at a time.  (A key can find the set full only after more
+      //    than WD_MAXD keys were claimed, so the sub-bucket goes to the block
+      //    kernel anyway.)
       uint32_t d = 0;
       for (uint64_t base = 0; base < n && !over; base += 32 * WD_U) {
         unsigned long long key[WD_U];
-        uint32_t p[WD_U];
+        uint32_t p[WD_U], h[WD_U], stp[WD_U];
+        bool claimed[WD_U], pend[WD_U];
   #pragma unroll
         for (int u = 0; u < WD_U; u++) {
           const uint64_t i = base + u * 32 + lane;
@@ -823,26 +829,39 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
         }
   #pragma unroll
         for (int u = 0; u < WD_U; u++) {
-          if (over) break;  // the set stays below full: at most WD_MAXD + 32 keys in it
-          bool claimed = false;
-          uint32_t h = 0;
+          claimed[u] = pend[u] = false;
+          h[u] = stp[u] = 0;
           if (key[u] != EMPTY) {
             const unsigned long long hk = key[u] * 0x9E3779B97F4A7C15ull;
-            h = (uint32_t)(hk >> 55);                               // top 9 bits: WD_TW = 512
-            const uint32_t step = ((uint32_t)(hk >> 40) | 1u) & (WD_TW - 1);
-            for (uint32_t probe = 0; probe < WD_TW; probe++) {
-              const unsigned long long old = atomicCAS(&m.tab[h], EMPTY, key[u]);
-              if (old == EMPTY || old == key[u]) {
-                claimed = old == EMPTY;
-                if (pay) atomicOr(reinterpret_cast<uint32_t *>(m.tpay) + (h >> 2), p[u] << (8 * (h & 3)));
-                break;
-              }
-              h = (h + step) & (WD_TW - 1);
+            h[u] = (uint32_t)(hk >> 55);                                // top 9 bits: WD_TW = 512
+            stp[u] = ((uint32_t)(hk >> 40) | 1u) & (WD_TW - 1);
+            const unsigned long long old = atomicCAS(&m.tab[h[u]], EMPTY, key[u]);
+            if (old == EMPTY || old == key[u]) {
+              claimed[u] = old == EMPTY;
+              if (pay) atomicOr(reinterpret_cast<uint32_t *>(m.tpay) + (h[u] >> 2), p[u] << (8 * (h[u] & 3)));
+            } else {
+              pend[u] = true;
+              h[u] = (h[u] + stp[u]) & (WD_TW - 1);
             }
           }
-          const unsigned b = __ballot_sync(FULL, claimed);
+        }
+  #pragma unroll
+        for (int u = 0; u < WD_U; u++) {
+          if (over) break;  // the set stays below full: at most WD_MAXD + 32 * WD_U keys in it
+          if (__any_sync(FULL, pend[u]) && pend[u]) {
+            for (uint32_t probe = 1; probe < WD_TW; probe++) {
+              const unsigned long long old = atomicCAS(&m.tab[h[u]], EMPTY, key[u]);
+              if (old == EMPTY || old == key[u]) {
+                claimed[u] = old == EMPTY;
+                if (pay) atomicOr(reinterpret_cast<uint32_t *>(m.tpay) + (h[u] >> 2), p[u] << (8 * (h[u] & 3)));
+                break;
+              }
+              h[u] = (h[u] + stp[u]) & (WD_TW - 1);
+            }
+          }
+          const unsigned b = __ballot_sync(FULL, claimed[u]);
           const uint32_t r = d + __popc(b & lt);
-          if (claimed && r < WD_MAXD) m.ins[r] = (uint16_t)h;
+          if (claimed[u] && r < WD_MAXD) m.ins[r] = (uint16_t)h[u];
           d += __popc(b);
           over = d > WD_MAXD;
         }
