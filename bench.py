@@ -468,7 +468,11 @@ def gpu_arm(args):
         # writes every distinct key and its joined byte (+ in the BBHash form
         # BBHash level 0: 8 bits per occurrence, stored as 16-B {bits, rank}
         # entries per 64 bits, i.e. 2 B per occurrence)
-        b_dd = (w + 1.0) * n_occ + (w + 1.0) * n_dist + (2.0 * n_occ if head_name == "bbhash" else 0.0)
+        # The BBHash form with 64-bit keys and a split of >= 6 bits runs the
+        # multisplit on packed words (the byte inside the key's word), so the
+        # dedup reads w bytes per occurrence there
+        packed = head_name == "bbhash" and w == 8 and 6 <= int(s["sort_msd_bits"]) <= 64
+        b_dd = (w if packed else w + 1.0) * n_occ + (w + 1.0) * n_dist + (2.0 * n_occ if head_name == "bbhash" else 0.0)
         ach = b_dd / (head["ms_dedup_kernel"] / 1e3) / 1e9
         # BBHash form: the warp dedup, with the block kernel for the few
         # sub-buckets it leaves (timed together); learned form: the sorted

@@ -215,6 +215,16 @@ CF1_HD uint32_t mix_order(uint32_t x) {
 // BBHash level 0 (bit = top bits of key * KEY_SPREAD_MUL, scaled) use the same
 // one, so the keys of one sub-bucket land in one stretch of level 0's bits.
 constexpr uint64_t KEY_SPREAD_MUL = 0xD6E8FEB86659FD93ull;
+// Its inverse mod 2^64 (Newton's iteration x <- x (2 - a x) doubles the
+// correct low bits, from 3 for x = a): key = (key * KEY_SPREAD_MUL) *
+// KEY_SPREAD_INV.
+constexpr uint64_t inverse_mod64(uint64_t a) {
+  uint64_t x = a;
+  for (int i = 0; i < 6; i++) x *= 2 - a * x;
+  return x;
+}
+constexpr uint64_t KEY_SPREAD_INV = inverse_mod64(KEY_SPREAD_MUL);
+static_assert(KEY_SPREAD_MUL * KEY_SPREAD_INV == 1, "KEY_SPREAD_INV inverts KEY_SPREAD_MUL");
 
 // Inverse of mix_order (the multipliers' inverses mod 2^32; x ^= x >> 15 is
 // undone by x ^= (x >> 15) ^ (x >> 30)).  mix_order is a bijection, so the

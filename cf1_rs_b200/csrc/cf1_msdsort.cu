@@ -58,6 +58,33 @@ CF1_D uint32_t ms_digit<Key2>(const Key2 &k, int shift, uint32_t mask, bool) {
   return KOps<Key2>::digit(k, shift, mask);
 }
 
+// Packed words (hashed split of 64-bit keys with payload bytes, pass 1 of at
+// least 6 bits): after the first pass a key's top p1 bits of h = key *
+// MS_HASH_MUL are its segment's, so the word keeps the other 64 - p1 bits of
+// h, shifted up, and the payload byte's 6-bit code in the p1 bits freed.
+// The next pass splits on the word's own top bits; the dedup rebuilds h from
+// the sub-bucket's index and the key as h * KEY_SPREAD_INV.  A single
+// occurrence's side-set byte has nibbles in {3, 5, 6, 9, F} (sideset_byte):
+// each nibble is a 3-bit code (0 also has one; anything else, which no
+// occurrence gives, reads as F).
+constexpr uint64_t pay_nib_codes() {
+  uint64_t t = 0;
+  for (uint32_t v = 0; v < 16; v++) {
+    const uint64_t c = v == 3 ? 0 : v == 5 ? 1 : v == 6 ? 2 : v == 9 ? 3 : v == 0 ? 5 : 4;
+    t |= c << (3 * v);
+  }
+  return t;
+}
+constexpr uint64_t PAY_NIB_CODE = pay_nib_codes();  // nibble -> code, 3 bits each
+constexpr uint32_t PAY_NIB_OF = 0x0F9653u;            // code -> nibble, 4 bits each (codes 0..5)
+CF1_HD uint32_t pay_code(uint32_t byte) {
+  return (uint32_t)((PAY_NIB_CODE >> (3 * (byte & 0xF))) & 7) | ((uint32_t)((PAY_NIB_CODE >> (3 * (byte >> 4))) & 7) << 3);
+}
+CF1_HD uint32_t pay_byte(uint32_t code) {
+  return ((PAY_NIB_OF >> (4 * (code & 7))) & 0xF) | (((PAY_NIB_OF >> (4 * ((code >> 3) & 7))) & 0xF) << 4);
+}
+constexpr uint32_t PACK_MIN_BITS = 6;  // a packed word's payload code needs 6 of the freed bits
+
 // ---------------------------------------------------------------- multisplit pass
 template <class KeyT, int BITS>
 __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, const uint64_t *seg_off,
@@ -89,11 +116,11 @@ __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, con
 // consecutive addresses.  Four CTAs per SM (64 registers): at 3.1 Gbp the
 // two 64-bit passes took 3.3 ms less than with three CTAs and 80 registers.
 // With pin/pout, each key's payload byte (its side-set byte) moves with it.
-template <class KeyT, int BITS>
+template <class KeyT, int BITS, bool PACK>
 __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
                                                                  const uint32_t *tile_off, uint32_t nseg, int shift,
                                                                  bool hashed, const uint64_t *Hs, const uint8_t *pin,
-                                                                 uint8_t *pout) {
+                                                                 uint8_t *pout, int pack) {
   constexpr uint32_t DIG = 1u << BITS;
   extern __shared__ __align__(16) unsigned char ms_smem[];
   KeyT *stage = reinterpret_cast<KeyT *>(ms_smem);                            // [MS_TILE]
@@ -185,8 +212,12 @@ __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in,
     KeyT kk = stage[i];
     uint32_t d = ms_digit(kk, shift, DIG - 1, hashed);
     const uint64_t o = base[d] + (i - lstart[d]);
-    out[o] = kk;
-    if (pin) pout[o] = pstage[i];
+    if constexpr (PACK) {  // hashed 64-bit keys with payloads: the packed word (see pay_code)
+      out[o] = ((kk * MS_HASH_MUL) << pack) | pay_code(pstage[i]);
+    } else {
+      out[o] = kk;
+      if (pout) pout[o] = pstage[i];
+    }
   }
 }
 
@@ -775,9 +806,15 @@ struct WdSmem {
 };
 static_assert(sizeof(WdSmem) % 8 == 0, "per-warp areas stay 8-byte aligned");
 
+// PK: T holds packed words of a first pass of p1 bits (see pay_code); the
+// set then holds each key's h = key * MS_HASH_MUL without its top p1 bits,
+// level 0's bit comes from h directly, and the keys written back (T, the
+// level-2 list) are h * KEY_SPREAD_INV.  TP is only written.
+template <bool PK>
 __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T, uint8_t *TP, const uint64_t *sb_off,
                                                                    uint64_t nsub, int P, uint32_t *cnt, Level0Out l0,
-                                                                   uint32_t *ov, uint32_t *ov_cnt, uint32_t *queue) {
+                                                                   uint32_t *ov, uint32_t *ov_cnt, uint32_t *queue,
+                                                                   int p1) {
   extern __shared__ __align__(16) unsigned char wd_smem[];
   WdSmem &m = reinterpret_cast<WdSmem *>(wd_smem)[threadIdx.x >> 5];
   const unsigned lane = lane_id(), lt = lanemask_lt();
@@ -806,6 +843,13 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
         first = l0.woff[bin] + (uint64_t)sub * sw;
       }
       bool over = lv0 && sw > WD_SWMAX;
+      // PK: the h bits the sub-bucket's first-pass digit gives; a set entry
+      // id stands for the key whose h is hi | id
+      const uint64_t hi = PK ? (uint64_t)(sub >> (P - p1)) << (64 - p1) : 0;
+      auto key_of = [&](unsigned long long id) -> uint64_t { return PK ? (hi | id) * KEY_SPREAD_INV : id; };
+      auto l0_bit = [&](unsigned long long id) -> uint64_t {
+        return PK ? (((uint64_t)(uint32_t)((hi | id) >> 32) * (uint32_t)W) >> 26) : bb_pos(id, 0, (uint32_t)W);
+      };
       // 1. one copy of each key, its copies' payloads ORed (WD_U keys per lane
       //    loaded before the first is inserted).  Double hashing: the probe
       //    step is odd (so a probe sequence visits every slot) and comes from
@@ -824,8 +868,14 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
   #pragma unroll
         for (int u = 0; u < WD_U; u++) {
           const uint64_t i = base + u * 32 + lane;
-          key[u] = i < n ? T[a + i] : EMPTY;
-          p[u] = (pay && i < n) ? TP[a + i] : 0u;
+          if constexpr (PK) {
+            const uint64_t w = i < n ? T[a + i] : 0;
+            key[u] = i < n ? w >> p1 : EMPTY;
+            p[u] = i < n ? pay_byte((uint32_t)w) : 0u;
+          } else {
+            key[u] = i < n ? T[a + i] : EMPTY;
+            p[u] = (pay && i < n) ? TP[a + i] : 0u;
+          }
         }
   #pragma unroll
         for (int u = 0; u < WD_U; u++) {
@@ -890,11 +940,11 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
         const uint32_t h = m.ins[r];
         const unsigned long long key = m.tab[h];
         const uint8_t pr = m.tpay[h];
-        T[a + r] = key;
+        T[a + r] = key_of(key);
         if (pay) TP[a + r] = pr;
         m.tpay[h] = 0;
         if (lv0) {
-          const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
+          const uint64_t bpos = l0_bit(key) - lo_bit;
           if (bpos < (uint64_t)sw * 64) {
             const unsigned long long bit = 1ull << (bpos & 63);
             if (atomicOr(&m.set[bpos >> 6], bit) & bit) atomicOr(&m.col[bpos >> 6], bit);
@@ -948,7 +998,7 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
           h = m.ins[r];
           pr = m.dp[r];
           const unsigned long long key = m.tab[h];
-          const uint64_t bpos = bb_pos(key, 0, (uint32_t)W) - lo_bit;
+          const uint64_t bpos = l0_bit(key) - lo_bit;
           if (bpos < (uint64_t)sw * 64) {
             const unsigned long long fin = m.set[bpos >> 6] & ~m.col[bpos >> 6], bit = 1ull << (bpos & 63);
             if (fin & bit) {
@@ -956,9 +1006,9 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
               m.tab[h] = EMPTY;
             } else if (l1ok) {
               lv = true;
-              const uint32_t p1 = bb_slice_pos(key, 1, sw1);
-              const unsigned long long bit1 = 1ull << (p1 & 63);
-              if (atomicOr(&m.set1[p1 >> 6], bit1) & bit1) atomicOr(&m.col1[p1 >> 6], bit1);
+              const uint32_t q1 = bb_slice_pos(key_of(key), 1, sw1);
+              const unsigned long long bit1 = 1ull << (q1 & 63);
+              if (atomicOr(&m.set1[q1 >> 6], bit1) & bit1) atomicOr(&m.col1[q1 >> 6], bit1);
             } else {
               m.tab[h] = EMPTY;
             }
@@ -1008,12 +1058,12 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
         unsigned long long key = 0;
         if (k < nsv) {
           const uint32_t h = m.ins[k];
-          key = m.tab[h];
+          key = key_of(m.tab[h]);
           m.tab[h] = EMPTY;
-          const uint32_t p1 = bb_slice_pos(key, 1, sw1);
-          const unsigned long long fin1 = m.set1[p1 >> 6] & ~m.col1[p1 >> 6], bit1 = 1ull << (p1 & 63);
+          const uint32_t q1 = bb_slice_pos(key, 1, sw1);
+          const unsigned long long fin1 = m.set1[q1 >> 6] & ~m.col1[q1 >> 6], bit1 = 1ull << (q1 & 63);
           if (fin1 & bit1) {
-            if (lpay) l0.l0pay[a + placed + m.pw1[p1 >> 6] + (uint32_t)__popcll(fin1 & (bit1 - 1))] = m.dp[k];
+            if (lpay) l0.l0pay[a + placed + m.pw1[q1 >> 6] + (uint32_t)__popcll(fin1 & (bit1 - 1))] = m.dp[k];
           } else {
             surv = true;
           }
@@ -1028,6 +1078,22 @@ __global__ void __launch_bounds__(WD_WARPS * 32, 4) wd_dedup_kernel(uint64_t *T,
       }
       __syncwarp();
     }
+  }
+}
+
+// Packed sub-buckets the warp dedup left to the block kernel, back to keys
+// and payload bytes (one warp per listed sub-bucket).
+__global__ void wd_unpack_kernel(uint64_t *T, uint8_t *TP, const uint64_t *sb_off, const uint32_t *ov,
+                                 const uint32_t *ov_cnt, int P, int p1) {
+  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= *ov_cnt) return;
+  const uint64_t j = ov[w], a = sb_off[j], n = sb_off[j + 1] - a;
+  const uint32_t sub = (uint32_t)(j & ((1ull << P) - 1));
+  const uint64_t hi = (uint64_t)(sub >> (P - p1)) << (64 - p1);
+  for (uint64_t i = lane_id(); i < n; i += 32) {
+    const uint64_t x = T[a + i];
+    TP[a + i] = (uint8_t)pay_byte((uint32_t)x);
+    T[a + i] = (hi | (x >> p1)) * KEY_SPREAD_INV;
   }
 }
 
@@ -1079,7 +1145,7 @@ __global__ void cs_bin_off_kernel(const uint64_t *out_off, uint32_t nbins, uint6
 
 template <class KeyT, int BITS>
 void ms_pass(const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift, bool hashed,
-             MsdScratch &sc, cudaStream_t s, const uint8_t *pin, uint8_t *pout) {
+             MsdScratch &sc, cudaStream_t s, const uint8_t *pin, uint8_t *pout, int pack) {
   constexpr uint32_t DIG = 1u << BITS;
   uint32_t ub = (uint32_t)(ceil_div(n, MS_TILE) + nseg);
   uint32_t *tile_off = sc.tile_off.get<uint32_t>(nseg + 1);
@@ -1091,24 +1157,26 @@ void ms_pass(const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uin
   exclusive_scan_u32(H, Hs, (uint64_t)ub * DIG, sc.scan_tmp, s);
   size_t smem = MS_TILE * sizeof(KeyT) + (MS_NW + 1) * DIG * sizeof(uint32_t) + DIG * sizeof(uint64_t) +
                 (pin ? MS_TILE : 0);
-  CF1_CUDA(cudaFuncSetAttribute(ms_scatter_kernel<KeyT, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  ms_scatter_kernel<KeyT, BITS><<<ub, MS_BLOCK, smem, s>>>(in, out, seg_off, tile_off, nseg, shift, hashed, Hs, pin,
-                                                           pout);
+  auto kern = ms_scatter_kernel<KeyT, BITS, false>;
+  if constexpr (KOps<KeyT>::WORDS == 1)
+    if (pack) kern = ms_scatter_kernel<KeyT, BITS, true>;
+  CF1_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<ub, MS_BLOCK, smem, s>>>(in, out, seg_off, tile_off, nseg, shift, hashed, Hs, pin, pout, pack);
   CF1_LAUNCH_CHECK();
 }
 
 template <class KeyT>
 void ms_pass_bits(int bits, const KeyT *in, KeyT *out, uint64_t n, const uint64_t *seg_off, uint32_t nseg, int shift,
-                  bool hashed, MsdScratch &sc, cudaStream_t s, const uint8_t *pin, uint8_t *pout) {
+                  bool hashed, MsdScratch &sc, cudaStream_t s, const uint8_t *pin, uint8_t *pout, int pack = 0) {
   switch (bits) {
-    case 1: ms_pass<KeyT, 1>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
-    case 2: ms_pass<KeyT, 2>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
-    case 3: ms_pass<KeyT, 3>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
-    case 4: ms_pass<KeyT, 4>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
-    case 5: ms_pass<KeyT, 5>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
-    case 6: ms_pass<KeyT, 6>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
-    case 7: ms_pass<KeyT, 7>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
-    case 8: ms_pass<KeyT, 8>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout); break;
+    case 1: ms_pass<KeyT, 1>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout, pack); break;
+    case 2: ms_pass<KeyT, 2>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout, pack); break;
+    case 3: ms_pass<KeyT, 3>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout, pack); break;
+    case 4: ms_pass<KeyT, 4>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout, pack); break;
+    case 5: ms_pass<KeyT, 5>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout, pack); break;
+    case 6: ms_pass<KeyT, 6>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout, pack); break;
+    case 7: ms_pass<KeyT, 7>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout, pack); break;
+    case 8: ms_pass<KeyT, 8>(in, out, n, seg_off, nseg, shift, hashed, sc, s, pin, pout, pack); break;
     default: throw Error(-1, "MSD pass width must be 1..8 bits");
   }
 }
@@ -1171,14 +1239,20 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
   // its hash when only distinct keys are wanted (64-bit keys)
   const bool hashed = !sorted && KOps<KeyT>::WORDS == 1;
   if (hashed) key_bits = 64;
-  const int P1 = P > 8 ? (P + 1) / 2 : P, P2 = P - P1;
+  // packed passes (see pay_code): the hashed split of keys with payloads
+  // whose dedup builds BBHash level 0, with a first pass of >= 6 bits
+  const bool pk = hashed && pkeys && palt && l0 && l0->AR && l0->with_pay && P >= (int)PACK_MIN_BITS;
+  int P1 = P > 8 ? (P + 1) / 2 : P;
+  if (pk && P1 < (int)PACK_MIN_BITS) P1 = PACK_MIN_BITS;
+  const int P2 = P - P1;
   KeyT *T = keys;
   uint64_t nsub = (uint64_t)nbins << P;
   uint64_t *sb_off = sc.sb_off.get<uint64_t>(nsub + 1);
   if (P == 0) {
     CF1_CUDA(cudaMemcpyAsync(sb_off, seg_off, (nbins + 1) * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
   } else if (n) {
-    ms_pass_bits<KeyT>(P1, keys, alt, n, seg_off, nbins, key_bits - P1, hashed, sc, s, pkeys, palt);
+    ms_pass_bits<KeyT>(P1, keys, alt, n, seg_off, nbins, key_bits - P1, hashed, sc, s, pkeys, pk ? nullptr : palt,
+                       pk ? P1 : 0);
     const uint64_t *seg2 = seg_off;
     uint32_t nseg2 = nbins;
     if (P2) {
@@ -1187,7 +1261,10 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
       subbuckets_bits(P1, seg_off, sc.tile_off.as<uint32_t>(), nbins, sc.hscan.as<uint64_t>(), sb1, s);
       nseg2 = (uint32_t)((uint64_t)nbins << P1);
       seg2 = sb1;
-      ms_pass_bits<KeyT>(P2, alt, keys, n, seg2, nseg2, key_bits - P1 - P2, hashed, sc, s, palt, pkeys);
+      if (pk)  // packed words: their own top bits are the next digit, the bytes travel inside
+        ms_pass_bits<KeyT>(P2, alt, keys, n, seg2, nseg2, 64 - P2, false, sc, s, nullptr, nullptr);
+      else
+        ms_pass_bits<KeyT>(P2, alt, keys, n, seg2, nseg2, key_bits - P1 - P2, hashed, sc, s, palt, pkeys);
       T = keys;
       PT = pkeys;
     } else {
@@ -1257,15 +1334,21 @@ bool msd_sort_unique(KeyT *keys, KeyT *alt, uint64_t n, const uint64_t *seg_off,
       uint32_t *ovc = sc.ovc.get<uint32_t>(2);  // overflow count, work counter
       CF1_CUDA(cudaMemsetAsync(ovc, 0, 2 * sizeof(uint32_t), s));
       const size_t wsm = WD_WARPS * sizeof(WdSmem);
-      CF1_CUDA(cudaFuncSetAttribute(wd_dedup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
-      const unsigned wgrid = persistent_grid(wd_dedup_kernel, WD_WARPS * 32, wsm, -1, ceil_div(nsub, WD_WARPS));
-      wd_dedup_kernel<<<wgrid, WD_WARPS * 32, wsm, s>>>(reinterpret_cast<uint64_t *>(T), PT, sb_off, nsub, P, cnt, lo,
-                                                        ov, ovc, ovc + 1);
+      auto wkern = pk ? wd_dedup_kernel<true> : wd_dedup_kernel<false>;
+      CF1_CUDA(cudaFuncSetAttribute(wkern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+      const unsigned wgrid = persistent_grid(wkern, WD_WARPS * 32, wsm, -1, ceil_div(nsub, WD_WARPS));
+      wkern<<<wgrid, WD_WARPS * 32, wsm, s>>>(reinterpret_cast<uint64_t *>(T), PT, sb_off, nsub, P, cnt, lo, ov, ovc,
+                                              ovc + 1, pk ? P1 : 0);
       CF1_LAUNCH_CHECK();
       uint32_t h_ov = 0;
       CF1_CUDA(cudaMemcpyAsync(&h_ov, ovc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
       CF1_CUDA(cudaStreamSynchronize(s));
       sc.last_overflow = h_ov;
+      if (h_ov && pk) {  // the block kernel takes keys and bytes
+        wd_unpack_kernel<<<(unsigned)ceil_div((uint64_t)h_ov * 32, 256), 256, 0, s>>>(
+            reinterpret_cast<uint64_t *>(T), PT, sb_off, ov, ovc, P, P1);
+        CF1_LAUNCH_CHECK();
+      }
       if (h_ov) {
         kern<<<h_ov, CS_BLOCK, smem, s>>>(T, U, sb_off, nsub, shift, rest > 0 ? bits : 0, cnt, over, P, lo, PT, PU,
                                           nullptr, nullptr, nbins, ov);
