@@ -86,6 +86,27 @@ def test_sorted_runs_over_sparse_key_ranges(tmp_path):
     g.close()
 
 
+@pytest.mark.parametrize("n_bases,bits", [(24_540, 6), (392_600, 10)])
+def test_packed_words_with_subbuckets_left_to_block_kernel(tmp_path, n_bases, bits):
+    """BBHash form, one bin of random sequence.  The tuner line sets the split
+    one bit below the default, so sub-buckets average ~383 distinct keys and
+    about half pass the warp dedup's 384: those go to the block kernel, whose
+    input is unpacked first.  With a split of 6 bits (one pass) or 10 (6 + 4)
+    the multisplit runs on packed words."""
+    rng = np.random.default_rng(n_bases)
+    s = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, n_bases)].tobytes()
+    seq, off = o.concat_records([s])
+    size_class = (n_bases + 1).bit_length() - 1  # floor(log2) of the input with its record separator
+    cache = tmp_path / "tuner.txt"
+    cache.write_text(f"cf1tune 1 wide=0 sorted=0 batched=0 size={size_class} sk_tile=2048 msd_delta=-1 "
+                     "p1_ms=1.000 p3_ms=1.000\n")
+    g, _ = assert_parity(seq, off, 31, mode="bbhash", num_bins=1, tuner_cache=str(cache))
+    st = g.stats()
+    assert st["tuner_state"] == 1 and st["sort_msd_bits"] == bits
+    assert st["dedup_overflow"] > 0
+    g.close()
+
+
 @pytest.mark.parametrize("mode", ["bbhash", "learned"])
 def test_phase3_join_with_lsd_fallback_and_oversized_subbuckets(mode):
     # The LSD sort carries no side-set bytes: phase 4 then classifies the
