@@ -109,7 +109,7 @@ def traffic_md(form: str, kernel: str) -> str:
         return os.path.join(ROOT, "profiles", "classify_traffic_workload5_full.md")
     if form == "bbhash":
         return os.path.join(ROOT, "profiles", "wd_dedup_kernel_workload5_scale0.05.md")
-    return os.path.join(ROOT, "profiles", f"cs_sort_unique_{form}_traffic_workload5.md")
+    return os.path.join(ROOT, "profiles", "cs_sort_unique_kernel_workload5_scale0.05.md")
 
 
 def committed_traffic(workload: int, scale: float, form: str, kernel: str = "classify"):
