@@ -115,7 +115,9 @@ __global__ void __launch_bounds__(MS_BLOCK) ms_hist_kernel(const KeyT *keys, con
 // and each digit's run is written out with consecutive threads on
 // consecutive addresses.  Four CTAs per SM (64 registers): at 3.1 Gbp the
 // two 64-bit passes took 3.3 ms less than with three CTAs and 80 registers.
-// With pin/pout, each key's payload byte (its side-set byte) moves with it.
+// With pin/pout, each key's payload byte (its side-set byte) moves with it;
+// with PACK (pin, no pout; hashed 64-bit keys, pack = the pass's bits) the
+// byte goes into the key's packed output word (see pay_code).
 template <class KeyT, int BITS, bool PACK>
 __global__ void __launch_bounds__(MS_BLOCK, 4) ms_scatter_kernel(const KeyT *in, KeyT *out, const uint64_t *seg_off,
                                                                  const uint32_t *tile_off, uint32_t nseg, int shift,
