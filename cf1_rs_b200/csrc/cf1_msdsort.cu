@@ -58,32 +58,6 @@ CF1_D uint32_t ms_digit<Key2>(const Key2 &k, int shift, uint32_t mask, bool) {
   return KOps<Key2>::digit(k, shift, mask);
 }
 
-// Packed words (hashed split of 64-bit keys with payload bytes, pass 1 of at
-// least 6 bits): after the first pass a key's top p1 bits of h = key *
-// MS_HASH_MUL are its segment's, so the word keeps the other 64 - p1 bits of
-// h, shifted up, and the payload byte's 6-bit code in the p1 bits freed.
-// The next pass splits on the word's own top bits; the dedup rebuilds h from
-// the sub-bucket's index and the key as h * KEY_SPREAD_INV.  A single
-// occurrence's side-set byte has nibbles in {3, 5, 6, 9, F} (sideset_byte):
-// each nibble is a 3-bit code (0 also has one; anything else, which no
-// occurrence gives, reads as F).
-constexpr uint64_t pay_nib_codes() {
-  uint64_t t = 0;
-  for (uint32_t v = 0; v < 16; v++) {
-    const uint64_t c = v == 3 ? 0 : v == 5 ? 1 : v == 6 ? 2 : v == 9 ? 3 : v == 0 ? 5 : 4;
-    t |= c << (3 * v);
-  }
-  return t;
-}
-constexpr uint64_t PAY_NIB_CODE = pay_nib_codes();  // nibble -> code, 3 bits each
-constexpr uint32_t PAY_NIB_OF = 0x0F9653u;            // code -> nibble, 4 bits each (codes 0..5)
-CF1_HD uint32_t pay_code(uint32_t byte) {
-  return (uint32_t)((PAY_NIB_CODE >> (3 * (byte & 0xF))) & 7) | ((uint32_t)((PAY_NIB_CODE >> (3 * (byte >> 4))) & 7) << 3);
-}
-CF1_HD uint32_t pay_byte(uint32_t code) {
-  return ((PAY_NIB_OF >> (4 * (code & 7))) & 0xF) | (((PAY_NIB_OF >> (4 * ((code >> 3) & 7))) & 0xF) << 4);
-}
-constexpr uint32_t PACK_MIN_BITS = 6;  // a packed word's payload code needs 6 of the freed bits
 
 // ---------------------------------------------------------------- multisplit pass
 template <class KeyT, int BITS>
